@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark of the variational ground-state sweep on B200.
+
+Workload (config 2 of the measurement plan): spin-1/2 Heisenberg chain,
+J = Jz = 1, hz = 0, open boundaries, L = 100, d = 2, Dw = 5, random uniform(-1,1)
+seeded initial MPS; D schedule 16 -> 32 -> 64 -> 128 -> 256 expressed as the
+reference's IterationSchedule lines {2,16,16},{2,32,16},{2,64,32},{2,128,64},
+{2,256,128} (each line first re-runs the current D, MPSImp_Variational.C:33-40),
+Krylov dimension 20, eigensolver tolerance 1e-10.
+
+A "step" is one sweep pair (Sweep(DLeft) + Sweep(DRight)) of the L=100 chain at
+D = 256, starting from the state the schedule produced.  `value` is device time
+per step (CUDA events on the library's launch stream, max over ranks); the
+schedule itself is run once before the warm-up steps and its wall time and
+final energy are reported too.  Inputs (all site tensors, 25 MB at D = 256
+... 100 MB) are larger than L2 between steps.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--precision fp64|mixed]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Sweep s and Heff TFLOP/s, L=100 D=256: mixed+learned vs FP64 GPU at ΔE/L≤1e-9"
+L_CHAIN, S_SPIN, D_FINAL = 100, 0.5, 256
+SCHEDULE = [(2, 16, 16), (2, 32, 16), (2, 64, 32), (2, 128, 64), (2, 256, 128)]
+EPS_EIGEN = 1e-10
+KRYLOV = 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--L", type=int, default=L_CHAIN)
+    p.add_argument("--D", type=int, default=D_FINAL)
+    p.add_argument("--cpu-sites", type=int, default=4, help="bulk site updates in the CPU baseline sample")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def schedule_for(D):
+    lines = [ln for ln in SCHEDULE if ln[1] <= D]
+    if not lines or lines[-1][1] != D:
+        lines.append((2, D, max(1, D - (lines[-1][1] if lines else 16))))
+    return lines
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self._proc = None
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max((float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()), default=None)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for nm, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def fp64_peak_tflops(torch):
+    """cuBLAS DGEMM 8192^3 (torch.matmul, float64) as the FP64 denominator, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def heff_flops(d, Dw1, Dw2, D1, D2):
+    return 2.0 * d * Dw1 * D1 * D1 * D2 + 2.0 * d * Dw2 * D1 * D2 * D2 + 2.0 * d * d * Dw1 * Dw2 * D1 * D2
+
+
+def matvec_microbench(T, ctx, torch, D, precision, reps=50):
+    """Average device time of one bulk Heff application at D x D (d=2, Dw=5) on the
+    library's launch stream (set to torch's current stream so torch events see it)."""
+    import numpy as np
+    lib = ctx._lib
+    H = T.Factory(ctx).Make1D_NN_HeisenbergHamiltonian(10, 0.5, T.RegularLower, 1.0, 1.0, 0.0)
+    W = np.ascontiguousarray(H.GetW(5).ravel())
+    d, Dw = 2, 5
+    g = torch.Generator(device="cuda").manual_seed(42)
+    F = torch.rand(Dw * D * D, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    G = torch.rand(Dw * D * D, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    x = torch.rand(d * D * D, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+    lib.tn_ctx_set_stream(ctx.handle, stream.cuda_stream)
+    try:
+        prec = 0 if precision == "fp64" else 1
+        for _ in range(5):
+            T._capi.check(lib.tn_heff_matvec(ctx.handle, prec, d, Dw, Dw, D, D, W.ctypes.data, F.data_ptr(),
+                                             G.data_ptr(), x.data_ptr(), y.data_ptr()), "matvec")
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            lib.tn_heff_matvec(ctx.handle, prec, d, Dw, Dw, D, D, W.ctypes.data, F.data_ptr(), G.data_ptr(),
+                               x.data_ptr(), y.data_ptr())
+        e.record()
+        e.synchronize()
+        t = s.elapsed_time(e) / 1e3 / reps
+    finally:
+        lib.tn_ctx_set_stream(ctx.handle, None)
+    return t, heff_flops(d, Dw, Dw, D, D)
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local_rank)
+    import tensornetworks_b200 as T
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    ctx = T.Context(local_rank)
+    lib = ctx._lib
+    prec = T.FP64 if args.precision == "fp64" else T.MIXED
+    opts = T.SolverOptions(precision=prec, krylov=KRYLOV, max_restarts=10)
+    f = T.Factory(ctx)
+    H = f.Make1D_NN_HeisenbergHamiltonian(args.L, S_SPIN, T.RegularLower, 1.0, 1.0, 0.0)
+    lines = schedule_for(args.D)
+    psi = H.CreateMPS(lines[0][1], 1e-12, 1e-12)
+    psi.InitializeWith(T.Random, seed=1234)
+    sched = T.IterationSchedule()
+    for (ms, Dm, dD) in lines:
+        eps = T.Epsilons(1e-12)
+        eps.itsEigenSolverEpsilon = EPS_EIGEN
+        sched.Insert(T.IterationScheduleLine(ms, Dm, dD, eps))
+    t0 = time.perf_counter()
+    var = psi.FindVariationalGroundState(H, sched, opts)
+    schedule_s = time.perf_counter() - t0
+    sched_stats = dict(psi.last_stats)
+    E_sched = psi.GetExpectation(H)
+
+    for _ in range(args.warmup):
+        psi.Sweep(H, 1, EPS_EIGEN, opts)
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = lib.tn_launch_count()
+    step_ms, matvecs, flops = [], 0, 0.0
+    for _ in range(args.steps):
+        st = psi.Sweep(H, 1, EPS_EIGEN, opts)
+        step_ms.append(st["sweep_ms"])
+        matvecs += st["matvecs"]
+        flops += st["heff_flop"]
+    torch.cuda.synchronize()
+    launches = lib.tn_launch_count() - launches0
+    clocks.stop()
+    t_step = sum(step_ms) / len(step_ms) / 1e3
+    if dist:
+        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = float(tt.item())
+    E_after = psi.GetExpectation(H)
+
+    # --- end to end through the C ABI with host buffers (per step: upload all sites,
+    #     one sweep pair, download all sites)
+    sites = [psi.GetSite(i) for i in range(1, args.L + 1)]
+    h2d = sum(a.nbytes for a in sites)
+    e2e_times = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i, a in enumerate(sites, start=1):
+            psi.SetSite(i, a)
+        psi.PrepareSweeps(H)
+        psi.Sweep(H, 1, EPS_EIGEN, opts)
+        sites = [psi.GetSite(i) for i in range(1, args.L + 1)]
+        e2e_times.append(time.perf_counter() - t0)
+    d2h = sum(a.nbytes for a in sites)
+    e2e = sum(e2e_times) / len(e2e_times)
+
+    # --- roofline of the dominant kernel (the bulk Heff contraction chain)
+    t_mv, F_mv = matvec_microbench(T, ctx, torch, args.D, args.precision)
+    peaks, peak_kind = measured_peaks()
+    if args.precision == "fp64":
+        peak = fp64_peak_tflops(torch)
+        peak_src = "cuBLAS DGEMM 8192^3 measured in this run"
+    else:
+        peak = peaks["bf16_tflops"] / 3.0
+        peak_src = f"{peak_kind} bf16 burst / 3 (BF16x3)"
+    achieved = F_mv / t_mv / 1e12
+    roofline = {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "kernel": "heff_matvec (3-stage chain)",
+                "per_launch_us": round(t_mv * 1e6, 2), "flop_per_launch": F_mv, "peak_source": peak_src}
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu:
+            cpu = cpu_baseline_same_state(args, sites, step_ms, psi)
+        clk = clocks.summary()
+        out = {
+            "metric": METRIC,
+            "value": round(t_step, 6),
+            "unit": "s per sweep pair (L=100, D=256)",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(t_step * 1e3, 3),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "bf16x3+f32acc / f64",
+            "data": "synthetic (seeded uniform(-1,1) initial MPS)",
+            "config": {"workload": f"Heisenberg S=1/2 L={args.L} open chain, d=2, Dw=5, one sweep pair at "
+                                   f"D={args.D} after the D 16->{args.D} schedule (2 sweeps/line), Krylov 20, "
+                                   f"eig tol 1e-10",
+                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "inputs > L2 (site tensors + environments ~ 0.6 GB at D=256)"},
+            "heff_tflops_sweep": round(flops / (sum(step_ms) / 1e3) / 1e12, 4),
+            "matvecs_per_step": matvecs / args.steps,
+            "schedule_s": round(schedule_s, 3),
+            "schedule_sweep_ms": round(sched_stats["sweep_ms"], 1),
+            "energy_per_bond": E_after / (args.L - 1),
+            "energy_schedule_per_bond": E_sched / (args.L - 1),
+            "variance": var,
+            "e2e": {"value": round(e2e, 6), "unit": "s per sweep pair (L=100, D=256)", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_baseline_same_state(args, sites, step_ms, psi):
+    """The oracle (FP64 C++ restatement, OpenMP on all host cores) timed on the same
+    MPS for a bounded sample of bulk site updates, scaled to a sweep pair by the
+    algorithmic Heff cost of every site."""
+    from oracle import oracle as O
+    ncores = os.cpu_count() or 1
+    first = args.L // 2 - args.cpu_sites // 2
+    sec, nmv = O.sweep_sample(args.L, S_SPIN, sites, first, args.cpu_sites, krylov=KRYLOV, max_restarts=10,
+                              tol=EPS_EIGEN, nthreads=ncores)
+    per_site = sec / args.cpu_sites
+    d, Dw = 2, 5
+    bulk = heff_flops(d, Dw, Dw, args.D, args.D)
+    w = 0.0
+    for a in sites:
+        D1, D2 = a.shape[1], a.shape[2]
+        w += heff_flops(d, Dw, Dw, D1, D2) / bulk
+    est = per_site * 2.0 * w
+    return {"value": round(est, 3), "unit": "s per sweep pair (L=100, D=256)", "cores": ncores, "kind": "port",
+            "sample": f"{args.cpu_sites} bulk D={args.D} site updates (Lanczos Krylov 20 tol 1e-10 + QR gauge + "
+                      f"environment) of the GPU's converged state in {sec:.2f}s ({nmv} matvecs); scaled by the "
+                      f"Heff cost of all 2L site updates of a sweep pair"}
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU algorithm for the path: the oracle restatement (the reference
+    itself cannot be built: its oml/LAPACK/ARPACK/PRIMME dependencies are absent), on
+    all host cores, on a bounded sample of the same workload."""
+    if rank != 0:
+        return None
+    import numpy as np
+    from oracle import oracle as O
+    O.build()
+    ncores = os.cpu_count() or 1
+    L, D, d = args.L, args.D, 2
+    # right-canonical random MPS of the final shapes (ramp min(d^k, D) from both ends)
+    dims = []
+    for i in range(L):
+        l = 1 if i == 0 else min(D, d ** i, d ** (L - i))
+        r = 1 if i == L - 1 else min(D, d ** (i + 1), d ** (L - i - 1))
+        dims.append((l, r))
+    rng = np.random.default_rng(1234)
+    sites = [rng.uniform(-1, 1, size=(d,) + dm) for dm in dims]
+    first = L // 2 - args.cpu_sites // 2
+    times = []
+    for _ in range(max(1, args.steps)):
+        sec, nmv = O.sweep_sample(L, S_SPIN, sites, first, args.cpu_sites, krylov=KRYLOV, max_restarts=10,
+                                  tol=EPS_EIGEN, nthreads=ncores)
+        times.append(sec)
+    per_site = sum(times) / len(times) / args.cpu_sites
+    bulk = heff_flops(d, 5, 5, D, D)
+    w = sum(heff_flops(d, 5, 5, a, b) / bulk for a, b in dims)
+    value = per_site * 2.0 * w
+    sample = (f"{args.cpu_sites} bulk D={D} site updates (Lanczos Krylov 20 tol 1e-10 + QR gauge + environment) "
+              f"of a random right-canonical L={L} MPS per step, scaled by the Heff cost of the 2L site updates "
+              f"of a sweep pair; oracle C++ restatement (reference not buildable here)")
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "s per sweep pair (L=100, D=256)",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value * 1e3, 1),
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "impl": "reference",
+           "config": {"workload": f"Heisenberg S=1/2 L={L}, one sweep pair at D={D}", "precision": "fp64"},
+           "cpu_baseline": {"value": round(value, 3), "unit": "s per sweep pair", "cores": ncores, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": round(value, 3), "unit": "s per sweep pair (L=100, D=256)", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus else 1)))
+    if "WORLD_SIZE" not in os.environ:
+        world = 1
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

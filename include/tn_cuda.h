@@ -1,0 +1,222 @@
+/*
+ * tn_cuda.h -- C ABI of the B200 (sm_100a) variational ground-state sweep.
+ *
+ * This is the drop-in boundary for the LAPACK/ARPACK/PRIMME solver path of
+ * JanReimers/TensorNetworks.  Every entry point names the reference interface
+ * it replaces (file:line, paths relative to the reference project root).
+ * Signatures use plain C types only: opaque handles, int status codes, raw
+ * pointers and sizes.  Pointers documented as "device" are CUDA device
+ * pointers; "host" pointers are ordinary CPU memory.
+ *
+ * Layout conventions (0-based indices, column-major matrices):
+ *   site tensor A (d x D1 x D2): d consecutive column-major D1 x D2 blocks,
+ *       element (n,i1,i2) at n*D1*D2 + i2*D1 + i1  (MPSSite::itsMs[n](i1,i2),
+ *       TensorNetworksImp/MPS/MPSSite.H:175-177);
+ *   MPO tensor W (Dw1 x Dw2 x d x d): element (w1,w2,m,n) at
+ *       ((w1*Dw2 + w2)*d + m)*d + n, the value <m|W(w1,w2)|n>;
+ *   environment F (Dw x D x D): Dw consecutive column-major D x D blocks,
+ *       element (w,i,j) at w*D*D + j*D + i (bra index i, ket index j; the
+ *       Vector3 caches of MPSSite_Contractions.C:292-400).
+ *
+ * Threading: a tn_ctx owns one CUDA stream and its scratch memory; calls on
+ * one context must not overlap.  Distinct contexts are independent.
+ */
+#ifndef TN_CUDA_H
+#define TN_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+    TN_OK             = 0,
+    TN_NOT_CONVERGED  = 1,  /* iteration cap reached (result still usable)  */
+    TN_BAD_SHAPE      = 2,  /* inconsistent dimensions                       */
+    TN_NAN_DETECTED   = 3,  /* non-finite value in an input or result        */
+    TN_CUDA_ERROR     = 4,  /* a CUDA runtime call failed                    */
+    TN_BAD_ARG        = 5,  /* null handle/pointer or out-of-range argument  */
+    TN_NO_DEVICE      = 6,  /* no sm_100 device visible                      */
+    TN_OUT_OF_MEMORY  = 7
+};
+
+/* MPO forms, numbered as TensorNetworks/Enums.H:17 (enum MPOForm). */
+enum { TN_FORM_REGULAR_UPPER = 1, TN_FORM_REGULAR_LOWER = 2 };
+/* Directions, as TensorNetworks/Enums.H:10 (enum Direction). */
+enum { TN_DLEFT = 0, TN_DRIGHT = 1 };
+/* Arithmetic of the Heff / environment contractions. */
+enum {
+    TN_PREC_FP64  = 0,  /* FP64 throughout (the plain GPU sweep)             */
+    TN_PREC_MIXED = 1   /* BF16x3 tcgen05 contractions with FP32 accumulate,
+                           FP64 Lanczos/QR/SVD/energies (mixed path)         */
+};
+/* Eigensolvers for the site problem. */
+enum {
+    TN_EIG_LANCZOS  = 0,  /* restarted Lanczos, full reorthogonalisation    */
+    TN_EIG_DAVIDSON = 1   /* Davidson with diagonal or learned preconditioner */
+};
+
+typedef struct tn_ctx_s*         tn_ctx;
+typedef struct tn_hamiltonian_s* tn_hamiltonian;
+typedef struct tn_mps_s*         tn_mps;
+
+/* One IterationScheduleLine (TensorNetworks/IterationSchedule.H:13-38) with
+ * the Epsilons fields the variational search reads (Epsilons.H:11-26). */
+typedef struct {
+    int    max_sweeps;   /* itsMaxGSSweepIterations (pairs of half-sweeps) */
+    int    Dmax;         /* itsDmax                                        */
+    int    deltaD;       /* itsDeltaD                                      */
+    double eps_energy;   /* itsDelatEnergy1Epsilon                         */
+    double eps_lambda;   /* itsDeltaLambdaEpsilon                          */
+    double eps_eigen;    /* itsEigenSolverEpsilon                          */
+} tn_sched_line;
+
+/* Solver options (no counterpart in the reference, which hard-wires
+ * LapackEigenSolver at MPSSite.C:29 and LapackSVDSolver at
+ * MPSSite_Normalization.C:49). */
+typedef struct {
+    int precision;       /* TN_PREC_*                                      */
+    int eigensolver;     /* TN_EIG_*                                       */
+    int krylov;          /* Krylov/Davidson basis size per restart (20)    */
+    int max_restarts;    /* restarts per site (10)                         */
+    int use_learned;     /* 1: learned preconditioner (Davidson only)      */
+    int verbose;         /* 1: print the reference's per-sweep log line     */
+} tn_solver_options;
+
+/* Per-run statistics, device-timed with CUDA events. */
+typedef struct {
+    double energy;          /* <H> after the last line (GetExpectation)    */
+    double energy2;         /* <H^2>                                        */
+    double variance;        /* <H^2>-<H>^2 (the reference's return value)  */
+    int    total_sweeps;    /* sweep pairs over all lines                   */
+    int    final_D;         /* GetMaxD()                                    */
+    long long matvecs;      /* Heff applications                            */
+    long long matvecs_fp64; /* of which FP64 (refinement steps, mixed path) */
+    double heff_flop;       /* algorithmic flops of all Heff applications    */
+    double heff_ms;         /* device time inside the Heff contractions      */
+    double sweep_ms;        /* device time of all sweeps                     */
+    double last_dE;         /* GetMaxDeltaE() after the last sweep pair      */
+    double last_dlambda;    /* GetMaxDeltal() after the last sweep pair      */
+    int    not_converged;   /* site solves that hit the iteration cap        */
+    int    fallbacks;       /* learned-preconditioner fallbacks taken        */
+} tn_sweep_stats;
+
+/* ---- context ------------------------------------------------------------- */
+const char* tn_status_string(int status);
+/* Last error message recorded on this thread (for diagnostics). */
+const char* tn_last_error(void);
+int tn_ctx_create(int device, tn_ctx* out);
+int tn_ctx_destroy(tn_ctx ctx);
+/* Use an external cudaStream_t (passed as void*); NULL restores the own stream. */
+int tn_ctx_set_stream(tn_ctx ctx, void* stream);
+int tn_ctx_synchronize(tn_ctx ctx);
+
+/* ---- Factory / Hamiltonian / MPO ------------------------------------------
+ * Factory::Make1D_NN_HeisenbergHamiltonian (TensorNetworks/Factory.H:16,
+ * TensorNetworksImp/FactoryImp.C:21-26) -> HamiltonianImp (MPO of L sites,
+ * Hamiltonian_1D_NN_Heisenberg.C:35-79, boundaries SiteOperatorImp.C:109-134). */
+int tn_hamiltonian_create_heisenberg(tn_ctx ctx, int L, double S, int form, double Jxy,
+                                     double Jz, double hz, tn_hamiltonian* out);
+int tn_hamiltonian_destroy(tn_hamiltonian H);
+/* SiteOperator::GetDws / Getd (TensorNetworks/SiteOperator.H:44-46). */
+int tn_hamiltonian_site_dims(tn_hamiltonian H, int site, int* Dw1, int* Dw2, int* d);
+/* SiteOperator::GetW (SiteOperator.H:52): copies W of a site into host memory. */
+int tn_hamiltonian_get_w(tn_hamiltonian H, int site, double* W_host);
+
+/* ---- MPS -------------------------------------------------------------------
+ * Hamiltonian::CreateMPS (TensorNetworks/Hamiltonian.H:26, HamiltonianImp.C:41-44). */
+int tn_mps_create(tn_hamiltonian H, int D, double normEps, double epsSV, tn_mps* out);
+int tn_mps_destroy(tn_mps psi);
+/* MPS::InitializeWith(Random) (MPS.H:17, MPSSite.C:119-127): uniform(-1,1)
+ * from mt19937_64(seed), sites 1..L in order, each scaled 1/sqrt(d*D1*D2). */
+int tn_mps_initialize_random(tn_mps psi, uint64_t seed);
+/* Site tensor access (host buffers, site 1-based). */
+int tn_mps_get_site_dims(tn_mps psi, int site, int* D1, int* D2);
+int tn_mps_get_site(tn_mps psi, int site, double* A_host);
+int tn_mps_set_site(tn_mps psi, int site, int D1, int D2, const double* A_host);
+/* Bond singular values (Bond::GetSVs, Bond.H), normalised; bond b in 1..L-1. */
+int tn_mps_get_bond(tn_mps psi, int bond, int* D, double* s_host);
+/* MPS::Normalize (MPS.C:8) / MPS::NormalizeQR (MPSImp_Normalization.C:39-63). */
+int tn_mps_normalize(tn_mps psi, int direction);
+/* MPS::GetMaxD (MPS.H:70). */
+int tn_mps_get_max_d(tn_mps psi, int* D);
+/* MPS::GetExpectation(MPO*) (MPSImp_ExpectationsAndDMs.C:33-45), FP64 on device. */
+int tn_mps_get_expectation(tn_mps psi, tn_hamiltonian H, double* E);
+/* <H^2> with the product MPO of Hamiltonian::CreateH2Operator (Hamiltonian.C:8-16). */
+int tn_mps_get_expectation_h2(tn_mps psi, tn_hamiltonian H, double* E2);
+/* MPS::FindVariationalGroundState(H, IterationSchedule) (MPS.H:36,
+ * MPSImp_Variational.C:16-62).  Returns <H^2>-<H>^2 in *variance. */
+int tn_mps_find_variational_ground_state(tn_mps psi, tn_hamiltonian H,
+                                         const tn_sched_line* lines, int nlines,
+                                         const tn_solver_options* opt,
+                                         tn_sweep_stats* stats, double* variance);
+/* nsweeps pairs of MPSImp::Sweep(DLeft) + Sweep(DRight) (MPSImp_Variational.C:43-47,
+ * 64-76) at the current bond dimension, without the <H>, <H^2> evaluation that
+ * closes each D step of FindVariationalGroundState.  The MPS must be right-
+ * normalised with its right environments loaded (true after
+ * tn_mps_find_variational_ground_state or tn_mps_prepare_sweeps). */
+int tn_mps_sweep(tn_mps psi, tn_hamiltonian H, int nsweeps, double eps_eigen,
+                 const tn_solver_options* opt, tn_sweep_stats* stats);
+/* MPS::Normalize(DRight) followed by MPSImp::LoadHeffCaches (MPSImp_Variational.C:18-19). */
+int tn_mps_prepare_sweeps(tn_mps psi, tn_hamiltonian H);
+/* Per-site Ritz energies of the last solves (MPSSite::itsEmin), L values. */
+int tn_mps_get_site_energies(tn_mps psi, double* E_host);
+
+/* Number of kernels this library has launched in this process (diagnostics;
+ * no counterpart in the reference). */
+unsigned long long tn_launch_count(void);
+
+/* ---- solver interfaces (device pointers) --------------------------------
+ * SparseEigenSolverClient::DoMatVecContraction (NumericalMethods/
+ * SparseEigenSolver.H:17-24) for the site problem: y = Heff x, the
+ * matrix-free form of MPSSite::GetHeff (MPSSite_Contractions.C:155-193). */
+int tn_heff_matvec(tn_ctx ctx, int precision, int d, int Dw1, int Dw2, int D1, int D2,
+                   const double* W_host, const double* F, const double* G,
+                   const double* x, double* y);
+/* diag(Heff) (feature of the Davidson preconditioner). */
+int tn_heff_diag(tn_ctx ctx, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
+                 const double* F, const double* G, double* diag);
+/* MPSSite::IterateLeft_F / IterateRightF (MPSSite_Contractions.C:292-400). */
+int tn_env_left(tn_ctx ctx, int precision, int d, int Dw1, int Dw2, int D1, int D2,
+                const double* W_host, const double* A, const double* F, double* Fout);
+int tn_env_right(tn_ctx ctx, int precision, int d, int Dw1, int Dw2, int D1, int D2,
+                 const double* W_host, const double* A, const double* G, double* Gout);
+/* Lowest eigenpair of Heff: replaces LapackEigenSolver<T>::Solve(Heff,eps,2)
+ * (NumericalMethods/LapackEigenSolver.C:62-109) as called by MPSSite::Refine
+ * (MPSSite_Variational.C:18-33).  x: start vector in, Ritz vector out. */
+int tn_eigensolve_heff(tn_ctx ctx, const tn_solver_options* opt, int d, int Dw1, int Dw2,
+                       int D1, int D2, const double* W_host, const double* F,
+                       const double* G, double* x, double tol, double* theta,
+                       double* residual, int* matvecs);
+/* Dense symmetric eigensolver, lowest k pairs: EigenSolver<T>::Solve
+ * (NumericalMethods/EigenSolver.H:31).  A: N x N (lda), U: N x k (ldu). */
+int tn_eigensolve_dense(tn_ctx ctx, int N, const double* A, int lda, int k, double tol,
+                        double* w_host, double* U, int ldu);
+/* SVDSolver<T>::Solve (NumericalMethods/SVDSolver.H:19, LapackSVDSolver.C:42-90),
+ * one-sided Jacobi: A (m x n) = U s Vt, k = min(m,n); U m x k, s k (device),
+ * Vt k x n.  Zero singular values get orthonormal completion vectors. */
+int tn_svd(tn_ctx ctx, int m, int n, const double* A, int lda, double* U, int ldu,
+           double* s, double* Vt, int ldvt);
+/* Singular values only (descending). */
+int tn_svd_values(tn_ctx ctx, int m, int n, const double* A, int lda, double* s);
+/* QRSolver<T>::SolveThinQR / SolveThinLQ (NumericalMethods/QRSolver.H:18-21,
+ * LapackQRSolver.C:116-160,277-320), Householder: Q m x k, R k x n;
+ * L m x k, Q k x n. */
+int tn_qr(tn_ctx ctx, int m, int n, const double* A, int lda, double* Q, int ldq,
+          double* R, int ldr);
+int tn_lq(tn_ctx ctx, int m, int n, const double* A, int lda, double* L, int ldl,
+          double* Q, int ldq);
+/* SVCompressor<T>::Compress (TensorNetworks/SVCompressor.H:20,
+ * SVCompressorImp.C:19-73) on device data: s (k, descending) is truncated and
+ * rescaled in place; U (m x k, ldu) and Vt (k x n, ldvt) keep their leading
+ * D columns/rows.  Returns the kept D and the discarded sum of s^2. */
+int tn_compress(tn_ctx ctx, int Dmax, double eps, int k, double* s, int* D_out,
+                double* discarded);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TN_CUDA_H */

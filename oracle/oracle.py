@@ -69,6 +69,8 @@ def lib():
         L.orc_compress.restype = C.c_double
         L.orc_find_ground_state.argtypes = [i, d, i, d, d, d, i, ull, C.POINTER(SchedLine), i,
                                             C.POINTER(Options), C.POINTER(Result), C.c_void_p]
+        L.orc_sweep_sample.argtypes = [i, d, i, d, d, d, C.c_void_p, C.c_void_p, _dp, i, i, i, i, d, i,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.orc_ed_ground.argtypes = [i, d, d, d, d, i, d, C.POINTER(C.c_double)]
         L.orc_itebd.argtypes = [d, d, d, d, i, _dp, C.POINTER(C.c_int), i, ull, d, C.POINTER(C.c_double)]
         _lib = L
@@ -251,6 +253,20 @@ def find_ground_state(L, S, Dstart, lines, *, form=2, Jxy=1.0, Jz=1.0, hz=0.0, s
     if se is not None:
         out["site_energies"] = se
     return out
+
+
+def sweep_sample(L, S, sites, first, nsites, *, form=2, Jxy=1.0, Jz=1.0, hz=0.0, krylov=20, max_restarts=10,
+                 tol=1e-10, nthreads=0):
+    """Time nsites DLeft site updates of the oracle on the given MPS (list of A[n,i1,i2])."""
+    D1s = np.array([a.shape[1] for a in sites], dtype=np.int32)
+    D2s = np.array([a.shape[2] for a in sites], dtype=np.int32)
+    flat = np.concatenate([site_flat(a) for a in sites])
+    sec = C.c_double(); nmv = C.c_longlong()
+    rc = lib().orc_sweep_sample(L, S, form, Jxy, Jz, hz, D1s.ctypes.data, D2s.ctypes.data, flat, first, nsites,
+                                krylov, max_restarts, tol, nthreads, C.byref(sec), C.byref(nmv))
+    if rc != 0:
+        raise RuntimeError("orc_sweep_sample failed")
+    return sec.value, nmv.value
 
 
 def ed_ground(L, S, Jxy=1.0, Jz=1.0, hz=0.0, field_mode=0, tol=1e-12):

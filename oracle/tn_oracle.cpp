@@ -10,6 +10,7 @@
 #include <cassert>
 #include <cmath>
 #include <cstdio>
+#include <chrono>
 #include <cstring>
 #include <limits>
 #include <random>
@@ -555,11 +556,12 @@ static void householder_qr(const Mat& Ain, Mat& Q, Mat& R) {
     Mat A = Ain;
     Vec tau(k, 0.0);
     for (int j = 0; j < k; ++j) {
-        double nrm = 0;
-        for (int i = j; i < m; ++i) nrm += A(i, j) * A(i, j);
-        nrm = std::sqrt(nrm);
+        // dlarfg convention: no reflection when the sub-column is already zero
+        double xn2 = 0;
+        for (int i = j + 1; i < m; ++i) xn2 += A(i, j) * A(i, j);
         double x0 = A(j, j);
-        if (nrm == 0.0) { tau[j] = 0; continue; }
+        if (xn2 == 0.0) { tau[j] = 0; continue; }
+        double nrm = std::sqrt(x0 * x0 + xn2);
         double beta = (x0 >= 0) ? -nrm : nrm;
         double v0 = x0 - beta;
         for (int i = j + 1; i < m; ++i) A(i, j) /= v0;
@@ -1497,6 +1499,56 @@ int orc_find_ground_state(int L, double S, int form, double Jxy, double Jz, doub
     res->last_dlambda = dl;
     if (site_energies)
         for (int ia = 1; ia <= L; ++ia) site_energies[ia - 1] = psi.sites[ia].Emin;
+    return 0;
+}
+
+int orc_sweep_sample(int L, double S, int form, double Jxy, double Jz, double hz, const int* D1s,
+                     const int* D2s, const double* sites, int first, int nsites, int krylov, int max_restarts,
+                     double tol, int nthreads, double* seconds, long long* matvecs) {
+    if (L < 2 || first < 1 || first + nsites - 1 > L - 1 || nsites < 1) return -1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    Model H = make_model(L, S, form, Jxy, Jz, hz);
+    MPS psi;
+    psi.opt.eig_mode = 1;
+    psi.opt.gauge = 1;
+    psi.opt.krylov = krylov > 0 ? krylov : 20;
+    psi.opt.max_restarts = max_restarts > 0 ? max_restarts : 10;
+    mps_init(psi, L, H.d, 1, 0);
+    size_t off = 0;
+    for (int ia = 1; ia <= L; ++ia) {
+        Site& st = psi.sites[ia];
+        st.D1 = D1s[ia - 1];
+        st.D2 = D2s[ia - 1];
+        size_t cnt = (size_t)H.d * st.D1 * st.D2;
+        st.A.assign(sites + off, sites + off + cnt);
+        off += cnt;
+    }
+    for (int b = 1; b < L; ++b) {
+        psi.bonds[b].D = psi.sites[b].D2;
+        psi.bonds[b].s.assign(psi.bonds[b].D, 1.0 / psi.bonds[b].D);
+    }
+    // untimed preparation: left-normalise 1..first-1, build the environments
+    for (int ia = 1; ia < first; ++ia) {
+        Site& s = psi.sites[ia];
+        Mat A = reshape_before(s, H.d, true);
+        Mat Q, R;
+        householder_qr(A, Q, R);
+        transfer(psi.sites[ia + 1], H.d, true, R);
+        reshape_after(s, H.d, true, Q);
+        compute_left_env(psi, H, ia);
+    }
+    for (int ia = L; ia > first; --ia) compute_right_env(psi, H, ia);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int ia = first; ia < first + nsites; ++ia) {
+        refine_site(psi, H, ia, tol);
+        normalize_site(psi, ia, true, 1);
+        compute_left_env(psi, H, ia);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    *seconds = std::chrono::duration<double>(t1 - t0).count();
+    *matvecs = psi.matvecs;
     return 0;
 }
 

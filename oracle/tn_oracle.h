@@ -136,6 +136,15 @@ int orc_find_ground_state(int L, double S, int form, double Jxy, double Jz, doub
                           const orc_sched_line* lines, int nlines,
                           const orc_options* opt, orc_result* res,
                           double* site_energies /* L, may be NULL */);
+/* Timing sample of the sweep's site update on a given MPS (the CPU baseline):
+ * sites are given as L tensors (dims D1s/D2s, concatenated in site order, shared
+ * layout).  Sites 1..first-1 are left-normalised (QR), environments built, and
+ * then nsites consecutive DLeft site updates (Lanczos + QR gauge + left
+ * environment, the same work as one site of the CUDA sweep) are timed. */
+int orc_sweep_sample(int L, double S, int form, double Jxy, double Jz, double hz,
+                     const int* D1s, const int* D2s, const double* sites, int first, int nsites,
+                     int krylov, int max_restarts, double tol, int nthreads,
+                     double* seconds, long long* matvecs);
 /* Exact diagonalisation (Lanczos on the d^L space). field_mode 0: the MPO's
  * +hz*Sz once per site; 1: the reference FullState's GetH convention
  * (hz*(Sz_a+Sz_b) on every bond). */

@@ -1,0 +1,8 @@
+"""tensornetworks_b200 -- B200-native (sm_100a) variational ground-state sweep
+for open 1-D spin chains, with the API surface of JanReimers/TensorNetworks'
+Factory -> Hamiltonian -> MPS::FindVariationalGroundState path."""
+from ._capi import LIB_PATH, TNError, load  # noqa: F401
+from .api import (  # noqa: F401
+    DAVIDSON, FP64, LANCZOS, MIXED, Context, CudaEigenSolver, CudaQRSolver, CudaSVDSolver, DLeft, DRight,
+    Epsilons, Factory, Hamiltonian, IterationSchedule, IterationScheduleLine, MPS, Random, RegularLower,
+    RegularUpper, SolverOptions, SVCompressor, default_context)

@@ -1,0 +1,432 @@
+"""Reference-shaped Python API over the C ABI.
+
+Mirrors the public surface of JanReimers/TensorNetworks used by the
+variational ground-state path (TensorNetworks/Factory.H, Hamiltonian.H,
+MPS.H, IterationSchedule.H, Epsilons.H, SVCompressor.H and the solver
+interfaces of NumericalMethods/), with the same names and argument meaning, so
+that a script written against PyTensorNetworks reads the same here:
+
+    f = Factory.GetFactory()
+    H = f.Make1D_NN_HeisenbergHamiltonian(L, S, Jxy, Jz, hz)
+    psi = H.CreateMPS(D, 1e-12, 1e-12)
+    psi.InitializeWith(Random)
+    isched = IterationSchedule(); isched.Insert(IterationScheduleLine(100, Dfinal, Epsilons()))
+    E2 = psi.FindVariationalGroundState(H, isched)
+    E1 = psi.GetExpectation(H) / (L - 1)
+
+All arithmetic runs in libtn_cuda.so on the GPU.  Device memory for the solver
+classes is handled with torch CUDA tensors (plumbing only).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import check
+
+# Enums (TensorNetworks/Enums.H)
+DLeft, DRight = capi.TN_DLEFT, capi.TN_DRIGHT
+Product, Random, Neel, Constant = 0, 1, 2, 3
+RegularUpper, RegularLower = capi.TN_FORM_REGULAR_UPPER, capi.TN_FORM_REGULAR_LOWER
+FP64, MIXED = capi.TN_PREC_FP64, capi.TN_PREC_MIXED
+LANCZOS, DAVIDSON = capi.TN_EIG_LANCZOS, capi.TN_EIG_DAVIDSON
+
+
+# ---------------------------------------------------------------------------
+# Context
+# ---------------------------------------------------------------------------
+class Context:
+    """One CUDA device + stream (tn_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = capi.load()
+        h = C.c_void_p()
+        check(self._lib.tn_ctx_create(device, C.byref(h)), "tn_ctx_create")
+        self.handle = h
+        self.device = device
+
+    def synchronize(self):
+        check(self._lib.tn_ctx_synchronize(self.handle), "tn_ctx_synchronize")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.tn_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+# ---------------------------------------------------------------------------
+# Schedule (TensorNetworks/Epsilons.H, IterationSchedule.H)
+# ---------------------------------------------------------------------------
+@dataclass
+class Epsilons:
+    """Epsilons (Epsilons.H:11-26); every field defaults to default_eps (Epsilons.C:9-19)."""
+    default_eps: float = 1e-12
+    itsDelatEnergy1Epsilon: float = None
+    itsDelatEnergy2Epsilon: float = None
+    itsDelatNormEpsilon: float = None
+    itsEigenSolverEpsilon: float = None
+    itsNormalizationEpsilon: float = None
+    itsMPSCompressEpsilon: float = None
+    itsMPOCompressEpsilon: float = None
+    itsSparseMatrixEpsilon: float = None
+    itsDeltaLambdaEpsilon: float = None
+
+    def __post_init__(self):
+        for f in self.__dataclass_fields__:
+            if f != "default_eps" and getattr(self, f) is None:
+                setattr(self, f, self.default_eps)
+
+
+class IterationScheduleLine:
+    """IterationScheduleLine(maxiter, Dmax, [DeltaD,] eps) (IterationSchedule.C:9-36)."""
+
+    def __init__(self, maxiter: int, Dmax: int, *args):
+        if len(args) == 1:
+            DeltaD, eps = 1, args[0]
+        elif len(args) == 2:
+            DeltaD, eps = args
+        else:
+            raise TypeError("IterationScheduleLine(maxiter, Dmax, [DeltaD,] eps)")
+        if maxiter <= 0 or Dmax <= 0 or DeltaD <= 0:
+            raise ValueError("maxiter, Dmax and DeltaD must be positive")
+        self.itsMaxGSSweepIterations = int(maxiter)
+        self.itsDmax = int(Dmax)
+        self.itsDeltaD = int(DeltaD)
+        self.itsEps = eps
+
+    def to_c(self) -> capi.SchedLine:
+        e = self.itsEps
+        return capi.SchedLine(self.itsMaxGSSweepIterations, self.itsDmax, self.itsDeltaD,
+                              e.itsDelatEnergy1Epsilon, e.itsDeltaLambdaEpsilon, e.itsEigenSolverEpsilon)
+
+
+class IterationSchedule:
+    def __init__(self):
+        self.lines: List[IterationScheduleLine] = []
+
+    def Insert(self, line: IterationScheduleLine):
+        self.lines.append(line)
+
+    def __len__(self):
+        return len(self.lines)
+
+
+@dataclass
+class SolverOptions:
+    precision: int = FP64
+    eigensolver: int = LANCZOS
+    krylov: int = 20
+    max_restarts: int = 10
+    use_learned: int = 0
+    verbose: int = 0
+
+    def to_c(self):
+        return capi.SolverOptions(self.precision, self.eigensolver, self.krylov, self.max_restarts,
+                                  self.use_learned, self.verbose)
+
+
+# ---------------------------------------------------------------------------
+# Factory / Hamiltonian / MPS
+# ---------------------------------------------------------------------------
+class Factory:
+    """Factory (TensorNetworks/Factory.H:9-33) for the Heisenberg/XXZ chain."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+
+    @staticmethod
+    def GetFactory(ctx: Optional[Context] = None) -> "Factory":
+        return Factory(ctx)
+
+    def Make1D_NN_HeisenbergHamiltonian(self, L: int, S: float, *args) -> "Hamiltonian":
+        """(L, S, MPOForm, Jxy, Jz, hz) as Factory.H:16, or (L, S, Jxy, Jz, hz) as the Python bindings."""
+        if len(args) == 4:
+            form, Jxy, Jz, hz = args
+        elif len(args) == 3:
+            form, (Jxy, Jz, hz) = RegularLower, args
+        else:
+            raise TypeError("Make1D_NN_HeisenbergHamiltonian(L, S, [form,] Jxy, Jz, hz)")
+        return Hamiltonian(self.ctx, L, S, form, Jxy, Jz, hz)
+
+    def MakeMPSCompressor(self, Dmax: int, epsSV: float) -> "SVCompressor":
+        return SVCompressor(Dmax, epsSV, self.ctx)
+
+
+class Hamiltonian:
+    """HamiltonianImp: the MPO of L sites (Hamiltonian.H:15-41)."""
+
+    def __init__(self, ctx: Context, L, S, form, Jxy, Jz, hz):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        self.L, self.S, self.form = int(L), float(S), int(form)
+        self.Jxy, self.Jz, self.hz = float(Jxy), float(Jz), float(hz)
+        h = C.c_void_p()
+        check(self._lib.tn_hamiltonian_create_heisenberg(ctx.handle, self.L, self.S, self.form, self.Jxy,
+                                                         self.Jz, self.hz, C.byref(h)),
+              "tn_hamiltonian_create_heisenberg")
+        self.handle = h
+
+    def GetL(self):
+        return self.L
+
+    def Getd(self):
+        return int(round(2 * self.S + 1))
+
+    def GetS(self):
+        return self.S
+
+    def GetW(self, site: int) -> np.ndarray:
+        """SiteOperator::GetW of a site (1-based) as an array (Dw1, Dw2, d, d)."""
+        a, b, d = C.c_int(), C.c_int(), C.c_int()
+        check(self._lib.tn_hamiltonian_site_dims(self.handle, site, C.byref(a), C.byref(b), C.byref(d)),
+              "tn_hamiltonian_site_dims")
+        W = np.empty((a.value, b.value, d.value, d.value))
+        check(self._lib.tn_hamiltonian_get_w(self.handle, site, W.ctypes.data), "tn_hamiltonian_get_w")
+        return W
+
+    def CreateMPS(self, D: int, normEps: float = 1e-12, epsSV: float = 1e-12) -> "MPS":
+        return MPS(self, D, normEps, epsSV)
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if getattr(self, "handle", None):
+                self._lib.tn_hamiltonian_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class MPS:
+    """Finite MPS resident on the GPU (TensorNetworks/MPS.H:14-75)."""
+
+    def __init__(self, H: Hamiltonian, D: int, normEps: float, epsSV: float):
+        self.H = H
+        self._lib = H._lib
+        self.L, self.d = H.L, H.Getd()
+        h = C.c_void_p()
+        check(self._lib.tn_mps_create(H.handle, int(D), normEps, epsSV, C.byref(h)), "tn_mps_create")
+        self.handle = h
+        self.last_stats: Optional[dict] = None
+
+    def InitializeWith(self, state: int = Random, seed: int = 1234):
+        if state != Random:
+            raise NotImplementedError("only the Random initial state is provided")
+        check(self._lib.tn_mps_initialize_random(self.handle, int(seed)), "tn_mps_initialize_random")
+
+    def Normalize(self, direction: int):
+        check(self._lib.tn_mps_normalize(self.handle, int(direction)), "tn_mps_normalize")
+
+    def GetMaxD(self) -> int:
+        D = C.c_int()
+        check(self._lib.tn_mps_get_max_d(self.handle, C.byref(D)), "tn_mps_get_max_d")
+        return D.value
+
+    def GetSite(self, site: int) -> np.ndarray:
+        """Site tensor as an array A[n, i1, i2]."""
+        D1, D2 = C.c_int(), C.c_int()
+        check(self._lib.tn_mps_get_site_dims(self.handle, site, C.byref(D1), C.byref(D2)), "dims")
+        buf = np.empty(self.d * D1.value * D2.value)
+        check(self._lib.tn_mps_get_site(self.handle, site, buf.ctypes.data), "tn_mps_get_site")
+        return np.transpose(buf.reshape(self.d, D2.value, D1.value), (0, 2, 1)).copy()
+
+    def SetSite(self, site: int, A: np.ndarray):
+        d, D1, D2 = A.shape
+        buf = np.ascontiguousarray(np.transpose(A, (0, 2, 1)), dtype=np.float64).ravel()
+        check(self._lib.tn_mps_set_site(self.handle, site, D1, D2, buf.ctypes.data), "tn_mps_set_site")
+
+    def GetBondSVs(self, bond: int) -> np.ndarray:
+        D = C.c_int()
+        check(self._lib.tn_mps_get_bond(self.handle, bond, C.byref(D), None), "tn_mps_get_bond")
+        s = np.empty(D.value)
+        check(self._lib.tn_mps_get_bond(self.handle, bond, C.byref(D), s.ctypes.data), "tn_mps_get_bond")
+        return s
+
+    def GetExpectation(self, H: Hamiltonian) -> float:
+        E = C.c_double()
+        check(self._lib.tn_mps_get_expectation(self.handle, H.handle, C.byref(E)), "tn_mps_get_expectation")
+        return E.value
+
+    def GetExpectationH2(self, H: Hamiltonian) -> float:
+        E = C.c_double()
+        check(self._lib.tn_mps_get_expectation_h2(self.handle, H.handle, C.byref(E)), "h2")
+        return E.value
+
+    def GetSiteEnergies(self) -> np.ndarray:
+        E = np.empty(self.L)
+        check(self._lib.tn_mps_get_site_energies(self.handle, E.ctypes.data), "site energies")
+        return E
+
+    def FindVariationalGroundState(self, H: Hamiltonian, schedule: IterationSchedule,
+                                   options: Optional[SolverOptions] = None) -> float:
+        """Returns <H^2>-<H>^2 (MPSImp_Variational.C:16-25); stats in self.last_stats."""
+        lines = (capi.SchedLine * len(schedule.lines))(*[ln.to_c() for ln in schedule.lines])
+        opt = (options or SolverOptions()).to_c()
+        st = capi.SweepStats()
+        var = C.c_double()
+        check(self._lib.tn_mps_find_variational_ground_state(self.handle, H.handle, lines, len(schedule.lines),
+                                                              C.byref(opt), C.byref(st), C.byref(var)),
+              "tn_mps_find_variational_ground_state")
+        self.last_stats = st.as_dict()
+        return var.value
+
+    def PrepareSweeps(self, H: Hamiltonian):
+        """Normalize(DRight) + LoadHeffCaches (MPSImp_Variational.C:18-19)."""
+        check(self._lib.tn_mps_prepare_sweeps(self.handle, H.handle), "tn_mps_prepare_sweeps")
+
+    def Sweep(self, H: Hamiltonian, nsweeps: int = 1, eps_eigen: float = 1e-10,
+              options: Optional[SolverOptions] = None) -> dict:
+        """nsweeps pairs of Sweep(DLeft)+Sweep(DRight) at the current D; returns the stats."""
+        opt = (options or SolverOptions()).to_c()
+        st = capi.SweepStats()
+        check(self._lib.tn_mps_sweep(self.handle, H.handle, int(nsweeps), float(eps_eigen), C.byref(opt),
+                                     C.byref(st)), "tn_mps_sweep")
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if getattr(self, "handle", None):
+                self._lib.tn_mps_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Solver interfaces (NumericalMethods/*.H) on the GPU
+# ---------------------------------------------------------------------------
+def _torch():
+    import torch
+    return torch
+
+
+def _dev(a: np.ndarray):
+    """Column-major device copy of a 2-D host array (torch tensor, returned with its shape)."""
+    torch = _torch()
+    a = np.asarray(a, dtype=np.float64)
+    return torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+
+
+def _host(t, rows, cols):
+    return t.cpu().numpy().reshape(cols, rows).T.copy()
+
+
+class CudaSVDSolver:
+    """SVDSolver<double> (SVDSolver.H:11-23): one-sided Jacobi on the GPU."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+
+    def SolveAll(self, A, eps: float = 1e-13):
+        m, n = np.shape(A)
+        return self.Solve(A, eps, min(m, n))
+
+    def Solve(self, A, eps: float, NumSingularValues: int):
+        torch = _torch()
+        m, n = np.shape(A)
+        k = min(m, n)
+        dA = _dev(A)
+        U = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        s = torch.empty(k, dtype=torch.float64, device="cuda")
+        Vt = torch.empty(k * n, dtype=torch.float64, device="cuda")
+        check(self.ctx._lib.tn_svd(self.ctx.handle, m, n, dA.data_ptr(), m, U.data_ptr(), m, s.data_ptr(),
+                                   Vt.data_ptr(), k), "tn_svd")
+        U, s, Vt = _host(U, m, k), s.cpu().numpy(), _host(Vt, k, n)
+        r = int(NumSingularValues)
+        return U[:, :r], s[:r], Vt[:r, :]
+
+
+class CudaQRSolver:
+    """QRSolver<double> (QRSolver.H:10-56): Householder on the GPU."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+
+    def SolveThinQR(self, A):
+        torch = _torch()
+        m, n = np.shape(A)
+        k = min(m, n)
+        dA = _dev(A)
+        Q = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        R = torch.empty(k * n, dtype=torch.float64, device="cuda")
+        check(self.ctx._lib.tn_qr(self.ctx.handle, m, n, dA.data_ptr(), m, Q.data_ptr(), m, R.data_ptr(), k),
+              "tn_qr")
+        return _host(Q, m, k), _host(R, k, n)
+
+    def SolveThinLQ(self, A):
+        torch = _torch()
+        m, n = np.shape(A)
+        k = min(m, n)
+        dA = _dev(A)
+        Lm = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        Q = torch.empty(k * n, dtype=torch.float64, device="cuda")
+        check(self.ctx._lib.tn_lq(self.ctx.handle, m, n, dA.data_ptr(), m, Lm.data_ptr(), m, Q.data_ptr(), k),
+              "tn_lq")
+        return _host(Lm, m, k), _host(Q, k, n)
+
+
+class CudaEigenSolver:
+    """EigenSolver<double>::Solve (EigenSolver.H:31): lowest eigenpairs of a dense symmetric matrix."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+
+    def Reset(self):
+        pass
+
+    def Solve(self, A, eps: float, NumEigenValues: int):
+        torch = _torch()
+        N = np.shape(A)[0]
+        k = int(NumEigenValues)
+        dA = _dev(A)
+        U = torch.empty(N * k, dtype=torch.float64, device="cuda")
+        w = np.empty(k)
+        check(self.ctx._lib.tn_eigensolve_dense(self.ctx.handle, N, dA.data_ptr(), N, k, max(eps, 1e-13),
+                                                w.ctypes.data, U.data_ptr(), N), "tn_eigensolve_dense")
+        return _host(U, N, k), w
+
+
+class SVCompressor:
+    """SVCompressor<double> (SVCompressor.H:10-24, SVCompressorImp.C:19-73)."""
+
+    def __init__(self, Dmax: int, eps: float, ctx: Optional[Context] = None):
+        self.Dmax, self.eps = int(Dmax), float(eps)
+        self.ctx = ctx or default_context()
+
+    def GetDmax(self):
+        return self.Dmax
+
+    def Donly(self):
+        return self.eps == 0.0
+
+    def Compress(self, U, s, Vt):
+        """Returns (U, s, Vt, discarded sum s^2) truncated as the reference does."""
+        torch = _torch()
+        ds = torch.from_numpy(np.ascontiguousarray(s, dtype=np.float64)).cuda()
+        D = C.c_int()
+        disc = C.c_double()
+        check(self.ctx._lib.tn_compress(self.ctx.handle, self.Dmax, self.eps, ds.numel(), ds.data_ptr(),
+                                        C.byref(D), C.byref(disc)), "tn_compress")
+        D = D.value
+        s2 = ds.cpu().numpy()[:D]
+        return np.asarray(U)[:, :D], s2, np.asarray(Vt)[:D, :], disc.value

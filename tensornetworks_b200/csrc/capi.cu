@@ -1,0 +1,600 @@
+// capi.cu -- the extern "C" boundary declared in include/tn_cuda.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <string>
+
+#include "engine.h"
+
+namespace tnb {
+
+static thread_local std::string g_last_error;
+static unsigned long long g_launches = 0;
+
+void count_launch() { __atomic_fetch_add(&g_launches, 1ULL, __ATOMIC_RELAXED); }
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+int DevBuf::ensure(size_t nbytes) {
+    if (nbytes <= bytes && p) return TN_OK;
+    release();
+    if (nbytes == 0) nbytes = 8;
+    cudaError_t e = cudaMalloc(&p, nbytes);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        set_error("cudaMalloc(%zu): %s", nbytes, cudaGetErrorString(e));
+        return TN_OUT_OF_MEMORY;
+    }
+    bytes = nbytes;
+    return TN_OK;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+int HostBuf::ensure(size_t nbytes) {
+    if (nbytes <= bytes && p) return TN_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMallocHost(&p, nbytes);
+    if (e != cudaSuccess) {
+        set_error("cudaMallocHost(%zu): %s", nbytes, cudaGetErrorString(e));
+        return TN_OUT_OF_MEMORY;
+    }
+    bytes = nbytes;
+    return TN_OK;
+}
+
+HostBuf::~HostBuf() {
+    if (p) cudaFreeHost(p);
+}
+
+}  // namespace tnb
+
+using namespace tnb;
+
+namespace {
+
+int upload_terms(Ctx& c, const double* W_host, int d, int Dw1, int Dw2, bool lr, const WTermDev** out, int* n) {
+    auto t = build_terms(W_host, d, Dw1, Dw2, lr);
+    TN_CHECK(c.wterms.ensure(sizeof(WTermDev) * t.size()));
+    TN_CUDA_CHECK(cudaMemcpyAsync(c.wterms.p, t.data(), sizeof(WTermDev) * t.size(), cudaMemcpyHostToDevice, c.stream));
+    // the host vector dies at return: wait for the copy
+    TN_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    *out = c.wterms.as<WTermDev>();
+    *n = (int)t.size();
+    return TN_OK;
+}
+
+bool valid_shape(int d, int Dw1, int Dw2, int D1, int D2) {
+    return d >= 1 && Dw1 >= 1 && Dw2 >= 1 && D1 >= 1 && D2 >= 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tn_status_string(int s) {
+    switch (s) {
+        case TN_OK: return "TN_OK";
+        case TN_NOT_CONVERGED: return "TN_NOT_CONVERGED";
+        case TN_BAD_SHAPE: return "TN_BAD_SHAPE";
+        case TN_NAN_DETECTED: return "TN_NAN_DETECTED";
+        case TN_CUDA_ERROR: return "TN_CUDA_ERROR";
+        case TN_BAD_ARG: return "TN_BAD_ARG";
+        case TN_NO_DEVICE: return "TN_NO_DEVICE";
+        case TN_OUT_OF_MEMORY: return "TN_OUT_OF_MEMORY";
+    }
+    return "TN_UNKNOWN";
+}
+
+const char* tn_last_error(void) { return tnb::g_last_error.c_str(); }
+
+int tn_ctx_create(int device, tn_ctx* out) {
+    if (!out) return TN_BAD_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+        set_error("no CUDA device %d", device);
+        return TN_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    TN_CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        set_error("device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+        return TN_NO_DEVICE;
+    }
+    TN_CUDA_CHECK(cudaSetDevice(device));
+    tn_ctx c = new tn_ctx_s();
+    c->c.device = device;
+    c->c.sm_count = prop.multiProcessorCount;
+    TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.own_stream, cudaStreamNonBlocking));
+    c->c.stream = c->c.own_stream;
+    TN_CUDA_CHECK(cudaEventCreate(&c->c.ev_a));
+    TN_CUDA_CHECK(cudaEventCreate(&c->c.ev_b));
+    *out = c;
+    return TN_OK;
+}
+
+int tn_ctx_destroy(tn_ctx c) {
+    if (!c) return TN_BAD_ARG;
+    cudaSetDevice(c->c.device);
+    cudaStreamSynchronize(c->c.stream);
+    if (c->c.ev_a) cudaEventDestroy(c->c.ev_a);
+    if (c->c.ev_b) cudaEventDestroy(c->c.ev_b);
+    if (c->c.own_stream) cudaStreamDestroy(c->c.own_stream);
+    delete c;
+    return TN_OK;
+}
+
+int tn_ctx_set_stream(tn_ctx c, void* stream) {
+    if (!c) return TN_BAD_ARG;
+    c->c.stream = stream ? (cudaStream_t)stream : c->c.own_stream;
+    return TN_OK;
+}
+
+int tn_ctx_synchronize(tn_ctx c) {
+    if (!c) return TN_BAD_ARG;
+    TN_CUDA_CHECK(cudaStreamSynchronize(c->c.stream));
+    return TN_OK;
+}
+
+// ---- Hamiltonian ---------------------------------------------------------------
+int tn_hamiltonian_create_heisenberg(tn_ctx c, int L, double S, int form, double Jxy, double Jz, double hz,
+                                     tn_hamiltonian* out) {
+    if (!c || !out) return TN_BAD_ARG;
+    *out = nullptr;
+    double twoS = 2.0 * S;
+    if (L < 2 || S <= 0 || std::fabs(twoS - std::round(twoS)) > 1e-12) {
+        set_error("bad L=%d or S=%g", L, S);
+        return TN_BAD_ARG;
+    }
+    if (form != TN_FORM_REGULAR_LOWER && form != TN_FORM_REGULAR_UPPER) {
+        set_error("unsupported MPO form %d", form);
+        return TN_BAD_ARG;
+    }
+    if (std::fabs(Jxy) + std::fabs(Jz) <= 0.0) {  // Hamiltonian_1D_NN_Heisenberg.C:18
+        set_error("Jxy and Jz both zero");
+        return TN_BAD_ARG;
+    }
+    TN_CUDA_CHECK(cudaSetDevice(c->c.device));
+    tn_hamiltonian h = new tn_hamiltonian_s();
+    h->h.ctx = &c->c;
+    h->h.L = L;
+    h->h.S = S;
+    h->h.d = (int)std::lround(twoS + 1.0);
+    h->h.form = form;
+    h->h.Jxy = Jxy;
+    h->h.Jz = Jz;
+    h->h.hz = hz;
+    int s = h->h.build();
+    if (s != TN_OK) {
+        delete h;
+        return s;
+    }
+    *out = h;
+    return TN_OK;
+}
+
+int tn_hamiltonian_destroy(tn_hamiltonian h) {
+    if (!h) return TN_BAD_ARG;
+    delete h;
+    return TN_OK;
+}
+
+int tn_hamiltonian_site_dims(tn_hamiltonian h, int site, int* Dw1, int* Dw2, int* d) {
+    if (!h || site < 1 || site > h->h.L) return TN_BAD_ARG;
+    if (Dw1) *Dw1 = h->h.ops[site].Dw1;
+    if (Dw2) *Dw2 = h->h.ops[site].Dw2;
+    if (d) *d = h->h.d;
+    return TN_OK;
+}
+
+int tn_hamiltonian_get_w(tn_hamiltonian h, int site, double* W) {
+    if (!h || !W || site < 1 || site > h->h.L) return TN_BAD_ARG;
+    const auto& w = h->h.ops[site].W;
+    std::memcpy(W, w.data(), sizeof(double) * w.size());
+    return TN_OK;
+}
+
+// ---- MPS --------------------------------------------------------------------------
+int tn_mps_create(tn_hamiltonian h, int D, double normEps, double epsSV, tn_mps* out) {
+    if (!h || !out || D < 1) return TN_BAD_ARG;
+    *out = nullptr;
+    TN_CUDA_CHECK(cudaSetDevice(h->h.ctx->device));
+    tn_mps m = new tn_mps_s();
+    m->m.normEps = normEps;
+    m->m.epsSV = epsSV;
+    int s = m->m.init(&h->h, D);
+    if (s != TN_OK) {
+        delete m;
+        return s;
+    }
+    *out = m;
+    return TN_OK;
+}
+
+int tn_mps_destroy(tn_mps m) {
+    if (!m) return TN_BAD_ARG;
+    cudaStreamSynchronize(m->m.ctx->stream);
+    delete m;
+    return TN_OK;
+}
+
+int tn_mps_initialize_random(tn_mps m, uint64_t seed) {
+    if (!m) return TN_BAD_ARG;
+    return m->m.initialize_random(seed);
+}
+
+int tn_mps_get_site_dims(tn_mps m, int site, int* D1, int* D2) {
+    if (!m || site < 1 || site > m->m.L) return TN_BAD_ARG;
+    if (D1) *D1 = m->m.D1[site];
+    if (D2) *D2 = m->m.D2[site];
+    return TN_OK;
+}
+
+int tn_mps_get_site(tn_mps m, int site, double* A) {
+    if (!m || !A || site < 1 || site > m->m.L) return TN_BAD_ARG;
+    auto& s = m->m;
+    TN_CUDA_CHECK(cudaStreamSynchronize(s.ctx->stream));
+    TN_CUDA_CHECK(cudaMemcpy(A, s.A[site]->p, sizeof(double) * (size_t)s.d * s.D1[site] * s.D2[site],
+                             cudaMemcpyDeviceToHost));
+    return TN_OK;
+}
+
+int tn_mps_set_site(tn_mps m, int site, int D1, int D2, const double* A) {
+    if (!m || !A || site < 1 || site > m->m.L || D1 < 1 || D2 < 1) return TN_BAD_ARG;
+    auto& s = m->m;
+    TN_CHECK(s.ensure_capacity(std::max(D1, D2)));
+    TN_CUDA_CHECK(cudaStreamSynchronize(s.ctx->stream));
+    TN_CUDA_CHECK(cudaMemcpy(s.A[site]->p, A, sizeof(double) * (size_t)s.d * D1 * D2, cudaMemcpyHostToDevice));
+    s.D1[site] = D1;
+    s.D2[site] = D2;
+    return TN_OK;
+}
+
+int tn_mps_get_bond(tn_mps m, int bond, int* D, double* s_host) {
+    if (!m || bond < 1 || bond >= m->m.L) return TN_BAD_ARG;
+    const auto& s = m->m.bond_s[bond];
+    if (D) *D = (int)s.size();
+    if (s_host) std::memcpy(s_host, s.data(), sizeof(double) * s.size());
+    return TN_OK;
+}
+
+int tn_mps_normalize(tn_mps m, int direction) {
+    if (!m) return TN_BAD_ARG;
+    TN_CHECK(m->m.normalize_all(direction == TN_DLEFT));
+    TN_CUDA_CHECK(cudaStreamSynchronize(m->m.ctx->stream));
+    return TN_OK;
+}
+
+int tn_mps_get_max_d(tn_mps m, int* D) {
+    if (!m || !D) return TN_BAD_ARG;
+    *D = m->m.max_D();
+    return TN_OK;
+}
+
+int tn_mps_get_expectation(tn_mps m, tn_hamiltonian h, double* E) {
+    if (!m || !h || !E || h->h.L != m->m.L) return TN_BAD_ARG;
+    return m->m.expectation(h->h.ops, E);
+}
+
+int tn_mps_get_expectation_h2(tn_mps m, tn_hamiltonian h, double* E2) {
+    if (!m || !h || !E2 || h->h.L != m->m.L) return TN_BAD_ARG;
+    return m->m.expectation(h->h.ops2, E2);
+}
+
+int tn_mps_find_variational_ground_state(tn_mps m, tn_hamiltonian h, const tn_sched_line* lines, int nlines,
+                                         const tn_solver_options* opt, tn_sweep_stats* stats, double* variance) {
+    if (!m || !h || !lines || nlines < 1 || h->h.L != m->m.L) return TN_BAD_ARG;
+    for (int i = 0; i < nlines; ++i)
+        if (lines[i].max_sweeps < 1 || lines[i].Dmax < 1) {
+            set_error("schedule line %d invalid", i);
+            return TN_BAD_ARG;
+        }
+    if (opt && opt->precision != TN_PREC_FP64 && opt->precision != TN_PREC_MIXED) return TN_BAD_ARG;
+    m->m.H = &h->h;
+    tn_sweep_stats st{};
+    TN_CHECK(m->m.find_ground_state(lines, nlines, opt, &st));
+    if (stats) *stats = st;
+    if (variance) *variance = st.variance;
+    return TN_OK;
+}
+
+int tn_mps_sweep(tn_mps m, tn_hamiltonian h, int nsweeps, double eps_eigen, const tn_solver_options* opt,
+                 tn_sweep_stats* stats) {
+    if (!m || !h || nsweeps < 1 || h->h.L != m->m.L) return TN_BAD_ARG;
+    m->m.H = &h->h;
+    return m->m.sweep_pairs(nsweeps, eps_eigen, opt, stats);
+}
+
+int tn_mps_prepare_sweeps(tn_mps m, tn_hamiltonian h) {
+    if (!m || !h || h->h.L != m->m.L) return TN_BAD_ARG;
+    m->m.H = &h->h;
+    return m->m.prepare_sweeps();
+}
+
+unsigned long long tn_launch_count(void) { return __atomic_load_n(&tnb::g_launches, __ATOMIC_RELAXED); }
+
+int tn_mps_get_site_energies(tn_mps m, double* E) {
+    if (!m || !E) return TN_BAD_ARG;
+    for (int ia = 1; ia <= m->m.L; ++ia) E[ia - 1] = m->m.Emin[ia];
+    return TN_OK;
+}
+
+// ---- solver interfaces -----------------------------------------------------------
+int tn_heff_matvec(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
+                   const double* F, const double* G, const double* x, double* y) {
+    if (!c || !W_host || !F || !G || !x || !y) return TN_BAD_ARG;
+    if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
+    if (precision != TN_PREC_FP64) {
+        set_error("precision %d not available for this entry point", precision);
+        return TN_BAD_ARG;
+    }
+    Ctx& cx = c->c;
+    const WTermDev* t;
+    int nt;
+    TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, true, &t, &nt));
+    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    TN_CHECK(cx.P.ensure(scr));
+    TN_CHECK(cx.Q.ensure(scr));
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    TN_CHECK(heff_matvec_f64(s, t, nt, F, G, x, y, cx.P.as<double>(), cx.Q.as<double>(), nullptr, cx.stream));
+    return TN_OK;
+}
+
+int tn_heff_diag(tn_ctx c, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host, const double* F,
+                 const double* G, double* diag) {
+    if (!c || !W_host || !F || !G || !diag) return TN_BAD_ARG;
+    if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
+    Ctx& cx = c->c;
+    size_t nw = (size_t)Dw1 * Dw2 * d * d;
+    TN_CHECK(cx.misc.ensure(sizeof(double) * nw));
+    TN_CUDA_CHECK(cudaMemcpyAsync(cx.misc.p, W_host, sizeof(double) * nw, cudaMemcpyHostToDevice, cx.stream));
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    TN_CHECK(heff_diag(s, cx.misc.as<double>(), F, G, diag, cx.stream));
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return TN_OK;
+}
+
+int tn_env_left(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
+                const double* A, const double* F, double* Fout) {
+    if (!c || !W_host || !A || !F || !Fout) return TN_BAD_ARG;
+    if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
+    if (precision != TN_PREC_FP64) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    const WTermDev* t;
+    int nt;
+    TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, true, &t, &nt));
+    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    TN_CHECK(cx.P.ensure(scr));
+    TN_CHECK(cx.Q.ensure(scr));
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    return env_left_f64(s, t, nt, A, F, Fout, cx.P.as<double>(), cx.Q.as<double>(), cx.stream);
+}
+
+int tn_env_right(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
+                 const double* A, const double* G, double* Gout) {
+    if (!c || !W_host || !A || !G || !Gout) return TN_BAD_ARG;
+    if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
+    if (precision != TN_PREC_FP64) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    const WTermDev* t;
+    int nt;
+    TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, false, &t, &nt));
+    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    TN_CHECK(cx.P.ensure(scr));
+    TN_CHECK(cx.Q.ensure(scr));
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    return env_right_f64(s, t, nt, A, G, Gout, cx.P.as<double>(), cx.Q.as<double>(), cx.stream);
+}
+
+int tn_eigensolve_heff(tn_ctx c, const tn_solver_options* opt, int d, int Dw1, int Dw2, int D1, int D2,
+                       const double* W_host, const double* F, const double* G, double* x, double tol,
+                       double* theta, double* residual, int* matvecs) {
+    if (!c || !W_host || !F || !G || !x) return TN_BAD_ARG;
+    if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
+    Ctx& cx = c->c;
+    int krylov = (opt && opt->krylov > 0) ? opt->krylov : 20;
+    int restarts = (opt && opt->max_restarts > 0) ? opt->max_restarts : 10;
+    const WTermDev* t;
+    int nt;
+    TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, true, &t, &nt));
+    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    TN_CHECK(cx.P.ensure(scr));
+    TN_CHECK(cx.Q.ensure(scr));
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    double* P = cx.P.as<double>();
+    double* Q = cx.Q.as<double>();
+    MatvecFn mv = [&](const double* xi, double* yo, const int* skip) {
+        return heff_matvec_f64(s, t, nt, F, G, xi, yo, P, Q, skip, cx.stream);
+    };
+    LzResult r{};
+    TN_CHECK(lanczos_solve(cx, (long long)d * D1 * D2, x, krylov, restarts, tol, mv, &r));
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    if (theta) *theta = r.theta;
+    if (residual) *residual = r.resid;
+    if (matvecs) *matvecs = r.matvecs;
+    return r.converged ? TN_OK : TN_NOT_CONVERGED;
+}
+
+int tn_eigensolve_dense(tn_ctx c, int N, const double* A, int lda, int k, double tol, double* w_host, double* U,
+                        int ldu) {
+    if (!c || !A || !w_host || !U || N < 1 || k < 1 || k > N || lda < N || ldu < N) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    // Lowest k pairs by Lanczos with shift deflation: A' = A + sigma sum_i u_i u_i^T.
+    // sigma above the spectral radius bound (max row sum).
+    std::vector<double> hA((size_t)lda * N);
+    TN_CUDA_CHECK(cudaMemcpy(hA.data(), A, sizeof(double) * hA.size(), cudaMemcpyDeviceToHost));
+    double rad = 0;
+    for (int i = 0; i < N; ++i) {
+        double r = 0;
+        for (int j = 0; j < N; ++j) r += std::fabs(hA[(size_t)j * lda + i]);
+        rad = std::max(rad, r);
+    }
+    const double sigma = 2.0 * rad + 1.0;
+    DevBuf tmpv;
+    TN_CHECK(tmpv.ensure(sizeof(double) * (size_t)(k + 1)));
+    for (int e = 0; e < k; ++e) {
+        double* u = U + (size_t)e * ldu;
+        TN_CHECK(fill(u, N, 1.0, cx.stream));
+        MatvecFn mv = [&](const double* xi, double* yo, const int* skip) -> int {
+            GemmArgs g;
+            g.M = N; g.N = 1; g.K = N;
+            g.A.ptr = A; g.A.mn = idx(1); g.A.k = idx(lda);
+            g.B.ptr = xi; g.B.k = idx(1); g.B.mn = idx(N);
+            g.C.ptr = yo; g.C.m = idx(1); g.C.n = idx(N);
+            g.skip = skip;
+            TN_CHECK(gemm_f64(g, cx.stream));
+            if (e > 0) {
+                // c = U_e^T x ; y += sigma U_e c
+                GemmArgs h;
+                h.M = e; h.N = 1; h.K = N;
+                h.A.ptr = U; h.A.mn = idx(ldu); h.A.k = idx(1);
+                h.B.ptr = xi; h.B.k = idx(1); h.B.mn = idx(N);
+                h.C.ptr = tmpv.as<double>(); h.C.m = idx(1); h.C.n = idx(e);
+                h.skip = skip;
+                TN_CHECK(gemm_f64(h, cx.stream));
+                GemmArgs q;
+                q.M = N; q.N = 1; q.K = e; q.alpha = sigma; q.beta = 1.0;
+                q.A.ptr = U; q.A.mn = idx(1); q.A.k = idx(ldu);
+                q.B.ptr = tmpv.as<double>(); q.B.k = idx(1); q.B.mn = idx(e);
+                q.C.ptr = yo; q.C.m = idx(1); q.C.n = idx(N);
+                q.skip = skip;
+                TN_CHECK(gemm_f64(q, cx.stream));
+            }
+            return (int)TN_OK;
+        };
+        LzResult r{};
+        TN_CHECK(lanczos_solve(cx, N, u, std::min(N, 40), 50, tol, mv, &r));
+        w_host[e] = r.theta;
+    }
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return TN_OK;
+}
+
+static int svd_common(tn_ctx c, int m, int n, const double* A, int lda, double* U, int ldu, double* s, double* Vt,
+                      int ldvt, bool vectors) {
+    if (!c || !A || !s || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    if (vectors && (!U || !Vt || ldu < m || ldvt < std::min(m, n))) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    const bool tall = m >= n;
+    const int tm = tall ? m : n, tn = tall ? n : m;
+    size_t need = (size_t)tm * tn + (size_t)tn * tn + (tall ? 0 : (size_t)tm * tn + (size_t)tn * tn);
+    TN_CHECK(cx.svdw.ensure(sizeof(double) * need + sizeof(SvdJob) * 2));
+    // svd_batched uploads its job array into cx.svdw: keep the matrices elsewhere
+    DevBuf work;
+    TN_CHECK(work.ensure(sizeof(double) * need));
+    double* Wm = work.as<double>();
+    double* V = Wm + (size_t)tm * tn;
+    double* Ut = V + (size_t)tn * tn;          // wide case: U of A^T (tm x tn)
+    double* Vtt = Ut + (size_t)tm * tn;        // wide case: Vt of A^T (tn x tn)
+    if (tall) TN_CHECK(copy2d(m, n, A, idx(1), idx(lda), Wm, idx(1), idx(m), 1.0, cx.stream));
+    else TN_CHECK(copy2d(m, n, A, idx(1), idx(lda), Wm, idx(n), idx(1), 1.0, cx.stream));
+    SvdJob j{};
+    j.W = Wm; j.m = tm; j.n = tn; j.V = V; j.s = s;
+    if (vectors) {
+        if (tall) { j.U = U; j.ldu = ldu; j.Vt = Vt; j.ldvt = ldvt; }
+        else { j.U = Ut; j.ldu = tm; j.Vt = Vtt; j.ldvt = tn; }
+    }
+    std::vector<SvdJob> jobs{j};
+    TN_CHECK(svd_batched(cx, jobs, vectors));
+    if (vectors && !tall) {
+        // A^T = U' s V'^T  ->  A = V' s U'^T :  U = V' = Vtt^T (m x m), Vt = U'^T (m x n)
+        TN_CHECK(copy2d(tn, tn, Vtt, idx(tn), idx(1), U, idx(1), idx(ldu), 1.0, cx.stream));
+        TN_CHECK(copy2d(tn, tm, Ut, idx(tm), idx(1), Vt, idx(1), idx(ldvt), 1.0, cx.stream));
+    }
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return TN_OK;
+}
+
+int tn_svd(tn_ctx c, int m, int n, const double* A, int lda, double* U, int ldu, double* s, double* Vt, int ldvt) {
+    return svd_common(c, m, n, A, lda, U, ldu, s, Vt, ldvt, true);
+}
+
+int tn_svd_values(tn_ctx c, int m, int n, const double* A, int lda, double* s) {
+    return svd_common(c, m, n, A, lda, nullptr, 0, s, nullptr, 0, false);
+}
+
+int tn_qr(tn_ctx c, int m, int n, const double* A, int lda, double* Q, int ldq, double* R, int ldr) {
+    if (!c || !A || !Q || !R || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    const int k = std::min(m, n);
+    if (ldq < m || ldr < k) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    DevBuf W;
+    TN_CHECK(W.ensure(sizeof(double) * (size_t)m * n));
+    TN_CHECK(copy2d(m, n, A, idx(1), idx(lda), W.as<double>(), idx(1), idx(m), 1.0, cx.stream));
+    TN_CHECK(qr_dense(cx, m, n, W.as<double>(), Q, ldq, R, ldr));
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return TN_OK;
+}
+
+int tn_lq(tn_ctx c, int m, int n, const double* A, int lda, double* L, int ldl, double* Q, int ldq) {
+    if (!c || !A || !Q || !L || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    const int k = std::min(m, n);
+    if (ldl < m || ldq < k) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    DevBuf W, Qt, Rt;
+    TN_CHECK(W.ensure(sizeof(double) * (size_t)m * n));
+    TN_CHECK(Qt.ensure(sizeof(double) * (size_t)n * k));
+    TN_CHECK(Rt.ensure(sizeof(double) * (size_t)k * m));
+    // A^T (n x m) = Qt Rt  ->  A = Rt^T Qt^T
+    TN_CHECK(copy2d(m, n, A, idx(1), idx(lda), W.as<double>(), idx(n), idx(1), 1.0, cx.stream));
+    TN_CHECK(qr_dense(cx, n, m, W.as<double>(), Qt.as<double>(), n, Rt.as<double>(), k));
+    TN_CHECK(copy2d(k, m, Rt.as<double>(), idx(1), idx(k), L, idx(ldl), idx(1), 1.0, cx.stream));
+    TN_CHECK(copy2d(n, k, Qt.as<double>(), idx(1), idx(n), Q, idx(ldq), idx(1), 1.0, cx.stream));
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return TN_OK;
+}
+
+// SVCompressorImp<T>::Compress (SVCompressorImp.C:19-73) on a device s vector.
+int tn_compress(tn_ctx c, int Dmax, double eps, int k, double* s, int* D_out, double* discarded) {
+    if (!c || !s || k < 1 || !D_out) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    std::vector<double> h(k);
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    TN_CUDA_CHECK(cudaMemcpy(h.data(), s, sizeof(double) * k, cudaMemcpyDeviceToHost));
+    int N = k, D = N;
+    double integ = 0.0;
+    if (eps == 0.0) {
+        if (Dmax < 1) return TN_BAD_ARG;
+        D = std::min(Dmax, N);
+        for (int id = D; id < N; ++id) integ += h[id] * h[id];
+    } else {
+        for (; D >= 1; --D) {
+            double s2 = h[D - 1] * h[D - 1];
+            if (integ + s2 >= eps) break;
+            integ += s2;
+        }
+        if (Dmax > 0 && D > Dmax) {
+            // capped at Dmax; the discarded weight is still the eps-scan sum (as the reference)
+            D = Dmax;
+        }
+    }
+    if (D < N) {
+        double before = 0, after = 0;
+        for (int i = 0; i < N; ++i) before += h[i] * h[i];
+        for (int i = 0; i < D; ++i) after += h[i] * h[i];
+        double rescale = after > 0 ? before / after : 1.0;
+        for (int i = 0; i < D; ++i) h[i] *= rescale;
+        TN_CUDA_CHECK(cudaMemcpy(s, h.data(), sizeof(double) * D, cudaMemcpyHostToDevice));
+    }
+    *D_out = std::max(D, 0);
+    if (discarded) *discarded = integ;
+    return TN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,693 @@
+// engine.cu -- the variational ground-state sweep on one GPU.
+//
+// Host C++ drives device kernels; all tensors (sites, environments, Krylov
+// bases, QR factors) stay resident in HBM.  The control flow restates
+// MPSImp::FindVariationalGroundState and its helpers
+// (TensorNetworksImp/MPS/MPSImp_Variational.C:16-173, MPSImp.C:69-147,
+// MPSSite_Normalization.C:20-107, Bond.C:60-168).  Differences from the
+// reference, all value-preserving:
+//   * the gauge move of each site is a Householder QR (LQ when sweeping
+//     right-to-left) and the bond singular values are the singular values of
+//     the triangular factor, computed for all bonds of a half-sweep in one
+//     batched Jacobi launch.  The single-site problem is invariant under the
+//     orthogonal change of bond basis that separates this from the
+//     reference's SVD gauge, so energies and singular values are the same;
+//   * only the environment the next site needs is rebuilt
+//     (MPSSite::UpdateCache builds both; the other is never read);
+//   * the eigensolver is matrix-free (Lanczos/Davidson) instead of a dense
+//     zheevx on the materialised Heff.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+
+#include "engine.h"
+
+namespace tnb {
+
+// ---------------------------------------------------------------------------
+// Model: spin operators and the Heisenberg/XXZ MPO
+// (SpinCalculator.C:20-70, Hamiltonian_1D_NN_Heisenberg.C:35-79,
+//  SiteOperatorImp.C:33-51,109-134)
+// ---------------------------------------------------------------------------
+namespace {
+
+double spin_of(int n, double S) { return n - S; }
+double op_val(int which, int m, int n, double S) {
+    switch (which) {
+        case 0: return m == n ? 1.0 : 0.0;
+        case 1: return (m == n + 1) ? std::sqrt(S * (S + 1.0) - spin_of(m, S) * spin_of(n, S)) : 0.0;
+        case 2: return (m + 1 == n) ? std::sqrt(S * (S + 1.0) - spin_of(m, S) * spin_of(n, S)) : 0.0;
+        case 3: return m == n ? spin_of(m, S) : 0.0;
+    }
+    return 0.0;
+}
+
+std::vector<double> bulk_w(double S, int d, int form, double Jxy, double Jz, double hz) {
+    const int Dw = 5;
+    std::vector<double> W((size_t)Dw * Dw * d * d, 0.0);
+    auto set = [&](int w1, int w2, int which, double f) {
+        for (int m = 0; m < d; ++m)
+            for (int n = 0; n < d; ++n) W[(((size_t)w1 * Dw + w2) * d + m) * d + n] = f * op_val(which, m, n, S);
+    };
+    if (form == TN_FORM_REGULAR_LOWER) {
+        set(0, 0, 0, 1.0); set(1, 0, 1, 1.0); set(2, 0, 2, 1.0); set(3, 0, 3, 1.0);
+        set(4, 0, 3, hz); set(4, 1, 2, Jxy / 2.0); set(4, 2, 1, Jxy / 2.0); set(4, 3, 3, Jz); set(4, 4, 0, 1.0);
+    } else {
+        set(0, 0, 0, 1.0); set(0, 1, 1, 1.0); set(0, 2, 2, 1.0); set(0, 3, 3, 1.0);
+        set(0, 4, 3, hz); set(1, 4, 2, Jxy / 2.0); set(2, 4, 1, Jxy / 2.0); set(3, 4, 3, Jz); set(4, 4, 0, 1.0);
+    }
+    return W;
+}
+
+SiteMPO site_mpo(int L, double S, int d, int form, double Jxy, double Jz, double hz, int site) {
+    const int Dw = 5;
+    std::vector<double> Wb = bulk_w(S, d, form, Jxy, Jz, hz);
+    SiteMPO op;
+    const int rowKeep = form == TN_FORM_REGULAR_LOWER ? Dw - 1 : 0;
+    const int colKeep = form == TN_FORM_REGULAR_LOWER ? 0 : Dw - 1;
+    const bool left = site == 1, right = site == L;
+    op.Dw1 = left ? 1 : Dw;
+    op.Dw2 = right ? 1 : Dw;
+    op.W.assign((size_t)op.Dw1 * op.Dw2 * d * d, 0.0);
+    for (int a = 0; a < op.Dw1; ++a)
+        for (int b = 0; b < op.Dw2; ++b) {
+            int w1 = left ? rowKeep : a, w2 = right ? colKeep : b;
+            for (int m = 0; m < d; ++m)
+                for (int n = 0; n < d; ++n)
+                    op.W[(((size_t)a * op.Dw2 + b) * d + m) * d + n] = Wb[(((size_t)w1 * Dw + w2) * d + m) * d + n];
+        }
+    return op;
+}
+
+// (W*W)[(w1,v1),(w2,v2)](m,n) = sum_k W[w1,w2](m,k) W[v1,v2](k,n)  (MPO::Product, MPO.C:73-79)
+SiteMPO product_mpo(const SiteMPO& A, const SiteMPO& B, int d) {
+    SiteMPO P;
+    P.Dw1 = A.Dw1 * B.Dw1;
+    P.Dw2 = A.Dw2 * B.Dw2;
+    P.W.assign((size_t)P.Dw1 * P.Dw2 * d * d, 0.0);
+    auto at = [&](const SiteMPO& X, int w1, int w2, int m, int n) {
+        return X.W[(((size_t)w1 * X.Dw2 + w2) * d + m) * d + n];
+    };
+    for (int w1 = 0; w1 < A.Dw1; ++w1)
+        for (int v1 = 0; v1 < B.Dw1; ++v1)
+            for (int w2 = 0; w2 < A.Dw2; ++w2)
+                for (int v2 = 0; v2 < B.Dw2; ++v2)
+                    for (int m = 0; m < d; ++m)
+                        for (int n = 0; n < d; ++n) {
+                            double s = 0;
+                            for (int k = 0; k < d; ++k) s += at(A, w1, w2, m, k) * at(B, v1, v2, k, n);
+                            P.W[(((size_t)(w1 * B.Dw1 + v1) * P.Dw2 + (w2 * B.Dw2 + v2)) * d + m) * d + n] = s;
+                        }
+    return P;
+}
+
+__global__ void resize_kernel(const double* __restrict__ src, int d, int D1, int D2, double* __restrict__ dst,
+                              int nD1, int nD2) {
+    long long total = (long long)d * nD1 * nD2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        int i1 = (int)(e % nD1);
+        int i2 = (int)((e / nD1) % nD2);
+        int n = (int)(e / ((long long)nD1 * nD2));
+        dst[e] = (i1 < D1 && i2 < D2) ? src[(long long)n * D1 * D2 + (long long)i2 * D1 + i1] : 0.0;
+    }
+}
+
+__global__ void sumsq_kernel(const double* __restrict__ x, long long n, double* out) {
+    __shared__ double sh[32];
+    double s = 0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) s = fma(x[i], x[i], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        *out = t;
+    }
+}
+
+__global__ void scale_by_norm_kernel(double* x, long long n, const double* sumsq) {
+    double nr = sqrt(*sumsq);
+    if (!(nr > 0)) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] /= nr;
+}
+
+inline int g1d(long long n) {
+    long long b = (n + 255) / 256;
+    return (int)std::max<long long>(1, std::min<long long>(b, 148 * 8));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Hamiltonian
+// ---------------------------------------------------------------------------
+int Hamiltonian::build() {
+    ops.assign(L + 1, SiteMPO());
+    ops2.assign(L + 1, SiteMPO());
+    for (int ia = 1; ia <= L; ++ia) {
+        ops[ia] = site_mpo(L, S, d, form, Jxy, Jz, hz, ia);
+        ops2[ia] = product_mpo(ops[ia], ops[ia], d);
+    }
+    std::vector<WTermDev> all;
+    std::vector<double> allW;
+    auto add = [&](SiteMPO& op) {
+        auto lr = build_terms(op.W.data(), d, op.Dw1, op.Dw2, true);
+        auto rl = build_terms(op.W.data(), d, op.Dw1, op.Dw2, false);
+        op.offLR = all.size(); op.nLR = (int)lr.size();
+        all.insert(all.end(), lr.begin(), lr.end());
+        op.offRL = all.size(); op.nRL = (int)rl.size();
+        all.insert(all.end(), rl.begin(), rl.end());
+        op.offW = allW.size();
+        allW.insert(allW.end(), op.W.begin(), op.W.end());
+    };
+    for (int ia = 1; ia <= L; ++ia) add(ops[ia]);
+    for (int ia = 1; ia <= L; ++ia) add(ops2[ia]);
+    TN_CHECK(terms.ensure(sizeof(WTermDev) * all.size()));
+    TN_CUDA_CHECK(cudaMemcpy(terms.p, all.data(), sizeof(WTermDev) * all.size(), cudaMemcpyHostToDevice));
+    TN_CHECK(Wdev.ensure(sizeof(double) * allW.size()));
+    TN_CUDA_CHECK(cudaMemcpy(Wdev.p, allW.data(), sizeof(double) * allW.size(), cudaMemcpyHostToDevice));
+    return TN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MPS
+// ---------------------------------------------------------------------------
+MPSState::~MPSState() {
+    for (auto p : A) delete p;
+    for (auto p : Lenv) delete p;
+    for (auto p : Renv) delete p;
+    for (auto p : bondR) delete p;
+}
+
+// MPSImp::InitSitesAndBonds (MPSImp.C:69-90); Bond ctor fills s = 1/D (Bond.C:11-25).
+int MPSState::init(Hamiltonian* h, int D) {
+    H = h;
+    ctx = h->ctx;
+    L = h->L;
+    d = h->d;
+    D1.assign(L + 2, 1);
+    D2.assign(L + 2, 1);
+    for (int ia = 1; ia <= L; ++ia) {
+        D1[ia] = ia == 1 ? 1 : D;
+        D2[ia] = ia == L ? 1 : D;
+    }
+    A.assign(L + 2, nullptr);
+    Lenv.assign(L + 2, nullptr);
+    Renv.assign(L + 2, nullptr);
+    bondR.assign(L + 1, nullptr);
+    for (int i = 0; i <= L + 1; ++i) {
+        A[i] = new DevBuf();
+        Lenv[i] = new DevBuf();
+        Renv[i] = new DevBuf();
+        if (i <= L) bondR[i] = new DevBuf();
+    }
+    LenvDw.assign(L + 2, 1); LenvD.assign(L + 2, 1);
+    RenvDw.assign(L + 2, 1); RenvD.assign(L + 2, 1);
+    bond_s.assign(L + 1, std::vector<double>());
+    bond_maxDelta.assign(L + 1, 0.0);
+    bondRm.assign(L + 1, 0); bondRn.assign(L + 1, 0);
+    bondK.assign(L + 1, D);
+    bondDirty.assign(L + 1, 0);
+    for (int b = 1; b < L; ++b) bond_s[b].assign(D, 1.0 / D);
+    Emin.assign(L + 1, 0.0);
+    iterDE.assign(L + 1, 1.0);
+    gapE.assign(L + 1, 0.0);
+    TN_CHECK(ensure_capacity(D));
+    // boundary environments (1x1x1 = 1)
+    double one = 1.0;
+    TN_CHECK(Lenv[0]->ensure(sizeof(double)));
+    TN_CHECK(Renv[L + 1]->ensure(sizeof(double)));
+    TN_CUDA_CHECK(cudaMemcpy(Lenv[0]->p, &one, sizeof(double), cudaMemcpyHostToDevice));
+    TN_CUDA_CHECK(cudaMemcpy(Renv[L + 1]->p, &one, sizeof(double), cudaMemcpyHostToDevice));
+    // zero site tensors
+    for (int ia = 1; ia <= L; ++ia)
+        TN_CUDA_CHECK(cudaMemset(A[ia]->p, 0, sizeof(double) * (size_t)d * D1[ia] * D2[ia]));
+    return TN_OK;
+}
+
+int MPSState::ensure_capacity(int D) {
+    size_t site = sizeof(double) * (size_t)d * D * D;
+    for (int ia = 1; ia <= L; ++ia) {
+        if (A[ia]->bytes < site) {
+            // grow preserving contents
+            DevBuf nb;
+            TN_CHECK(nb.ensure(site));
+            if (A[ia]->p) TN_CUDA_CHECK(cudaMemcpy(nb.p, A[ia]->p, A[ia]->bytes, cudaMemcpyDeviceToDevice));
+            std::swap(A[ia]->p, nb.p);
+            std::swap(A[ia]->bytes, nb.bytes);
+        }
+    }
+    return TN_OK;
+}
+
+// MPSSite::InitializeWith(Random) (MPSSite.C:119-127) with mt19937_64(seed),
+// uniform(-1,1) on the 53-bit grid, sites in order, per-n column-major.
+int MPSState::initialize_random(unsigned long long seed) {
+    std::mt19937_64 g(seed);
+    for (int ia = 1; ia <= L; ++ia) {
+        size_t cnt = (size_t)d * D1[ia] * D2[ia];
+        std::vector<double> h(cnt);
+        double sc = 1.0 / std::sqrt((double)cnt);
+        for (size_t i = 0; i < cnt; ++i) {
+            unsigned long long x = g();
+            double u = (double)(x >> 11) * (1.0 / 9007199254740992.0);
+            h[i] = (2.0 * u - 1.0) * sc;
+        }
+        TN_CUDA_CHECK(cudaMemcpy(A[ia]->p, h.data(), sizeof(double) * cnt, cudaMemcpyHostToDevice));
+    }
+    return TN_OK;
+}
+
+int MPSState::max_D() const {
+    int D = 0;
+    for (int ia = 1; ia <= L; ++ia) D = std::max(D, D2[ia]);
+    return D;
+}
+
+// MPSSite::NewBondDimensions (MPSSite.C:156-171): keep the top-left block, zero the rest.
+int MPSState::site_resize(int ia, int nD1, int nD2) {
+    if (nD1 == D1[ia] && nD2 == D2[ia]) return TN_OK;
+    size_t cnt = (size_t)d * nD1 * nD2;
+    TN_CHECK(tmp.ensure(sizeof(double) * cnt));
+    if (A[ia]->bytes < sizeof(double) * cnt) TN_CHECK(ensure_capacity(std::max(nD1, nD2)));
+    resize_kernel<<<g1d((long long)cnt), 256, 0, ctx->stream>>>(A[ia]->as<double>(), d, D1[ia], D2[ia],
+                                                                tmp.as<double>(), nD1, nD2);
+    TN_LAUNCH_CHECK();
+    TN_CUDA_CHECK(cudaMemcpyAsync(A[ia]->p, tmp.p, sizeof(double) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
+    D1[ia] = nD1;
+    D2[ia] = nD2;
+    return TN_OK;
+}
+
+// MPSSite::Rescale(sqrt(GetNorm(lr)(1,1))) of HandleEdges: divide by the 2-norm.
+int MPSState::rescale_site(int ia) {
+    long long n = (long long)d * D1[ia] * D2[ia];
+    TN_CHECK(tmp.ensure(sizeof(double) * 2));
+    sumsq_kernel<<<1, 512, 0, ctx->stream>>>(A[ia]->as<double>(), n, tmp.as<double>());
+    TN_LAUNCH_CHECK();
+    scale_by_norm_kernel<<<g1d(n), 256, 0, ctx->stream>>>(A[ia]->as<double>(), n, tmp.as<double>());
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+// MPSSite::SVDNormalize / NormalizeQR + Bond::SVDTransfer / TransferQR
+// (MPSSite_Normalization.C:20-107, Bond.C:162-176, MPSSite_Contractions.C:402-513).
+int MPSState::normalize_site(int ia, bool left) {
+    cudaStream_t st = ctx->stream;
+    // HandleEdges
+    if (!left && ia == 1) {
+        if (L > 1) {
+            int newD2 = std::max(bondK[1], d);
+            if (newD2 < D2[ia]) TN_CHECK(site_resize(ia, D1[ia], newD2));
+        }
+        return rescale_site(ia);
+    }
+    if (left && ia == L) {
+        if (L > 1) {
+            int newD1 = std::max(bondK[L - 1], d);
+            if (newD1 < D1[ia]) TN_CHECK(site_resize(ia, newD1, D2[ia]));
+        }
+        return rescale_site(ia);
+    }
+    const int a1 = D1[ia], a2 = D2[ia];
+    const long long blk = (long long)a1 * a2;
+    double* Aia = A[ia]->as<double>();
+    if (left) {
+        const int m = d * a1, n = a2, k = std::min(m, n);
+        TN_CHECK(Wqr.ensure(sizeof(double) * (size_t)m * n));
+        TN_CHECK(Qqr.ensure(sizeof(double) * (size_t)m * k));
+        TN_CHECK(bondR[ia]->ensure(sizeof(double) * (size_t)k * n));
+        // W(r=(n_,i1), c=i2) = A(n_,i1,i2)
+        TN_CHECK(copy2d(m, n, Aia, idx2(1, a1, blk), idx(a1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
+        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, bondR[ia]->as<double>(), k));
+        // site := Q with D2 = k
+        TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(1, a1, (long long)a1 * k), idx(a1), 1.0, st));
+        D2[ia] = k;
+        // right neighbour: M_n <- R M_n
+        const int nb1 = D1[ia + 1], nb2 = D2[ia + 1];
+        TN_CHECK(tmp.ensure(sizeof(double) * (size_t)d * k * nb2));
+        GemmArgs g;
+        g.M = k; g.N = nb2; g.K = nb1; g.nb0 = d;
+        g.A.ptr = bondR[ia]->as<double>(); g.A.mn = idx(1); g.A.k = idx(k);
+        g.B.ptr = A[ia + 1]->as<double>(); g.B.k = idx(1); g.B.mn = idx(nb1); g.B.sb0 = (long long)nb1 * nb2;
+        g.C.ptr = tmp.as<double>(); g.C.m = idx(1); g.C.n = idx(k); g.C.sb0 = (long long)k * nb2;
+        TN_CHECK(gemm_f64(g, st));
+        TN_CUDA_CHECK(cudaMemcpyAsync(A[ia + 1]->p, tmp.p, sizeof(double) * (size_t)d * k * nb2,
+                                      cudaMemcpyDeviceToDevice, st));
+        D1[ia + 1] = k;
+        bondRm[ia] = k; bondRn[ia] = n; bondDirty[ia] = 1; bondK[ia] = k;
+    } else {
+        // LQ of the D1 x (d*D2) matrix as QR of its transpose (m = d*D2 rows, n = D1 cols)
+        const int m = d * a2, n = a1, k = std::min(m, n);
+        TN_CHECK(Wqr.ensure(sizeof(double) * (size_t)m * n));
+        TN_CHECK(Qqr.ensure(sizeof(double) * (size_t)m * k));
+        TN_CHECK(bondR[ia - 1]->ensure(sizeof(double) * (size_t)k * n));
+        // W(r=(n_,i2), c=i1) = A(n_,i1,i2)
+        TN_CHECK(copy2d(m, n, Aia, idx2(a1, a2, blk), idx(1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
+        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, bondR[ia - 1]->as<double>(), k));
+        // site := Q^T with D1 = k: element (n_, i1', i2) = Q(n_*D2+i2, i1')
+        TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(k, a2, (long long)k * a2), idx(1), 1.0, st));
+        D1[ia] = k;
+        // left neighbour: M_n <- M_n L, L = R^T (n x k)
+        const int pb1 = D1[ia - 1], pb2 = D2[ia - 1];
+        TN_CHECK(tmp.ensure(sizeof(double) * (size_t)d * pb1 * k));
+        GemmArgs g;
+        g.M = pb1; g.N = k; g.K = pb2; g.nb0 = d;
+        g.A.ptr = A[ia - 1]->as<double>(); g.A.mn = idx(1); g.A.k = idx(pb1); g.A.sb0 = (long long)pb1 * pb2;
+        g.B.ptr = bondR[ia - 1]->as<double>(); g.B.k = idx(k); g.B.mn = idx(1);
+        g.C.ptr = tmp.as<double>(); g.C.m = idx(1); g.C.n = idx(pb1); g.C.sb0 = (long long)pb1 * k;
+        TN_CHECK(gemm_f64(g, st));
+        TN_CUDA_CHECK(cudaMemcpyAsync(A[ia - 1]->p, tmp.p, sizeof(double) * (size_t)d * pb1 * k,
+                                      cudaMemcpyDeviceToDevice, st));
+        D2[ia - 1] = k;
+        bondRm[ia - 1] = k; bondRn[ia - 1] = n; bondDirty[ia - 1] = 1; bondK[ia - 1] = k;
+    }
+    return TN_OK;
+}
+
+// Singular values of every bond normalised since the last call, in one
+// batched Jacobi launch, then Bond::SetSingularValues (Bond.C:86-106).
+int MPSState::bond_values_update(bool initial) {
+    std::vector<int> bonds;
+    size_t total = 0;
+    for (int b = 1; b < L; ++b)
+        if (bondDirty[b]) {
+            bonds.push_back(b);
+            total += (size_t)bondRm[b] * bondRn[b] + std::min(bondRm[b], bondRn[b]);
+        }
+    if (bonds.empty()) return TN_OK;
+    TN_CHECK(svdw.ensure(sizeof(double) * total));
+    std::vector<SvdJob> jobs;
+    std::vector<size_t> soff;
+    size_t off = 0;
+    for (int b : bonds) {
+        int r = bondRm[b], c = bondRn[b];
+        int tm = std::max(r, c), tn = std::min(r, c);
+        double* Wb = svdw.as<double>() + off;
+        if (r >= c)
+            TN_CHECK(copy2d(r, c, bondR[b]->as<double>(), idx(1), idx(r), Wb, idx(1), idx(r), 1.0, ctx->stream));
+        else
+            TN_CHECK(copy2d(r, c, bondR[b]->as<double>(), idx(1), idx(r), Wb, idx(c), idx(1), 1.0, ctx->stream));
+        off += (size_t)tm * tn;
+        SvdJob j{};
+        j.W = Wb; j.m = tm; j.n = tn; j.s = svdw.as<double>() + off;
+        soff.push_back(off);
+        off += tn;
+        jobs.push_back(j);
+    }
+    TN_CHECK(svd_batched(*ctx, jobs, false));
+    std::vector<double> hs(total);
+    TN_CUDA_CHECK(cudaMemcpy(hs.data(), svdw.p, sizeof(double) * total, cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < bonds.size(); ++q) {
+        int b = bonds[q];
+        int k = jobs[q].n;
+        std::vector<double> s(hs.begin() + soff[q], hs.begin() + soff[q] + k);
+        double nrm = 0;
+        for (double v : s) nrm += v * v;
+        nrm = std::sqrt(nrm);
+        for (double& v : s) v = nrm > 0 ? v / nrm : 0.0;
+        std::vector<double> old = bond_s[b];
+        old.resize(s.size(), 0.0);
+        double md = 0;
+        for (size_t i = 0; i < s.size(); ++i) md = std::max(md, std::fabs(s[i] - old[i]));
+        bond_maxDelta[b] = md;
+        bond_s[b] = s;
+        bondK[b] = (int)s.size();
+        bondDirty[b] = 0;
+    }
+    (void)initial;
+    return TN_OK;
+}
+
+int MPSState::compute_left_env(int ia) {
+    const SiteMPO& op = H->ops[ia];
+    ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+    size_t need = sizeof(double) * (size_t)op.Dw2 * D2[ia] * D2[ia];
+    TN_CHECK(Lenv[ia]->ensure(need));
+    size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+    TN_CHECK(ctx->P.ensure(scr));
+    TN_CHECK(ctx->Q.ensure(scr));
+    const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;
+    TN_CHECK(env_left_f64(s, t, op.nLR, A[ia]->as<double>(), Lenv[ia - 1]->as<double>(), Lenv[ia]->as<double>(),
+                          ctx->P.as<double>(), ctx->Q.as<double>(), ctx->stream));
+    LenvDw[ia] = op.Dw2;
+    LenvD[ia] = D2[ia];
+    return TN_OK;
+}
+
+int MPSState::compute_right_env(int ia) {
+    const SiteMPO& op = H->ops[ia];
+    ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+    size_t need = sizeof(double) * (size_t)op.Dw1 * D1[ia] * D1[ia];
+    TN_CHECK(Renv[ia]->ensure(need));
+    size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+    TN_CHECK(ctx->P.ensure(scr));
+    TN_CHECK(ctx->Q.ensure(scr));
+    const WTermDev* t = H->terms.as<WTermDev>() + op.offRL;
+    TN_CHECK(env_right_f64(s, t, op.nRL, A[ia]->as<double>(), Renv[ia + 1]->as<double>(), Renv[ia]->as<double>(),
+                           ctx->P.as<double>(), ctx->Q.as<double>(), ctx->stream));
+    RenvDw[ia] = op.Dw1;
+    RenvD[ia] = D1[ia];
+    return TN_OK;
+}
+
+int MPSState::normalize_all(bool left) {
+    if (left) for (int ia = 1; ia <= L; ++ia) TN_CHECK(normalize_site(ia, true));
+    else for (int ia = L; ia >= 1; --ia) TN_CHECK(normalize_site(ia, false));
+    return bond_values_update(true);
+}
+
+// MPSImp::LoadHeffCaches -> CalcHeffRight (MPSImp_Variational.C:120-149).
+int MPSState::load_heff_caches() {
+    for (int ia = L; ia >= 2; --ia) TN_CHECK(compute_right_env(ia));
+    return TN_OK;
+}
+
+// MPSSite::Refine (MPSSite_Variational.C:18-44) with the device eigensolver.
+int MPSState::refine_site(int ia, double epsEigen) {
+    const SiteMPO& op = H->ops[ia];
+    ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+    const long long N = (long long)d * D1[ia] * D2[ia];
+    size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+    TN_CHECK(ctx->P.ensure(scr));
+    TN_CHECK(ctx->Q.ensure(scr));
+    const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;
+    const double* F = Lenv[ia - 1]->as<double>();
+    const double* G = Renv[ia + 1]->as<double>();
+    double* P = ctx->P.as<double>();
+    double* Q = ctx->Q.as<double>();
+    cudaStream_t st = ctx->stream;
+    MatvecFn mv = [&](const double* x, double* y, const int* skip) {
+        return heff_matvec_f64(s, t, op.nLR, F, G, x, y, P, Q, skip, st);
+    };
+    LzResult r{};
+    int krylov = opt.krylov > 0 ? opt.krylov : 20;
+    int restarts = opt.max_restarts > 0 ? opt.max_restarts : 10;
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, &r));
+    matvecs += r.matvecs;
+    matvecs_fp64 += r.matvecs;
+    heff_flop += heff_flops(s) * r.matvecs;
+    if (!r.converged) ++not_converged;
+    iterDE[ia] = r.theta - Emin[ia];
+    Emin[ia] = r.theta;
+    gapE[ia] = r.theta2 - r.theta;
+    return TN_OK;
+}
+
+// MPSImp::Sweep / MPSImp::Refine (MPSImp_Variational.C:64-99).
+int MPSState::sweep(bool left, double epsEigen) {
+    if (left) {
+        for (int ia = 1; ia <= L; ++ia) {
+            TN_CHECK(refine_site(ia, epsEigen));
+            TN_CHECK(normalize_site(ia, true));
+            if (ia < L) TN_CHECK(compute_left_env(ia));
+        }
+    } else {
+        for (int ia = L; ia >= 1; --ia) {
+            TN_CHECK(refine_site(ia, epsEigen));
+            TN_CHECK(normalize_site(ia, false));
+            if (ia > 1) TN_CHECK(compute_right_env(ia));
+        }
+    }
+    return bond_values_update(false);
+}
+
+// MPSImp::IncreaseBondDimensions (MPSImp.C:123-147) with Bond::NewBondDimension (Bond.C:60-84).
+int MPSState::increase_bond_dims(int D) {
+    TN_CHECK(ensure_capacity(std::max(D, max_D())));
+    auto bond_new = [&](int b, int nD) {
+        std::vector<double>& s = bond_s[b];
+        int oD = (int)s.size();
+        if (nD > oD) {
+            double mn = s.empty() ? 1.0 : *std::min_element(s.begin(), s.end());
+            s.resize(nD, mn / 10.0);
+        } else {
+            s.resize(nD);
+        }
+        double nrm = 0;
+        for (double v : s) nrm += v * v;
+        nrm = std::sqrt(nrm);
+        for (double& v : s) v /= nrm;
+        bondK[b] = nD;
+    };
+    int Dideal = 1, ia = 1;
+    for (; ia <= L / 2; ++ia) {
+        int nD1 = std::min(Dideal, D), nD2 = std::min(Dideal * d, D);
+        TN_CHECK(site_resize(ia, nD1, nD2));
+        bond_new(ia, nD2);
+        Dideal *= d;
+    }
+    Dideal = 1;
+    for (int ib = L; ib >= ia; --ib) {
+        int nD2 = std::min(Dideal, D), nD1 = std::min(Dideal * d, D);
+        TN_CHECK(site_resize(ib, nD1, nD2));
+        bond_new(ib - 1, nD1);
+        Dideal *= d;
+    }
+    return TN_OK;
+}
+
+// MPSImp::GetExpectation (MPSImp_ExpectationsAndDMs.C:33-45): left-to-right
+// environment chain with ket = bra, FP64.
+int MPSState::expectation(const std::vector<SiteMPO>& ops, double* E) {
+    cudaStream_t st = ctx->stream;
+    double one = 1.0;
+    TN_CHECK(envA.ensure(sizeof(double)));
+    TN_CUDA_CHECK(cudaMemcpyAsync(envA.p, &one, sizeof(double), cudaMemcpyHostToDevice, st));
+    DevBuf* cur = &envA;
+    DevBuf* nxt = &envB;
+    for (int ia = 1; ia <= L; ++ia) {
+        const SiteMPO& op = ops[ia];
+        ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+        TN_CHECK(nxt->ensure(sizeof(double) * (size_t)op.Dw2 * D2[ia] * D2[ia]));
+        size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+        TN_CHECK(ctx->P.ensure(scr));
+        TN_CHECK(ctx->Q.ensure(scr));
+        const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;
+        TN_CHECK(env_left_f64(s, t, op.nLR, A[ia]->as<double>(), cur->as<double>(), nxt->as<double>(),
+                              ctx->P.as<double>(), ctx->Q.as<double>(), st));
+        std::swap(cur, nxt);
+    }
+    TN_CUDA_CHECK(cudaMemcpyAsync(E, cur->p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    TN_CUDA_CHECK(cudaStreamSynchronize(st));
+    return TN_OK;
+}
+
+// Sweep pairs only (MPSImp_Variational.C:43-47): no D growth, no expectations.
+int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options* o, tn_sweep_stats* stats) {
+    if (o) opt = *o;
+    if (opt.krylov <= 0) opt.krylov = 20;
+    if (opt.max_restarts <= 0) opt.max_restarts = 10;
+    cudaStream_t st = ctx->stream;
+    matvecs = matvecs_fp64 = 0;
+    heff_flop = 0;
+    not_converged = fallbacks = 0;
+    TN_CUDA_CHECK(cudaEventRecord(ctx->ev_a, st));
+    double dE = 0, dl = 0;
+    for (int in = 0; in < nsweeps; ++in) {
+        TN_CHECK(sweep(true, epsEigen));
+        TN_CHECK(sweep(false, epsEigen));
+        dE = 0;
+        for (int ia = 1; ia <= L; ++ia) dE = std::max(dE, std::fabs(iterDE[ia]));
+        dl = 0;
+        for (int b = 1; b < L; ++b) dl = std::max(dl, bond_maxDelta[b]);
+    }
+    TN_CUDA_CHECK(cudaEventRecord(ctx->ev_b, st));
+    TN_CUDA_CHECK(cudaEventSynchronize(ctx->ev_b));
+    float ms = 0;
+    TN_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        double e = 0;
+        for (int ia = 1; ia <= L; ++ia) e = Emin[ia];
+        stats->energy = e;
+        stats->total_sweeps = nsweeps;
+        stats->final_D = max_D();
+        stats->matvecs = matvecs;
+        stats->matvecs_fp64 = matvecs_fp64;
+        stats->heff_flop = heff_flop;
+        stats->sweep_ms = ms;
+        stats->last_dE = dE;
+        stats->last_dlambda = dl;
+        stats->not_converged = not_converged;
+        stats->fallbacks = fallbacks;
+    }
+    return TN_OK;
+}
+
+int MPSState::prepare_sweeps() {
+    TN_CHECK(normalize_all(false));
+    return load_heff_caches();
+}
+
+// MPSImp::FindVariationalGroundState (MPSImp_Variational.C:16-62).
+int MPSState::find_ground_state(const tn_sched_line* lines, int nlines, const tn_solver_options* o,
+                                tn_sweep_stats* stats) {
+    if (o) opt = *o;
+    if (opt.krylov <= 0) opt.krylov = 20;
+    if (opt.max_restarts <= 0) opt.max_restarts = 10;
+    cudaStream_t st = ctx->stream;
+    TN_CUDA_CHECK(cudaEventRecord(ctx->ev_a, st));
+    matvecs = matvecs_fp64 = 0;
+    heff_flop = 0;
+    not_converged = fallbacks = 0;
+    TN_CHECK(normalize_all(false));
+    TN_CHECK(load_heff_caches());
+    double E1 = 0, E2 = 0, DE2 = 0, dE = 0, dl = 0;
+    int total = 0;
+    for (int li = 0; li < nlines; ++li) {
+        const tn_sched_line& isl = lines[li];
+        int Dmax = max_D();
+        for (int D = Dmax; D <= isl.Dmax; D += std::max(1, isl.deltaD)) {
+            if (D > Dmax) {
+                TN_CHECK(increase_bond_dims(D));
+                TN_CHECK(normalize_all(false));
+                TN_CHECK(load_heff_caches());
+            }
+            int in = 0;
+            for (; in < isl.max_sweeps; ++in) {
+                TN_CHECK(sweep(true, isl.eps_eigen));
+                TN_CHECK(sweep(false, isl.eps_eigen));
+                ++total;
+                dE = 0;
+                for (int ia = 1; ia <= L; ++ia) dE = std::max(dE, std::fabs(iterDE[ia]));
+                dl = 0;
+                for (int b = 1; b < L; ++b) dl = std::max(dl, bond_maxDelta[b]);
+                if (opt.verbose) std::printf("%4d %4d %.1e %.1e\n", in, D, dE, dl);
+                if (dE < isl.eps_energy && dl < isl.eps_lambda) break;
+            }
+            TN_CHECK(expectation(H->ops, &E1));
+            TN_CHECK(expectation(H->ops2, &E2));
+            DE2 = E2 - E1 * E1;
+            if (opt.verbose)
+                std::printf("Variational GS D=%4d, %4d iterations, <E>=%.11f, <E^2>-<E>^2=%.2e\n", D,
+                            std::min(in + 1, isl.max_sweeps), E1 / (L - 1), DE2);
+        }
+    }
+    TN_CUDA_CHECK(cudaEventRecord(ctx->ev_b, st));
+    TN_CUDA_CHECK(cudaEventSynchronize(ctx->ev_b));
+    float ms = 0;
+    TN_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->energy = E1;
+        stats->energy2 = E2;
+        stats->variance = DE2;
+        stats->total_sweeps = total;
+        stats->final_D = max_D();
+        stats->matvecs = matvecs;
+        stats->matvecs_fp64 = matvecs_fp64;
+        stats->heff_flop = heff_flop;
+        stats->sweep_ms = ms;
+        stats->last_dE = dE;
+        stats->last_dlambda = dl;
+        stats->not_converged = not_converged;
+        stats->fallbacks = fallbacks;
+    }
+    return TN_OK;
+}
+
+}  // namespace tnb

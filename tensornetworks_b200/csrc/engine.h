@@ -1,0 +1,82 @@
+// engine.h -- device-resident Hamiltonian (MPO) and MPS with the reference's
+// variational sweep semantics (MPSImp_Variational.C:16-173).
+#pragma once
+#include <vector>
+
+#include "contract.h"
+#include "lanczos.h"
+#include "qr.h"
+
+namespace tnb {
+
+struct SiteMPO {
+    int Dw1 = 1, Dw2 = 1;
+    std::vector<double> W;  // (w1,w2,m,n)
+    size_t offLR = 0, offRL = 0, offW = 0;
+    int nLR = 0, nRL = 0;
+};
+
+struct Hamiltonian {
+    Ctx* ctx = nullptr;
+    int L = 0, d = 2, form = 2;
+    double S = 0.5, Jxy = 1, Jz = 1, hz = 0;
+    std::vector<SiteMPO> ops;   // 1-based
+    std::vector<SiteMPO> ops2;  // product MPO (H^2), 1-based
+    DevBuf terms;               // all term lists (WTermDev)
+    DevBuf Wdev;                // all W tensors (for diag(Heff))
+    int build();
+};
+
+struct MPSState {
+    Ctx* ctx = nullptr;
+    Hamiltonian* H = nullptr;
+    int L = 0, d = 2;
+    double normEps = 1e-12, epsSV = 1e-12;
+    std::vector<int> D1, D2;                  // 1-based
+    std::vector<DevBuf*> A;                   // site tensors
+    std::vector<DevBuf*> Lenv, Renv;          // 0..L+1
+    std::vector<int> LenvDw, LenvD, RenvDw, RenvD;
+    std::vector<std::vector<double>> bond_s;  // 1..L-1, normalised
+    std::vector<double> bond_maxDelta;
+    std::vector<DevBuf*> bondR;               // R / L factor of the last normalisation
+    std::vector<int> bondRm, bondRn;          // its dims (rows, cols)
+    std::vector<int> bondK;                   // current bond dimension (Bond::GetD)
+    std::vector<char> bondDirty;
+    std::vector<double> Emin, iterDE, gapE;
+    DevBuf tmp, Wqr, Qqr, svdw, envA, envB;
+    long long matvecs = 0, matvecs_fp64 = 0;
+    double heff_flop = 0;
+    int not_converged = 0, fallbacks = 0;
+    tn_solver_options opt{};
+
+    ~MPSState();
+    int init(Hamiltonian* h, int D);
+    int initialize_random(unsigned long long seed);
+    int max_D() const;
+    int ensure_capacity(int D);
+    int normalize_site(int ia, bool left);
+    int normalize_all(bool left);
+    int bond_values_update(bool initial);
+    int compute_left_env(int ia);
+    int compute_right_env(int ia);
+    int load_heff_caches();
+    int refine_site(int ia, double epsEigen);
+    int sweep(bool left, double epsEigen);
+    int increase_bond_dims(int D);
+    int expectation(const std::vector<SiteMPO>& ops, double* E);
+    int find_ground_state(const tn_sched_line* lines, int nlines, const tn_solver_options* opt,
+                          tn_sweep_stats* stats);
+    int sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options* opt, tn_sweep_stats* stats);
+    int prepare_sweeps();
+    int site_resize(int ia, int nD1, int nD2);
+    int rescale_site(int ia);
+};
+
+}  // namespace tnb
+
+struct tn_hamiltonian_s {
+    tnb::Hamiltonian h;
+};
+struct tn_mps_s {
+    tnb::MPSState m;
+};

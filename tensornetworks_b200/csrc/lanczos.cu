@@ -1,0 +1,466 @@
+// lanczos.cu -- device-resident restarted Lanczos for the lowest eigenpair of Heff.
+//
+// Replaces the dense zheevx call of MPSSite::Refine (MPSSite_Variational.C:18-33,
+// LapackEigenSolver.C:62-109).  Everything except the decision to restart stays
+// on the device: the dots, the full reorthogonalisation (classical Gram-Schmidt
+// applied twice, FP64 coefficients), the norm, the tridiagonal eigenproblem
+// (multisection on Sturm counts over a whole thread block) and the convergence
+// flag.  Kernels launched after convergence see the flag and return at once.
+// Vector passes are grid-stride, coalesced, FP64, with warp-shuffle block
+// reductions and a deterministic last-block final reduction.
+#include "lanczos.h"
+
+#include <cmath>
+
+namespace tnb {
+
+namespace {
+
+constexpr int LZ_THREADS = 256;
+constexpr int KCHUNK = 8;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Reduce KCHUNK per-thread values over the block; result valid in thread 0's out[].
+__device__ void block_sum_chunk(double (&v)[KCHUNK], double* out, double* sh /* [KCHUNK][32] */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < KCHUNK; ++q) v[q] = warp_sum(v[q]);
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < KCHUNK; ++q) sh[q * 32 + wid] = v[q];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int q = 0; q < KCHUNK; ++q) {
+            double s = lane < nw ? sh[q * 32 + lane] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) out[q] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// Number of eigenvalues of the symmetric tridiagonal (a, b) below x.
+__device__ int sturm_count(int n, const double* a, const double* b, double x, double pivmin) {
+    int cnt = 0;
+    double q = a[0] - x;
+    if (q < 0) ++cnt;
+    for (int i = 1; i < n; ++i) {
+        if (fabs(q) < pivmin) q = (q < 0 ? -pivmin : pivmin);
+        q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
+        if (q < 0) ++cnt;
+    }
+    return cnt;
+}
+
+// k-th smallest eigenvalue by block-wide multisection: every round each
+// thread evaluates one Sturm count, shrinking the bracket by blockDim+1.
+__device__ double block_eig_k(int n, const double* a, const double* b, int k) {
+    __shared__ double s_lo, s_hi;
+    double lo = a[0], hi = a[0];
+    for (int i = 0; i < n; ++i) {
+        double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i < n - 1 ? fabs(b[i]) : 0.0);
+        lo = fmin(lo, a[i] - r);
+        hi = fmax(hi, a[i] + r);
+    }
+    double scale = fmax(fabs(lo), fabs(hi));
+    double pivmin = 2.2e-16 * fmax(scale, 1e-300);
+    lo -= 1e-14 * scale + 1e-300;
+    hi += 1e-14 * scale + 1e-300;
+    const int T = blockDim.x;
+    for (int round = 0; round < 12; ++round) {
+        double x = lo + (hi - lo) * (double)(threadIdx.x + 1) / (double)(T + 1);
+        int ok = sturm_count(n, a, b, x, pivmin) <= k;
+        int cnt = __syncthreads_count(ok);
+        if (threadIdx.x == 0) {
+            double nlo = cnt > 0 ? lo + (hi - lo) * (double)cnt / (double)(T + 1) : lo;
+            double nhi = cnt < T ? lo + (hi - lo) * (double)(cnt + 1) / (double)(T + 1) : hi;
+            s_lo = nlo;
+            s_hi = nhi;
+        }
+        __syncthreads();
+        lo = s_lo;
+        hi = s_hi;
+        __syncthreads();
+        if (hi - lo <= 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300) break;
+    }
+    return 0.5 * (lo + hi);
+}
+
+// |last component| of the normalised eigenvector of T for eigenvalue th:
+// y_n^2 = p_{n-1}(th) / p_n'(th) with the monic characteristic polynomials of
+// the leading blocks (scaled recurrences; the ratio is scale-free).
+__device__ double last_component(int n, const double* a, const double* b, double th) {
+    if (n == 1) return 1.0;
+    double pm2 = 1.0, pm1 = th - a[0];  // p0, p1
+    double dm2 = 0.0, dm1 = 1.0;        // p0', p1'
+    for (int k = 2; k <= n; ++k) {
+        double bb = b[k - 2] * b[k - 2];
+        double p = (th - a[k - 1]) * pm1 - bb * pm2;
+        double dp = pm1 + (th - a[k - 1]) * dm1 - bb * dm2;
+        pm2 = pm1; pm1 = p;
+        dm2 = dm1; dm1 = dp;
+        double mx = fmax(fmax(fabs(pm1), fabs(pm2)), fmax(fabs(dm1), fabs(dm2)));
+        if (mx > 1e150) { pm1 *= 1e-150; pm2 *= 1e-150; dm1 *= 1e-150; dm2 *= 1e-150; }
+        else if (mx < 1e-150 && mx > 0) { pm1 *= 1e150; pm2 *= 1e150; dm1 *= 1e150; dm2 *= 1e150; }
+    }
+    // after the loop: pm2 = p_{n-1}, dm1 = p_n'
+    double r = (dm1 != 0.0) ? pm2 / dm1 : 1.0;
+    return sqrt(fabs(r));
+}
+
+// Tridiagonal (T - shift) y = rhs with partial pivoting (dlagtf/dlagts style).
+__device__ void tri_solve(int n, const double* a, const double* b, double shift, double pivmin, double* rhs,
+                          double* dl, double* dd, double* du, double* du2, int* piv) {
+    for (int i = 0; i < n; ++i) dd[i] = a[i] - shift;
+    for (int i = 0; i < n - 1; ++i) { dl[i] = b[i]; du[i] = b[i]; }
+    for (int i = 0; i < n - 1; ++i) {
+        du2[i] = 0;
+        if (fabs(dd[i]) >= fabs(dl[i])) {
+            piv[i] = 0;
+            if (fabs(dd[i]) < pivmin) dd[i] = (dd[i] < 0 ? -pivmin : pivmin);
+            double f = dl[i] / dd[i];
+            dl[i] = f;
+            dd[i + 1] -= f * du[i];
+        } else {
+            piv[i] = 1;
+            double f = dd[i] / dl[i];
+            dd[i] = dl[i];
+            dl[i] = f;
+            double t = du[i];
+            du[i] = dd[i + 1];
+            dd[i + 1] = t - f * du[i];
+            if (i < n - 2) { du2[i] = du[i + 1]; du[i + 1] = -f * du[i + 1]; }
+        }
+    }
+    if (fabs(dd[n - 1]) < pivmin) dd[n - 1] = (dd[n - 1] < 0 ? -pivmin : pivmin);
+    for (int i = 0; i < n - 1; ++i) {
+        if (piv[i] == 0) rhs[i + 1] -= dl[i] * rhs[i];
+        else { double t = rhs[i]; rhs[i] = rhs[i + 1]; rhs[i + 1] = t - dl[i] * rhs[i]; }
+    }
+    rhs[n - 1] /= dd[n - 1];
+    if (n > 1) rhs[n - 2] = (rhs[n - 2] - du[n - 2] * rhs[n - 1]) / dd[n - 2];
+    for (int i = n - 3; i >= 0; --i) rhs[i] = (rhs[i] - du[i] * rhs[i + 1] - du2[i] * rhs[i + 2]) / dd[i];
+}
+
+// ---- kernels ---------------------------------------------------------------
+
+__global__ void lz_reset_kernel(LzState* st, double tol, int first) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        st->done = 0;
+        st->nb = 0;
+        st->counter = 0;
+        if (first) {
+            st->matvecs = 0;
+            st->converged = 0;
+            st->tol = tol;
+            st->theta = 0;
+            st->theta2 = 0;
+            st->resid = 1e300;
+        }
+    }
+}
+
+// ||x||^2 -> st->xnorm (last block).
+__global__ void lz_norm_kernel(const double* __restrict__ x, long long N, double* partial, LzState* st) {
+    __shared__ double sh[KCHUNK * 32];
+    __shared__ double res[KCHUNK];
+    __shared__ bool last;
+    double v[KCHUNK] = {0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        double t = x[i];
+        v[0] = fma(t, t, v[0]);
+    }
+    block_sum_chunk(v, res, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = res[0];
+        __threadfence();
+        unsigned int prev = atomicAdd(&st->counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        double s = 0;
+        for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + b);
+        st->xnorm = sqrt(s);
+        st->counter = 0;
+    }
+}
+
+__global__ void lz_scale_kernel(const double* __restrict__ x, double* __restrict__ v0, long long N,
+                                const LzState* st, int fill_if_zero) {
+    double nr = st->xnorm;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        if (nr > 0) v0[i] = x[i] / nr;
+        else if (fill_if_zero) {
+            // deterministic start vector when x = 0
+            unsigned long long h = (unsigned long long)i * 0x9E3779B97F4A7C15ULL;
+            h ^= h >> 29;
+            v0[i] = ((double)((h >> 11) & 0xFFFFF) / 1048576.0 - 0.5) / sqrt((double)N / 12.0);
+        } else v0[i] = 0.0;
+    }
+}
+
+// h_k = V_k . w for k = 0..j  (partials per block, last block reduces).
+__global__ void lz_dots_kernel(const double* __restrict__ V, const double* __restrict__ w, long long N, int j,
+                               double* partial, LzState* st) {
+    if (st->done) return;
+    __shared__ double sh[KCHUNK * 32];
+    __shared__ double res[KCHUNK];
+    __shared__ bool last;
+    const int nk = j + 1;
+    for (int k0 = 0; k0 < nk; k0 += KCHUNK) {
+        double v[KCHUNK] = {0};
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+             i += (long long)gridDim.x * blockDim.x) {
+            double wi = w[i];
+#pragma unroll
+            for (int q = 0; q < KCHUNK; ++q)
+                if (k0 + q < nk) v[q] = fma(V[(long long)(k0 + q) * N + i], wi, v[q]);
+        }
+        block_sum_chunk(v, res, sh);
+        if (threadIdx.x < KCHUNK && k0 + threadIdx.x < nk)
+            partial[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int prev = atomicAdd(&st->counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+            double s = 0;
+            for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + (long long)b * LZ_MAXK + k);
+            st->h[k] = s;
+        }
+        if (threadIdx.x == 0) st->counter = 0;
+    }
+}
+
+// w' = w - V h;  h2 = V^T w';  nrm2 = |w'|^2.  The last block forms alpha_j,
+// beta_j, solves the tridiagonal problem and sets the convergence flag.
+__global__ void lz_update_kernel(const double* __restrict__ V, double* __restrict__ w, long long N, int j,
+                                 int mmax, double* partial, LzState* st) {
+    if (st->done) return;
+    __shared__ double sh[KCHUNK * 32];
+    __shared__ double res[KCHUNK];
+    __shared__ double hs[LZ_MAXK];
+    __shared__ bool last;
+    const int nk = j + 1;
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h[k];
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        double wi = w[i];
+        for (int k = 0; k < nk; ++k) wi = fma(-hs[k], V[(long long)k * N + i], wi);
+        w[i] = wi;
+    }
+    // second projection (h2) and the norm of w'
+    for (int k0 = 0; k0 < nk + 1; k0 += KCHUNK) {
+        double v[KCHUNK] = {0};
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+             i += (long long)gridDim.x * blockDim.x) {
+            double wi = w[i];
+#pragma unroll
+            for (int q = 0; q < KCHUNK; ++q) {
+                int k = k0 + q;
+                if (k < nk) v[q] = fma(V[(long long)k * N + i], wi, v[q]);
+                else if (k == nk) v[q] = fma(wi, wi, v[q]);
+            }
+        }
+        block_sum_chunk(v, res, sh);
+        if (threadIdx.x < KCHUNK && k0 + (int)threadIdx.x <= nk)
+            partial[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int prev = atomicAdd(&st->counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __shared__ double h2s[LZ_MAXK + 1];
+    for (int k = threadIdx.x; k <= nk; k += blockDim.x) {
+        double s = 0;
+        for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + (long long)b * LZ_MAXK + k);
+        h2s[k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ss = 0;
+        for (int k = 0; k < nk; ++k) { st->h2[k] = h2s[k]; ss += h2s[k] * h2s[k]; }
+        double nrm2 = h2s[nk];
+        st->alpha[j] = hs[j] + h2s[j];
+        st->beta[j] = sqrt(fmax(nrm2 - ss, 0.0));
+        st->counter = 0;
+        st->matvecs += 1;
+    }
+    __syncthreads();
+    const double* a = st->alpha;
+    const double* b = st->beta;
+    double th = block_eig_k(nk, a, b, 0);
+    if (threadIdx.x == 0) {
+        double yl = last_component(nk, a, b, th);
+        double bj = b[j];
+        double resid = bj * yl;
+        double tolEff = fmax(st->tol, 1e-13 * fmax(1.0, fabs(th)));
+        st->theta = th;
+        st->resid = resid;
+        st->nb = nk;
+        bool conv = (resid <= tolEff) || (bj <= 1e-14 * fmax(1.0, fabs(th)));
+        if (conv) { st->done = 1; st->converged = 1; }
+        if (nk >= mmax) st->done = 1;  // basis exhausted for this restart
+    }
+}
+
+// V_{j+1} = (w' - V h2) / beta_j
+__global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N, int j, LzState* st) {
+    if (st->done) return;
+    __shared__ double hs[LZ_MAXK];
+    __shared__ double inv;
+    const int nk = j + 1;
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h2[k];
+    if (threadIdx.x == 0) inv = 1.0 / st->beta[j];
+    __syncthreads();
+    double* vn = V + (long long)(j + 1) * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        double wi = w[i];
+        for (int k = 0; k < nk; ++k) wi = fma(-hs[k], V[(long long)k * N + i], wi);
+        vn[i] = wi * inv;
+    }
+}
+
+// Ritz coefficients y of the lowest eigenpair of T_nb (inverse iteration), and theta2.
+__global__ void lz_ritz_coeffs_kernel(LzState* st) {
+    const int n = st->nb;
+    if (n <= 0) return;
+    double th = block_eig_k(n, st->alpha, st->beta, 0);
+    double th2 = n > 1 ? block_eig_k(n, st->alpha, st->beta, 1) : th;
+    if (threadIdx.x != 0) return;
+    st->theta = th;
+    st->theta2 = th2;
+    __shared__ double y[LZ_MAXK], dl[LZ_MAXK], dd[LZ_MAXK], du[LZ_MAXK], du2[LZ_MAXK];
+    __shared__ int piv[LZ_MAXK];
+    double scale = 0;
+    for (int i = 0; i < n; ++i) scale = fmax(scale, fabs(st->alpha[i]) + (i < n - 1 ? fabs(st->beta[i]) : 0.0));
+    scale = fmax(scale, 1e-300);
+    for (int i = 0; i < n; ++i) y[i] = 1.0 + 0.1 * ((i * 7919) % 97) / 97.0;
+    for (int it = 0; it < 3; ++it) {
+        tri_solve(n, st->alpha, st->beta, th + 4e-15 * scale, 2.2e-16 * scale, y, dl, dd, du, du2, piv);
+        double mx = 0;
+        for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(y[i]));
+        if (mx > 0) for (int i = 0; i < n; ++i) y[i] /= mx;
+    }
+    double nr = 0;
+    for (int i = 0; i < n; ++i) nr += y[i] * y[i];
+    nr = sqrt(nr);
+    int im = 0;
+    for (int i = 1; i < n; ++i) if (fabs(y[i]) > fabs(y[im])) im = i;
+    double sg = (y[im] < 0) ? -1.0 : 1.0;
+    for (int i = 0; i < n; ++i) st->y[i] = sg * y[i] / nr;
+}
+
+// x = V y
+__global__ void lz_ritz_vector_kernel(const double* __restrict__ V, double* __restrict__ x, long long N,
+                                      const LzState* st) {
+    __shared__ double ys[LZ_MAXK];
+    const int n = st->nb;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) ys[k] = st->y[k];
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = 0; k < n; ++k) s = fma(ys[k], V[(long long)k * N + i], s);
+        x[i] = s;
+    }
+}
+
+inline int vec_grid(long long N, int sm) {
+    long long b = (N + LZ_THREADS - 1) / LZ_THREADS;
+    long long cap = (long long)sm * 2;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+}  // namespace
+
+int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
+                  LzResult* out) {
+    cudaStream_t st = c.stream;
+    if (N <= 0) return TN_BAD_SHAPE;
+    int mm = m;
+    if (mm > LZ_MAXK - 1) mm = LZ_MAXK - 1;
+    if ((long long)mm > N) mm = (int)N;
+    if (mm < 1) mm = 1;
+    const int grid = vec_grid(N, c.sm_count);
+    // workspace: V (mm+1 vectors), w, partials
+    size_t need = sizeof(double) * ((size_t)(mm + 2) * N + (size_t)grid * LZ_MAXK + 64);
+    TN_CHECK(c.lz.ensure(need));
+    TN_CHECK(c.lzstate.ensure(sizeof(LzState)));
+    TN_CHECK(c.pinned.ensure(sizeof(LzState)));
+    double* V = c.lz.as<double>();
+    double* w = V + (size_t)(mm + 1) * N;
+    double* partial = w + N;
+    LzState* s = c.lzstate.as<LzState>();
+    LzState* hs = reinterpret_cast<LzState*>(c.pinned.p);
+
+    int restarts = 0;
+    bool converged = false;
+    for (restarts = 0; restarts < (maxRestarts > 0 ? maxRestarts : 1); ++restarts) {
+        lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, restarts == 0);
+        TN_LAUNCH_CHECK();
+        lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
+        TN_LAUNCH_CHECK();
+        lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, V, N, s, 1);
+        TN_LAUNCH_CHECK();
+        for (int j = 0; j < mm; ++j) {
+            double* vj = V + (size_t)j * N;
+            TN_CHECK(mv(vj, w, &s->done));
+            lz_dots_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, j, partial, s);
+            TN_LAUNCH_CHECK();
+            lz_update_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, j, mm, partial, s);
+            TN_LAUNCH_CHECK();
+            if (j + 1 < mm) {
+                lz_next_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, j, s);
+                TN_LAUNCH_CHECK();
+            }
+        }
+        lz_ritz_coeffs_kernel<<<1, LZ_THREADS, 0, st>>>(s);
+        TN_LAUNCH_CHECK();
+        lz_ritz_vector_kernel<<<grid, LZ_THREADS, 0, st>>>(V, x, N, s);
+        TN_LAUNCH_CHECK();
+        TN_CUDA_CHECK(cudaMemcpyAsync(hs, s, sizeof(LzState), cudaMemcpyDeviceToHost, st));
+        TN_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (hs->converged) { converged = true; ++restarts; break; }
+        if ((long long)mm >= N) { converged = true; ++restarts; break; }  // full space spanned: exact
+    }
+    // final normalisation of the Ritz vector
+    lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, 0);
+    TN_LAUNCH_CHECK();
+    lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
+    TN_LAUNCH_CHECK();
+    lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, x, N, s, 0);
+    TN_LAUNCH_CHECK();
+    if (out) {
+        out->theta = hs->theta;
+        out->theta2 = hs->theta2;
+        out->resid = hs->resid;
+        out->matvecs = hs->matvecs;
+        out->restarts = restarts;
+        out->converged = converged ? 1 : 0;
+    }
+    if (!std::isfinite(hs->theta)) {
+        set_error("lanczos: non-finite Ritz value");
+        return TN_NAN_DETECTED;
+    }
+    return TN_OK;
+}
+
+}  // namespace tnb

@@ -1,0 +1,36 @@
+// lanczos.h -- device Lanczos state and host driver.
+#pragma once
+#include <functional>
+
+#include "tn_internal.h"
+
+namespace tnb {
+
+constexpr int LZ_MAXK = 64;
+
+struct LzState {
+    int done;              // 1: converged or basis exhausted; later kernels skip
+    int nb;                // basis size of the current restart
+    int matvecs;           // Heff applications so far
+    int converged;         // residual criterion met
+    unsigned int counter;  // last-block reduction ticket
+    int pad;
+    double tol, theta, theta2, resid, xnorm;
+    double alpha[LZ_MAXK], beta[LZ_MAXK];
+    double h[LZ_MAXK], h2[LZ_MAXK];
+    double y[LZ_MAXK];
+};
+
+struct LzResult {
+    double theta, theta2, resid;
+    int matvecs, restarts, converged;
+};
+
+// mv(x, y, skip): enqueue y = Heff x on the context stream; the launches must
+// do nothing when *skip != 0 (device flag).
+using MatvecFn = std::function<int(const double*, double*, const int*)>;
+
+int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
+                  LzResult* out);
+
+}  // namespace tnb

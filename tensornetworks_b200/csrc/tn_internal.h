@@ -1,0 +1,130 @@
+// tn_internal.h -- shared host/device declarations of libtn_cuda.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/tn_cuda.h"
+
+namespace tnb {
+
+void set_error(const char* fmt, ...);
+
+#define TN_CUDA_CHECK(x)                                                                       \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) {                                                               \
+            ::tnb::set_error("%s:%d %s: %s", __FILE__, __LINE__, #x, cudaGetErrorString(e_)); \
+            return e_ == cudaErrorMemoryAllocation ? TN_OUT_OF_MEMORY : TN_CUDA_ERROR;         \
+        }                                                                                      \
+    } while (0)
+
+#define TN_CHECK(x)                   \
+    do {                              \
+        int s_ = (x);                 \
+        if (s_ != TN_OK) return s_;   \
+    } while (0)
+
+// Every launch site calls TN_LAUNCH_CHECK once per kernel launch: it checks the
+// launch and counts it (tn_launch_count).
+void count_launch();
+#define TN_LAUNCH_CHECK()                 \
+    do {                                  \
+        ::tnb::count_launch();            \
+        TN_CUDA_CHECK(cudaGetLastError()); \
+    } while (0)
+
+// Growable device buffer (bytes); contents are not preserved on growth.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t nbytes);
+    void release();
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+    ~DevBuf() { release(); }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+// Pinned host buffer for small device->host reads.
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t nbytes);
+    ~HostBuf();
+};
+
+// ---------------------------------------------------------------------------
+// FP64 batched GEMM with general (split-index) addressing.
+//   C(i,j) = alpha * sum_k A(i,k) B(k,j) + beta * C(i,j)
+// Each index x of an operand maps to  (x % div) * s + (x / div) * sb, so a
+// single GEMM can walk a contraction index that is split over two tensor
+// indices (e.g. k = (w, j) for environments stored as Dw blocks).
+// Two batch levels (b0, b1) with independent strides.
+// ---------------------------------------------------------------------------
+struct IdxMap {
+    long long s = 0, sb = 0;
+    int div = 1 << 30;
+    __host__ __device__ long long at(int x) const {
+        int q = x / div;
+        return (long long)(x - q * div) * s + (long long)q * sb;
+    }
+};
+inline IdxMap idx(long long s) { IdxMap m; m.s = s; m.sb = 0; m.div = 1 << 30; return m; }
+inline IdxMap idx2(long long s, int div, long long sb) { IdxMap m; m.s = s; m.sb = sb; m.div = div; return m; }
+
+struct GemmOperand {
+    const double* ptr = nullptr;
+    IdxMap mn;       // row index for A (i), column index for B (j)
+    IdxMap k;        // contraction index
+    long long sb0 = 0, sb1 = 0;
+};
+struct GemmOut {
+    double* ptr = nullptr;
+    IdxMap m, n;
+    long long sb0 = 0, sb1 = 0;
+};
+struct GemmArgs {
+    int M = 0, N = 0, K = 0;
+    int nb0 = 1, nb1 = 1;
+    double alpha = 1.0, beta = 0.0;
+    GemmOperand A, B;
+    GemmOut C;
+    const int* skip = nullptr;  // device flag: when nonzero the launch does nothing
+};
+int gemm_f64(const GemmArgs& g, cudaStream_t st);
+
+// Sparse MPO term list: out[(m,wout)] += c * in[(win,n)].
+struct WTerm {
+    int win, n, wout, m;
+    double c;
+};
+
+// Execution context (one per tn_ctx handle).
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    // scratch
+    DevBuf P, Q;           // contraction intermediates
+    DevBuf lz;             // Lanczos basis + work vectors
+    DevBuf lzstate;        // Lanczos device state
+    DevBuf qrw;            // QR workspace
+    DevBuf svdw;           // SVD workspace
+    DevBuf wterms;         // MPO term lists
+    DevBuf misc;
+    HostBuf pinned;
+    int sm_count = 148;
+};
+
+}  // namespace tnb
+
+struct tn_ctx_s {
+    tnb::Ctx c;
+};

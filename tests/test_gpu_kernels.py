@@ -1,0 +1,188 @@
+"""GPU parity of the individual kernels against the FP64 CPU oracle.
+
+Every call goes through the C ABI (libtn_cuda.so); device buffers are torch
+CUDA tensors.  FP64 kernels are compared at tolerances a few ulps times the
+problem norm.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def T():
+    import tensornetworks_b200 as T
+    return T
+
+
+@pytest.fixture(scope="module")
+def ctx(T):
+    return T.default_context()
+
+
+def dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def envs(oracle, d, D1, D2, site, L=6, hz=0.2, seed=3):
+    """Physical environments of a random L-site chain around `site`, whose
+    tensor is D1 x D2 (D1 = 1 at site 1, D2 = 1 at site L); Heff is symmetric."""
+    rng = np.random.default_rng(seed)
+    S = (d - 1) / 2
+    Ws = {i: oracle.mpo_site(L, S, 2, 1.0, 1.0, hz, i) for i in range(1, L + 1)}
+    shapes = {}
+    for i in range(1, L + 1):
+        if i < site:
+            shapes[i] = (1 if i == 1 else D1, D1)
+        elif i == site:
+            shapes[i] = (D1, D2)
+        else:
+            shapes[i] = (D2, 1 if i == L else D2)
+    A = {i: rng.uniform(-1, 1, size=(d,) + shapes[i]) for i in range(1, L + 1)}
+    F = np.ones(1)
+    for i in range(1, site):
+        F = oracle.env_left(Ws[i], A[i], F)
+    G = np.ones(1)
+    for i in range(L, site, -1):
+        G = oracle.env_right(Ws[i], A[i], G)
+    return Ws[site], A[site], F, G
+
+
+@pytest.mark.parametrize("d,D1,D2,site", [(2, 8, 8, 3), (2, 16, 32, 3), (3, 9, 9, 3), (2, 1, 2, 1),
+                                          (2, 64, 64, 3), (2, 48, 40, 4), (2, 8, 1, 6)])
+def test_heff_matvec_and_envs(T, ctx, oracle, d, D1, D2, site):
+    W, A, F, G = envs(oracle, d, D1, D2, site)
+    Dw1, Dw2 = W.shape[:2]
+    D1, D2 = A.shape[1:]
+    x = oracle.site_flat(A)
+    lib = ctx._lib
+    Wc = np.ascontiguousarray(W.ravel())
+    dF, dG, dx = dev(F), dev(G), dev(x)
+    y = dev(np.zeros_like(x))
+    T._capi.check(lib.tn_heff_matvec(ctx.handle, 0, d, Dw1, Dw2, D1, D2, Wc.ctypes.data, dF.data_ptr(),
+                                     dG.data_ptr(), dx.data_ptr(), y.data_ptr()), "matvec")
+    ref = oracle.heff_matvec(W, F, G, x, D1, D2)
+    scale = np.abs(ref).max() + 1e-300
+    assert np.abs(host(y) - ref).max() <= 1e-12 * scale
+    # diag
+    dg = dev(np.zeros_like(x))
+    T._capi.check(lib.tn_heff_diag(ctx.handle, d, Dw1, Dw2, D1, D2, Wc.ctypes.data, dF.data_ptr(), dG.data_ptr(),
+                                   dg.data_ptr()), "diag")
+    np.testing.assert_allclose(host(dg), oracle.heff_diag(W, F, G, D1, D2), rtol=1e-12, atol=1e-12 * scale)
+    # environments
+    outL = dev(np.zeros(Dw2 * D2 * D2))
+    T._capi.check(lib.tn_env_left(ctx.handle, 0, d, Dw1, Dw2, D1, D2, Wc.ctypes.data, dx.data_ptr(), dF.data_ptr(),
+                                  outL.data_ptr()), "env_left")
+    refL = oracle.env_left(W, A, F)
+    assert np.abs(host(outL) - refL).max() <= 1e-12 * (np.abs(refL).max() + 1e-300)
+    outR = dev(np.zeros(Dw1 * D1 * D1))
+    T._capi.check(lib.tn_env_right(ctx.handle, 0, d, Dw1, Dw2, D1, D2, Wc.ctypes.data, dx.data_ptr(), dG.data_ptr(),
+                                   outR.data_ptr()), "env_right")
+    refR = oracle.env_right(W, A, G)
+    assert np.abs(host(outR) - refR).max() <= 1e-12 * (np.abs(refR).max() + 1e-300)
+
+
+@pytest.mark.parametrize("d,D1,D2,site", [(2, 8, 8, 3), (2, 32, 32, 3), (3, 9, 9, 3), (2, 2, 4, 2)])
+def test_lanczos_heff(T, ctx, oracle, d, D1, D2, site):
+    W, A, F, G = envs(oracle, d, D1, D2, site)
+    Dw1, Dw2 = W.shape[:2]
+    D1, D2 = A.shape[1:]
+    H = oracle.heff_dense(W, F, G, D1, D2)
+    H = 0.5 * (H + H.T)
+    w = np.linalg.eigvalsh(H)
+    x0 = oracle.site_flat(A)
+    dx = dev(x0)
+    th, res, nmv = C.c_double(), C.c_double(), C.c_int()
+    opt = T.SolverOptions(krylov=20, max_restarts=30).to_c()
+    Wc = np.ascontiguousarray(W.ravel())
+    st = ctx._lib.tn_eigensolve_heff(ctx.handle, C.byref(opt), d, Dw1, Dw2, D1, D2, Wc.ctypes.data,
+                                     dev(F).data_ptr(), dev(G).data_ptr(), dx.data_ptr(), 1e-10, C.byref(th),
+                                     C.byref(res), C.byref(nmv))
+    assert st == 0, T._capi.last_error()
+    assert abs(th.value - w[0]) < 1e-9 * max(1, abs(w[0]))
+    x = host(dx)
+    assert abs(np.linalg.norm(x) - 1) < 1e-12
+    assert np.linalg.norm(H @ x - th.value * x) < 1e-8 * max(1, abs(w[0]))
+    # same algorithm as the oracle: same Ritz value
+    tho, _, _, _ = oracle.lanczos_heff(W, F, G, x0, D1, D2, krylov=20, max_restarts=30, tol=1e-10)
+    assert abs(th.value - tho) < 1e-10 * max(1, abs(tho))
+
+
+@pytest.mark.parametrize("m,n", [(7, 5), (5, 7), (64, 32), (32, 64), (512, 256), (130, 130), (1, 5), (9, 1)])
+def test_qr_lq(T, ctx, oracle, m, n):
+    rng = np.random.default_rng(m * 1000 + n)
+    A = rng.uniform(-1, 1, size=(m, n))
+    Q, R = T.CudaQRSolver(ctx).SolveThinQR(A)
+    k = min(m, n)
+    assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-13
+    assert np.allclose(np.triu(R), R)
+    assert np.abs(Q @ R - A).max() < 1e-12
+    Qo, Ro = oracle.qr(A)
+    np.testing.assert_allclose(R, Ro, atol=1e-11)    # same reflector convention -> same factors
+    Lm, Q2 = T.CudaQRSolver(ctx).SolveThinLQ(A)
+    assert np.abs(Q2 @ Q2.T - np.eye(k)).max() < 1e-13
+    assert np.abs(Lm @ Q2 - A).max() < 1e-12
+    assert np.allclose(np.tril(Lm), Lm)
+
+
+def test_qr_zero_columns_complete(T, ctx):
+    rng = np.random.default_rng(1)
+    A = np.zeros((40, 16))
+    A[:, :5] = rng.uniform(-1, 1, size=(40, 5))
+    Q, R = T.CudaQRSolver(ctx).SolveThinQR(A)
+    assert np.abs(Q.T @ Q - np.eye(16)).max() < 1e-13
+    assert np.abs(Q @ R - A).max() < 1e-13
+
+
+@pytest.mark.parametrize("m,n", [(7, 5), (5, 7), (64, 32), (32, 64), (200, 120), (1, 4), (6, 1)])
+def test_svd(T, ctx, oracle, m, n):
+    rng = np.random.default_rng(m * 7 + n)
+    A = rng.uniform(-1, 1, size=(m, n))
+    U, s, Vt = T.CudaSVDSolver(ctx).SolveAll(A)
+    k = min(m, n)
+    tol = 2 * np.sqrt(m * n) * 1e-13
+    np.testing.assert_allclose(s, oracle.svd_values(A), atol=tol * s[0])
+    np.testing.assert_allclose(s, np.linalg.svd(A, compute_uv=False), atol=tol * s[0])
+    assert np.abs(U.T @ U - np.eye(k)).max() < tol
+    assert np.abs(Vt @ Vt.T - np.eye(k)).max() < tol
+    assert np.abs(U @ np.diag(s) @ Vt - A).max() < tol
+
+
+def test_svd_rank_deficient(T, ctx):
+    rng = np.random.default_rng(5)
+    A = np.zeros((24, 12))
+    A[:, :3] = rng.uniform(-1, 1, size=(24, 3))
+    U, s, Vt = T.CudaSVDSolver(ctx).SolveAll(A)
+    assert np.all(s[3:] < 1e-13)
+    assert np.abs(U.T @ U - np.eye(12)).max() < 1e-12
+    assert np.abs(U @ np.diag(s) @ Vt - A).max() < 1e-12
+
+
+def test_dense_eigensolver(T, ctx):
+    rng = np.random.default_rng(2)
+    B = rng.uniform(-1, 1, size=(60, 60))
+    A = B + B.T
+    U, w = T.CudaEigenSolver(ctx).Solve(A, 1e-12, 2)
+    ev = np.linalg.eigvalsh(A)
+    np.testing.assert_allclose(w, ev[:2], atol=1e-9)
+    assert np.linalg.norm(A @ U - U * w) < 1e-7
+
+
+def test_compressor(T, ctx, oracle):
+    rng = np.random.default_rng(4)
+    A = rng.uniform(-1, 1, size=(12, 10))
+    U, s, Vt = oracle.svd(A)
+    for Dmax, eps in [(4, 0.0), (0, np.sum(s[7:] ** 2) * 1.0001), (5, 1e-3)]:
+        U2, s2, Vt2, err = T.SVCompressor(Dmax, eps, ctx).Compress(U, s, Vt)
+        Uo, so, Vto, erro = oracle.compress(U, s, Vt, Dmax, eps)
+        np.testing.assert_allclose(s2, so, rtol=1e-14)
+        np.testing.assert_allclose(err, erro, rtol=1e-14)
+        assert U2.shape == Uo.shape and Vt2.shape == Vto.shape
