@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--D", type=int, default=D_FINAL)
     p.add_argument("--cpu-sites", type=int, default=4, help="bulk site updates in the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--profile-region", action="store_true",
+                   help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
 
 
@@ -219,12 +221,16 @@ def run_ours(args, rank, world, local_rank):
     clocks.start()
     launches0 = lib.tn_launch_count()
     step_ms, matvecs, flops = [], 0, 0.0
+    if args.profile_region:
+        torch.cuda.profiler.start()
     for _ in range(args.steps):
         st = psi.Sweep(H, 1, EPS_EIGEN, opts)
         step_ms.append(st["sweep_ms"])
         matvecs += st["matvecs"]
         flops += st["heff_flop"]
     torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.stop()
     launches = lib.tn_launch_count() - launches0
     clocks.stop()
     t_step = sum(step_ms) / len(step_ms) / 1e3

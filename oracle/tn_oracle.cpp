@@ -1136,19 +1136,21 @@ static int max_D(const MPS& psi) {
 // MPSImp::IncreaseBondDimensions (MPSImp.C:123-147).
 static void increase_bond_dims(MPS& psi, int D) {
     int L = psi.L, d = psi.d;
-    int Dideal = 1, ia = 1;
+    // Dideal = d^k saturates at D (the reference's int product overflows beyond L ~ 60)
+    long long Dideal = 1;
+    int ia = 1;
     for (; ia <= L / 2; ++ia) {
-        int D1 = std::min(Dideal, D), D2 = std::min(Dideal * d, D);
+        int D1 = (int)std::min<long long>(Dideal, D), D2 = (int)std::min<long long>(Dideal * d, D);
         site_resize(psi.sites[ia], d, D1, D2);
         bond_new_dim(psi.bonds[ia], D2);
-        Dideal *= d;
+        Dideal = std::min<long long>(Dideal * d, D);
     }
     Dideal = 1;
     for (int ib = L; ib >= ia; --ib) {
-        int D2 = std::min(Dideal, D), D1 = std::min(Dideal * d, D);
+        int D2 = (int)std::min<long long>(Dideal, D), D1 = (int)std::min<long long>(Dideal * d, D);
         site_resize(psi.sites[ib], d, D1, D2);
         bond_new_dim(psi.bonds[ib - 1], D1);
-        Dideal *= d;
+        Dideal = std::min<long long>(Dideal * d, D);
     }
 }
 

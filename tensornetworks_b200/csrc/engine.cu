@@ -533,19 +533,21 @@ int MPSState::increase_bond_dims(int D) {
         for (double& v : s) v /= nrm;
         bondK[b] = nD;
     };
-    int Dideal = 1, ia = 1;
+    // Dideal = d^k saturates at D (the reference's int product overflows beyond L ~ 60)
+    long long Dideal = 1;
+    int ia = 1;
     for (; ia <= L / 2; ++ia) {
-        int nD1 = std::min(Dideal, D), nD2 = std::min(Dideal * d, D);
+        int nD1 = (int)std::min<long long>(Dideal, D), nD2 = (int)std::min<long long>(Dideal * d, D);
         TN_CHECK(site_resize(ia, nD1, nD2));
         bond_new(ia, nD2);
-        Dideal *= d;
+        Dideal = std::min<long long>(Dideal * d, D);
     }
     Dideal = 1;
     for (int ib = L; ib >= ia; --ib) {
-        int nD2 = std::min(Dideal, D), nD1 = std::min(Dideal * d, D);
+        int nD2 = (int)std::min<long long>(Dideal, D), nD1 = (int)std::min<long long>(Dideal * d, D);
         TN_CHECK(site_resize(ib, nD1, nD2));
         bond_new(ib - 1, nD1);
-        Dideal *= d;
+        Dideal = std::min<long long>(Dideal * d, D);
     }
     return TN_OK;
 }

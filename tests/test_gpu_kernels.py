@@ -103,8 +103,9 @@ def test_lanczos_heff(T, ctx, oracle, d, D1, D2, site):
     th, res, nmv = C.c_double(), C.c_double(), C.c_int()
     opt = T.SolverOptions(krylov=20, max_restarts=30).to_c()
     Wc = np.ascontiguousarray(W.ravel())
+    dF, dG = dev(F), dev(G)   # keep the device buffers alive across the call
     st = ctx._lib.tn_eigensolve_heff(ctx.handle, C.byref(opt), d, Dw1, Dw2, D1, D2, Wc.ctypes.data,
-                                     dev(F).data_ptr(), dev(G).data_ptr(), dx.data_ptr(), 1e-10, C.byref(th),
+                                     dF.data_ptr(), dG.data_ptr(), dx.data_ptr(), 1e-10, C.byref(th),
                                      C.byref(res), C.byref(nmv))
     assert st == 0, T._capi.last_error()
     assert abs(th.value - w[0]) < 1e-9 * max(1, abs(w[0]))
