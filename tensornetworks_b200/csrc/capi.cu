@@ -68,12 +68,25 @@ using namespace tnb;
 
 namespace {
 
+// Term list of a host W on the device; the last upload is cached per context so
+// repeated calls with the same W (a Krylov loop) add no copy and no sync.
 int upload_terms(Ctx& c, const double* W_host, int d, int Dw1, int Dw2, bool lr, const WTermDev** out, int* n) {
+    const size_t nw = (size_t)Dw1 * Dw2 * d * d;
+    const int key[4] = {d, Dw1, Dw2, lr ? 1 : 0};
+    if (c.wcache_n > 0 && std::memcmp(key, c.wcache_key, sizeof(key)) == 0 && c.wcache_W.size() == nw &&
+        std::memcmp(c.wcache_W.data(), W_host, nw * sizeof(double)) == 0) {
+        *out = c.wterms.as<WTermDev>();
+        *n = c.wcache_n;
+        return TN_OK;
+    }
     auto t = build_terms(W_host, d, Dw1, Dw2, lr);
     TN_CHECK(c.wterms.ensure(sizeof(WTermDev) * t.size()));
     TN_CUDA_CHECK(cudaMemcpyAsync(c.wterms.p, t.data(), sizeof(WTermDev) * t.size(), cudaMemcpyHostToDevice, c.stream));
     // the host vector dies at return: wait for the copy
     TN_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    c.wcache_W.assign(W_host, W_host + nw);
+    std::memcpy(c.wcache_key, key, sizeof(key));
+    c.wcache_n = (int)t.size();
     *out = c.wterms.as<WTermDev>();
     *n = (int)t.size();
     return TN_OK;

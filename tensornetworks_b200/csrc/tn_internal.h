@@ -121,6 +121,10 @@ struct Ctx {
     DevBuf misc;
     HostBuf pinned;
     int sm_count = 148;
+    // cache of the last MPO term list uploaded through the C ABI
+    std::vector<double> wcache_W;
+    int wcache_key[4] = {0, 0, 0, 0};
+    int wcache_n = 0;
 };
 
 }  // namespace tnb
