@@ -49,9 +49,12 @@ enum { TN_FORM_REGULAR_UPPER = 1, TN_FORM_REGULAR_LOWER = 2 };
 enum { TN_DLEFT = 0, TN_DRIGHT = 1 };
 /* Arithmetic of the Heff / environment contractions. */
 enum {
-    TN_PREC_FP64  = 0,  /* FP64 throughout (the plain GPU sweep)             */
-    TN_PREC_MIXED = 1   /* BF16x3 tcgen05 contractions with FP32 accumulate,
-                           FP64 Lanczos/QR/SVD/energies (mixed path)         */
+    TN_PREC_FP64     = 0,  /* FP64 throughout (the plain GPU sweep)          */
+    TN_PREC_MIXED    = 1,  /* BF16x3 tcgen05 contractions (2 BF16 pieces per
+                              operand, 3 products, FP32 accumulate); FP64
+                              Lanczos coefficients, QR, SVD and energies     */
+    TN_PREC_MIXED_HI = 2   /* BF16x6 (3 pieces, 6 products: ~FP32 operand
+                              accuracy) on the same tcgen05 kernels         */
 };
 /* Eigensolvers for the site problem. */
 enum {
@@ -84,6 +87,12 @@ typedef struct {
     int max_restarts;    /* restarts per site (10)                         */
     int use_learned;     /* 1: learned preconditioner (Davidson only)      */
     int verbose;         /* 1: print the reference's per-sweep log line     */
+    double mixed_tol;    /* residual target of the split-precision Krylov
+                            phase (0: 1e-6 for MIXED, 1e-9 for MIXED_HI)   */
+    double refine_tol;   /* FP64 residual above which an FP64 Lanczos
+                            continuation follows the split-precision solve
+                            (0: never; the FP64 Rayleigh quotient always
+                            supplies the site energy)                       */
 } tn_solver_options;
 
 /* Per-run statistics, device-timed with CUDA events. */
@@ -176,6 +185,18 @@ unsigned long long tn_launch_count(void);
 int tn_heff_matvec(tn_ctx ctx, int precision, int d, int Dw1, int Dw2, int D1, int D2,
                    const double* W_host, const double* F, const double* G,
                    const double* x, double* y);
+/* Heff operator object: the device-side SparseEigenSolverClient
+ * (SparseEigenSolver.H:17-24) of one site.  Creation uploads W and, for the
+ * split-precision modes, splits F and G into BF16 pieces once; apply is then
+ * the client's DoMatVecContraction(N, x, y) on device vectors.  F and G must
+ * stay unchanged while the handle is in use. */
+typedef struct tn_heff_s* tn_heff;
+int tn_heff_create(tn_ctx ctx, int precision, int d, int Dw1, int Dw2, int D1, int D2,
+                   const double* W_host, const double* F, const double* G, tn_heff* out);
+/* GetSize(): d*D1*D2. */
+long long tn_heff_size(tn_heff op);
+int tn_heff_apply(tn_heff op, const double* x, double* y);
+int tn_heff_destroy(tn_heff op);
 /* diag(Heff) (feature of the Davidson preconditioner). */
 int tn_heff_diag(tn_ctx ctx, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
                  const double* F, const double* G, double* diag);

@@ -3,6 +3,6 @@ for open 1-D spin chains, with the API surface of JanReimers/TensorNetworks'
 Factory -> Hamiltonian -> MPS::FindVariationalGroundState path."""
 from ._capi import LIB_PATH, TNError, load  # noqa: F401
 from .api import (  # noqa: F401
-    DAVIDSON, FP64, LANCZOS, MIXED, Context, CudaEigenSolver, CudaQRSolver, CudaSVDSolver, DLeft, DRight,
+    DAVIDSON, FP64, LANCZOS, MIXED, MIXED_HI, Context, CudaEigenSolver, CudaQRSolver, CudaSVDSolver, DLeft, DRight,
     Epsilons, Factory, Hamiltonian, IterationSchedule, IterationScheduleLine, MPS, Random, RegularLower,
     RegularUpper, SolverOptions, SVCompressor, default_context)

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libtn_cuda.so")
 TN_OK, TN_NOT_CONVERGED, TN_BAD_SHAPE, TN_NAN_DETECTED = 0, 1, 2, 3
 TN_CUDA_ERROR, TN_BAD_ARG, TN_NO_DEVICE, TN_OUT_OF_MEMORY = 4, 5, 6, 7
 TN_FORM_REGULAR_UPPER, TN_FORM_REGULAR_LOWER = 1, 2
+TN_PREC_MIXED_HI = 2
 TN_DLEFT, TN_DRIGHT = 0, 1
 TN_PREC_FP64, TN_PREC_MIXED = 0, 1
 TN_EIG_LANCZOS, TN_EIG_DAVIDSON = 0, 1
@@ -38,7 +39,8 @@ class SchedLine(C.Structure):
 
 class SolverOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("eigensolver", C.c_int), ("krylov", C.c_int),
-                ("max_restarts", C.c_int), ("use_learned", C.c_int), ("verbose", C.c_int)]
+                ("max_restarts", C.c_int), ("use_learned", C.c_int), ("verbose", C.c_int),
+                ("mixed_tol", C.c_double), ("refine_tol", C.c_double)]
 
 
 class SweepStats(C.Structure):
@@ -87,6 +89,10 @@ SIGNATURES = {
     "tn_launch_count": (C.c_ulonglong, []),
     "tn_heff_matvec": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _V, _V]),
     "tn_heff_diag": (_I, [_V, _I, _I, _I, _I, _I, _V, _V, _V, _V]),
+    "tn_heff_create": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _PV]),
+    "tn_heff_size": (C.c_longlong, [_V]),
+    "tn_heff_apply": (_I, [_V, _V, _V]),
+    "tn_heff_destroy": (_I, [_V]),
     "tn_env_left": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _V]),
     "tn_env_right": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _V]),
     "tn_eigensolve_heff": (_I, [_V, C.POINTER(SolverOptions), _I, _I, _I, _I, _I, _V, _V, _V, _V, _D,

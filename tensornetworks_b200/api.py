@@ -32,7 +32,7 @@ from ._capi import check
 DLeft, DRight = capi.TN_DLEFT, capi.TN_DRIGHT
 Product, Random, Neel, Constant = 0, 1, 2, 3
 RegularUpper, RegularLower = capi.TN_FORM_REGULAR_UPPER, capi.TN_FORM_REGULAR_LOWER
-FP64, MIXED = capi.TN_PREC_FP64, capi.TN_PREC_MIXED
+FP64, MIXED, MIXED_HI = capi.TN_PREC_FP64, capi.TN_PREC_MIXED, capi.TN_PREC_MIXED_HI
 LANCZOS, DAVIDSON = capi.TN_EIG_LANCZOS, capi.TN_EIG_DAVIDSON
 
 
@@ -139,10 +139,12 @@ class SolverOptions:
     max_restarts: int = 10
     use_learned: int = 0
     verbose: int = 0
+    mixed_tol: float = 0.0
+    refine_tol: float = 0.0
 
     def to_c(self):
         return capi.SolverOptions(self.precision, self.eigensolver, self.krylov, self.max_restarts,
-                                  self.use_learned, self.verbose)
+                                  self.use_learned, self.verbose, self.mixed_tol, self.refine_tol)
 
 
 # ---------------------------------------------------------------------------

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "engine.h"
+#include "mixed.h"
 
 namespace tnb {
 
@@ -349,22 +350,100 @@ int tn_mps_get_site_energies(tn_mps m, double* E) {
 }
 
 // ---- solver interfaces -----------------------------------------------------------
+}  // extern "C"
+
+struct tn_heff_s {
+    tn_ctx ctx = nullptr;
+    int precision = TN_PREC_FP64;
+    tnb::ContractShape s{};
+    tnb::DevBuf terms, P, Q;
+    int nterms = 0;
+    const double* F = nullptr;
+    const double* G = nullptr;
+    tnb::MixedSite ms;
+};
+
+extern "C" {
+
+int tn_heff_create(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
+                   const double* F, const double* G, tn_heff* out) {
+    if (!c || !W_host || !F || !G || !out) return TN_BAD_ARG;
+    *out = nullptr;
+    if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
+    if (precision < TN_PREC_FP64 || precision > TN_PREC_MIXED_HI) return TN_BAD_ARG;
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    if (precision != TN_PREC_FP64 && !mixed_supported(s)) {
+        set_error("split precision needs D1, D2 multiples of 16 (got %d, %d)", D1, D2);
+        return TN_BAD_SHAPE;
+    }
+    tn_heff h = new tn_heff_s();
+    h->ctx = c;
+    h->precision = precision;
+    h->s = s;
+    h->F = F;
+    h->G = G;
+    auto t = build_terms(W_host, d, Dw1, Dw2, true);
+    int st = h->terms.ensure(sizeof(WTermDev) * t.size());
+    if (st == TN_OK && cudaMemcpy(h->terms.p, t.data(), sizeof(WTermDev) * t.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        st = TN_CUDA_ERROR;
+    h->nterms = (int)t.size();
+    if (st == TN_OK) {
+        if (precision == TN_PREC_FP64) {
+            size_t scr = sizeof(double) * contract_scratch_doubles(s);
+            st = h->P.ensure(scr);
+            if (st == TN_OK) st = h->Q.ensure(scr);
+        } else {
+            st = mixed_prepare_site(c->c, h->ms, s, h->terms.as<WTermDev>(), h->nterms, F, G, -1, -1,
+                                    precision == TN_PREC_MIXED_HI ? 3 : 2);
+        }
+    }
+    if (st != TN_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return TN_OK;
+}
+
+long long tn_heff_size(tn_heff h) { return h ? (long long)h->s.d * h->s.D1 * h->s.D2 : -1; }
+
+int tn_heff_apply(tn_heff h, const double* x, double* y) {
+    if (!h || !x || !y) return TN_BAD_ARG;
+    Ctx& cx = h->ctx->c;
+    if (h->precision == TN_PREC_FP64)
+        return heff_matvec_f64(h->s, h->terms.as<WTermDev>(), h->nterms, h->F, h->G, x, y, h->P.as<double>(),
+                               h->Q.as<double>(), nullptr, cx.stream);
+    return heff_matvec_mixed(cx, h->ms, x, y, nullptr);
+}
+
+int tn_heff_destroy(tn_heff h) {
+    if (!h) return TN_BAD_ARG;
+    cudaStreamSynchronize(h->ctx->c.stream);
+    int st = TN_OK;
+    if (h->precision != TN_PREC_FP64 && h->ms.ready) st = mixed_check_error(h->ms, h->ctx->c.stream);
+    delete h;
+    return st;
+}
+
 int tn_heff_matvec(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
                    const double* F, const double* G, const double* x, double* y) {
     if (!c || !W_host || !F || !G || !x || !y) return TN_BAD_ARG;
     if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
     if (precision != TN_PREC_FP64) {
-        set_error("precision %d not available for this entry point", precision);
-        return TN_BAD_ARG;
+        tn_heff h = nullptr;
+        TN_CHECK(tn_heff_create(c, precision, d, Dw1, Dw2, D1, D2, W_host, F, G, &h));
+        int st = tn_heff_apply(h, x, y);
+        int st2 = tn_heff_destroy(h);
+        return st != TN_OK ? st : st2;
     }
     Ctx& cx = c->c;
     const WTermDev* t;
     int nt;
     TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, true, &t, &nt));
-    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(cx.P.ensure(scr));
     TN_CHECK(cx.Q.ensure(scr));
-    ContractShape s{d, Dw1, Dw2, D1, D2};
     TN_CHECK(heff_matvec_f64(s, t, nt, F, G, x, y, cx.P.as<double>(), cx.Q.as<double>(), nullptr, cx.stream));
     return TN_OK;
 }
@@ -392,10 +471,10 @@ int tn_env_left(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2
     const WTermDev* t;
     int nt;
     TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, true, &t, &nt));
-    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(cx.P.ensure(scr));
     TN_CHECK(cx.Q.ensure(scr));
-    ContractShape s{d, Dw1, Dw2, D1, D2};
     return env_left_f64(s, t, nt, A, F, Fout, cx.P.as<double>(), cx.Q.as<double>(), cx.stream);
 }
 
@@ -408,10 +487,10 @@ int tn_env_right(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D
     const WTermDev* t;
     int nt;
     TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, false, &t, &nt));
-    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(cx.P.ensure(scr));
     TN_CHECK(cx.Q.ensure(scr));
-    ContractShape s{d, Dw1, Dw2, D1, D2};
     return env_right_f64(s, t, nt, A, G, Gout, cx.P.as<double>(), cx.Q.as<double>(), cx.stream);
 }
 
@@ -426,10 +505,10 @@ int tn_eigensolve_heff(tn_ctx c, const tn_solver_options* opt, int d, int Dw1, i
     const WTermDev* t;
     int nt;
     TN_CHECK(upload_terms(cx, W_host, d, Dw1, Dw2, true, &t, &nt));
-    size_t scr = sizeof(double) * (size_t)d * std::max(Dw1, Dw2) * D1 * D2;
+    ContractShape s{d, Dw1, Dw2, D1, D2};
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(cx.P.ensure(scr));
     TN_CHECK(cx.Q.ensure(scr));
-    ContractShape s{d, Dw1, Dw2, D1, D2};
     double* P = cx.P.as<double>();
     double* Q = cx.Q.as<double>();
     MatvecFn mv = [&](const double* xi, double* yo, const int* skip) {

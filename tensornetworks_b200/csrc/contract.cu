@@ -64,6 +64,16 @@ __global__ void copy2d_kernel(int rows, int cols, const double* __restrict__ src
     }
 }
 
+// out[e] = sum_s in[s*slab + e]  (deterministic split-K reduction)
+__global__ void slab_sum_kernel(const double* __restrict__ in, int nslab, long long slab, double* __restrict__ out) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < slab;
+         e += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int q = 0; q < nslab; ++q) s += in[(long long)q * slab + e];
+        out[e] = s;
+    }
+}
+
 __global__ void fill_kernel(double* p, long long n, double v) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
          e += (long long)gridDim.x * blockDim.x)
@@ -118,6 +128,32 @@ int copy2d(int rows, int cols, const double* src, IdxMap sr, IdxMap sc, double* 
     return TN_OK;
 }
 
+__global__ void slab_sum_skip_kernel(const double* __restrict__ in, int nslab, long long slab, double* __restrict__ out,
+                                     const int* skip) {
+    if (*skip) return;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < slab;
+         e += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int q = 0; q < nslab; ++q) s += in[(long long)q * slab + e];
+        out[e] = s;
+    }
+}
+
+int slab_sum_skip(const double* in, int nslab, long long slab, double* out, const int* skip, cudaStream_t st) {
+    if (slab <= 0) return TN_OK;
+    slab_sum_skip_kernel<<<grid_for(slab), 256, 0, st>>>(in, nslab, slab, out, skip);
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+int slab_sum(const double* in, int nslab, long long slab, double* out, const int* skip, cudaStream_t st) {
+    if (slab <= 0) return TN_OK;
+    (void)skip;
+    slab_sum_kernel<<<grid_for(slab), 256, 0, st>>>(in, nslab, slab, out);
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
 int fill(double* p, long long n, double v, cudaStream_t st) {
     if (n <= 0) return TN_OK;
     fill_kernel<<<grid_for(n), 256, 0, st>>>(p, n, v);
@@ -148,15 +184,30 @@ int heff_matvec_f64(const ContractShape& s, const WTermDev* termsLR, int nLR, co
     TN_CHECK(gemm_f64(g1, st));
     // Stage 2: Q[m][w2] = sum W P
     TN_CHECK(wcombine(P, Q, termsLR, nLR, blk, skip, st));
-    // Stage 3: y_m = sum_w2 Q[m][w2] G_w2^T   (k = (w2, j2))
+    // Stage 3: y_m = sum_w2 Q[m][w2] G_w2^T, split over w2 for parallelism:
+    // partial P[w2][m] = Q[m][w2] G_w2^T (the stage-1 buffer is free again), then a
+    // deterministic sum over w2.
+    if (Dw2 == 1) {
+        GemmArgs g3;
+        g3.M = D1; g3.N = D2; g3.K = D2; g3.nb0 = d;
+        g3.A.ptr = Q; g3.A.mn = idx(1); g3.A.k = idx(D1); g3.A.sb0 = blk;
+        g3.B.ptr = G; g3.B.mn = idx(1); g3.B.k = idx(D2);
+        g3.C.ptr = y; g3.C.m = idx(1); g3.C.n = idx(D1); g3.C.sb0 = blk;
+        g3.skip = skip;
+        return gemm_f64(g3, st);
+    }
     GemmArgs g3;
-    g3.M = D1; g3.N = D2; g3.K = Dw2 * D2; g3.nb0 = d; g3.nb1 = 1;
-    g3.A.ptr = Q; g3.A.mn = idx(1); g3.A.k = idx2(D1, D2, blk); g3.A.sb0 = (long long)Dw2 * blk;
-    g3.B.ptr = G; g3.B.mn = idx(1); g3.B.k = idx2(D2, D2, (long long)D2 * D2); g3.B.sb0 = 0;
-    g3.C.ptr = y; g3.C.m = idx(1); g3.C.n = idx(D1); g3.C.sb0 = blk;
+    g3.M = D1; g3.N = D2; g3.K = D2; g3.nb0 = Dw2; g3.nb1 = d;
+    g3.A.ptr = Q; g3.A.mn = idx(1); g3.A.k = idx(D1); g3.A.sb0 = blk; g3.A.sb1 = (long long)Dw2 * blk;
+    g3.B.ptr = G; g3.B.mn = idx(1); g3.B.k = idx(D2); g3.B.sb0 = (long long)D2 * D2; g3.B.sb1 = 0;
+    g3.C.ptr = P; g3.C.m = idx(1); g3.C.n = idx(D1); g3.C.sb0 = (long long)d * blk; g3.C.sb1 = blk;
     g3.skip = skip;
     TN_CHECK(gemm_f64(g3, st));
-    return TN_OK;
+    if (skip) {
+        // the reduction must also honour the skip flag
+        return slab_sum_skip(P, Dw2, (long long)d * blk, y, skip, st);
+    }
+    return slab_sum(P, Dw2, (long long)d * blk, y, nullptr, st);
 }
 
 int env_left_f64(const ContractShape& s, const WTermDev* termsLR, int nLR, const double* A, const double* F,
@@ -170,14 +221,20 @@ int env_left_f64(const ContractShape& s, const WTermDev* termsLR, int nLR, const
     g1.C.ptr = P; g1.C.m = idx(1); g1.C.n = idx(D1); g1.C.sb0 = d * blk; g1.C.sb1 = blk;
     TN_CHECK(gemm_f64(g1, st));
     TN_CHECK(wcombine(P, Q, termsLR, nLR, blk, nullptr, st));
-    // F'_w2(i2,j2) = sum_{m,i1} A_m(i1,i2) Q[m][w2](i1,j2)   (k = (m, i1))
+    // F'_w2(i2,j2) = sum_{m,i1} A_m(i1,i2) Q[m][w2](i1,j2), split over m:
+    // partial P[m][w2] = A_m^T Q[m][w2] (D2 x D2), then a sum over m.
     GemmArgs g3;
-    g3.M = D2; g3.N = D2; g3.K = d * D1; g3.nb0 = Dw2;
-    g3.A.ptr = A; g3.A.mn = idx(D1); g3.A.k = idx2(1, D1, blk);
-    g3.B.ptr = Q; g3.B.k = idx2(1, D1, (long long)Dw2 * blk); g3.B.mn = idx(D1); g3.B.sb0 = blk;
-    g3.C.ptr = Fout; g3.C.m = idx(1); g3.C.n = idx(D2); g3.C.sb0 = (long long)D2 * D2;
+    g3.M = D2; g3.N = D2; g3.K = D1; g3.nb0 = d; g3.nb1 = Dw2;
+    g3.A.ptr = A; g3.A.mn = idx(D1); g3.A.k = idx(1); g3.A.sb0 = blk;
+    g3.B.ptr = Q; g3.B.k = idx(1); g3.B.mn = idx(D1); g3.B.sb0 = (long long)Dw2 * blk; g3.B.sb1 = blk;
+    const long long out = (long long)Dw2 * D2 * D2;
+    if (d == 1) {
+        g3.C.ptr = Fout; g3.C.m = idx(1); g3.C.n = idx(D2); g3.C.sb0 = 0; g3.C.sb1 = (long long)D2 * D2;
+        return gemm_f64(g3, st);
+    }
+    g3.C.ptr = P; g3.C.m = idx(1); g3.C.n = idx(D2); g3.C.sb0 = out; g3.C.sb1 = (long long)D2 * D2;
     TN_CHECK(gemm_f64(g3, st));
-    return TN_OK;
+    return slab_sum(P, d, out, Fout, nullptr, st);
 }
 
 int env_right_f64(const ContractShape& s, const WTermDev* termsRL, int nRL, const double* A, const double* G,
@@ -192,14 +249,20 @@ int env_right_f64(const ContractShape& s, const WTermDev* termsRL, int nRL, cons
     g1.C.ptr = P; g1.C.m = idx(1); g1.C.n = idx(D2); g1.C.sb0 = d * blk; g1.C.sb1 = blk;
     TN_CHECK(gemm_f64(g1, st));
     TN_CHECK(wcombine(P, Q, termsRL, nRL, blk, nullptr, st));
-    // G'_w1(i1,j1) = sum_{m,i2} A_m(i1,i2) Q[m][w1](i2,j1)   (k = (m, i2))
+    // G'_w1(i1,j1) = sum_{m,i2} A_m(i1,i2) Q[m][w1](i2,j1), split over m:
+    // partial P[m][w1] = A_m Q[m][w1] (D1 x D1), then a sum over m.
     GemmArgs g3;
-    g3.M = D1; g3.N = D1; g3.K = d * D2; g3.nb0 = Dw1;
-    g3.A.ptr = A; g3.A.mn = idx(1); g3.A.k = idx2(D1, D2, blk);
-    g3.B.ptr = Q; g3.B.k = idx2(1, D2, (long long)Dw1 * blk); g3.B.mn = idx(D2); g3.B.sb0 = blk;
-    g3.C.ptr = Gout; g3.C.m = idx(1); g3.C.n = idx(D1); g3.C.sb0 = (long long)D1 * D1;
+    g3.M = D1; g3.N = D1; g3.K = D2; g3.nb0 = d; g3.nb1 = Dw1;
+    g3.A.ptr = A; g3.A.mn = idx(1); g3.A.k = idx(D1); g3.A.sb0 = blk;
+    g3.B.ptr = Q; g3.B.k = idx(1); g3.B.mn = idx(D2); g3.B.sb0 = (long long)Dw1 * blk; g3.B.sb1 = blk;
+    const long long out = (long long)Dw1 * D1 * D1;
+    if (d == 1) {
+        g3.C.ptr = Gout; g3.C.m = idx(1); g3.C.n = idx(D1); g3.C.sb0 = 0; g3.C.sb1 = (long long)D1 * D1;
+        return gemm_f64(g3, st);
+    }
+    g3.C.ptr = P; g3.C.m = idx(1); g3.C.n = idx(D1); g3.C.sb0 = out; g3.C.sb1 = (long long)D1 * D1;
     TN_CHECK(gemm_f64(g3, st));
-    return TN_OK;
+    return slab_sum(P, d, out, Gout, nullptr, st);
 }
 
 }  // namespace tnb

@@ -21,6 +21,8 @@ int wcombine(const double* P, double* Q, const WTermDev* terms, int nterms, long
 int copy2d(int rows, int cols, const double* src, IdxMap sr, IdxMap sc, double* dst, IdxMap dr, IdxMap dc,
            double scale, cudaStream_t st);
 int fill(double* p, long long n, double v, cudaStream_t st);
+int slab_sum(const double* in, int nslab, long long slab, double* out, const int* skip, cudaStream_t st);
+int slab_sum_skip(const double* in, int nslab, long long slab, double* out, const int* skip, cudaStream_t st);
 int heff_diag(const ContractShape& s, const double* Wdev, const double* F, const double* G, double* diag,
               cudaStream_t st);
 int heff_matvec_f64(const ContractShape& s, const WTermDev* termsLR, int nLR, const double* F, const double* G,
@@ -29,6 +31,13 @@ int env_left_f64(const ContractShape& s, const WTermDev* termsLR, int nLR, const
                  double* Fout, double* P, double* Q, cudaStream_t st);
 int env_right_f64(const ContractShape& s, const WTermDev* termsRL, int nRL, const double* A, const double* G,
                   double* Gout, double* P, double* Q, cudaStream_t st);
+
+// Doubles each of the two contraction scratch buffers (P, Q) must hold.
+inline size_t contract_scratch_doubles(const ContractShape& s) {
+    size_t Dm = (size_t)(s.D1 > s.D2 ? s.D1 : s.D2);
+    size_t Dw = (size_t)(s.Dw1 > s.Dw2 ? s.Dw1 : s.Dw2);
+    return (size_t)s.d * Dw * Dm * Dm;
+}
 
 // Algorithmic flops of one Heff application (dense W, as counted in the
 // measurement plan): 2 d Dw D1 D2 (D1+D2) + 2 d^2 Dw^2 D1 D2, with Dw1/Dw2.

@@ -427,7 +427,7 @@ int MPSState::compute_left_env(int ia) {
     ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
     size_t need = sizeof(double) * (size_t)op.Dw2 * D2[ia] * D2[ia];
     TN_CHECK(Lenv[ia]->ensure(need));
-    size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(ctx->P.ensure(scr));
     TN_CHECK(ctx->Q.ensure(scr));
     const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;
@@ -443,7 +443,7 @@ int MPSState::compute_right_env(int ia) {
     ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
     size_t need = sizeof(double) * (size_t)op.Dw1 * D1[ia] * D1[ia];
     TN_CHECK(Renv[ia]->ensure(need));
-    size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(ctx->P.ensure(scr));
     TN_CHECK(ctx->Q.ensure(scr));
     const WTermDev* t = H->terms.as<WTermDev>() + op.offRL;
@@ -466,12 +466,77 @@ int MPSState::load_heff_caches() {
     return TN_OK;
 }
 
+// Split-precision site solve: Lanczos on the BF16-split tcgen05 operator
+// (shifted by the mean block energies), then one FP64 matvec for the Rayleigh
+// quotient (the site energy) and the FP64 residual; an FP64 Lanczos
+// continuation follows when that residual exceeds opt.refine_tol.
+int MPSState::refine_site_mixed(int ia, double epsEigen) {
+    const SiteMPO& op = H->ops[ia];
+    ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+    const long long N = (long long)d * D1[ia] * D2[ia];
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
+    TN_CHECK(ctx->P.ensure(scr));
+    TN_CHECK(ctx->Q.ensure(scr));
+    TN_CHECK(yvec.ensure(sizeof(double) * (size_t)N));
+    const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;
+    const double* F = Lenv[ia - 1]->as<double>();
+    const double* G = Renv[ia + 1]->as<double>();
+    double* P = ctx->P.as<double>();
+    double* Q = ctx->Q.as<double>();
+    cudaStream_t st = ctx->stream;
+    const int ns = opt.precision == TN_PREC_MIXED_HI ? 3 : 2;
+    // channels carrying the completed block energy (lower form: left 0, right Dw-1)
+    const int wF = H->form == TN_FORM_REGULAR_LOWER ? 0 : op.Dw1 - 1;
+    const int wG = H->form == TN_FORM_REGULAR_LOWER ? op.Dw2 - 1 : 0;
+    TN_CHECK(mixed_prepare_site(*ctx, msite, s, t, op.nLR, F, G, wF, wG, ns));
+    MatvecFn mvm = [&](const double* x, double* y, const int* skip) {
+        return heff_matvec_mixed(*ctx, msite, x, y, skip);
+    };
+    int krylov = opt.krylov > 0 ? opt.krylov : 20;
+    int restarts = opt.max_restarts > 0 ? opt.max_restarts : 10;
+    double tolm = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-6);
+    tolm = std::max(tolm, epsEigen);
+    LzResult rm{};
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, tolm, mvm, &rm));
+    TN_CHECK(mixed_check_error(msite, st));
+    matvecs += rm.matvecs;
+    heff_flop += heff_flops(s) * rm.matvecs;
+    // FP64 Rayleigh quotient and residual of the Ritz vector
+    TN_CHECK(heff_matvec_f64(s, t, op.nLR, F, G, A[ia]->as<double>(), yvec.as<double>(), P, Q, nullptr, st));
+    double theta = 0, resid = 0;
+    TN_CHECK(rayleigh_residual(*ctx, N, A[ia]->as<double>(), yvec.as<double>(), &theta, &resid));
+    matvecs += 1;
+    matvecs_fp64 += 1;
+    heff_flop += heff_flops(s);
+    double theta2 = theta + (rm.theta2 - rm.theta);
+    if (opt.refine_tol > 0 && resid > opt.refine_tol) {
+        MatvecFn mv = [&](const double* x, double* y, const int* skip) {
+            return heff_matvec_f64(s, t, op.nLR, F, G, x, y, P, Q, skip, st);
+        };
+        LzResult r{};
+        TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, std::max(epsEigen, opt.refine_tol * 1e-3),
+                               mv, &r));
+        matvecs += r.matvecs;
+        matvecs_fp64 += r.matvecs;
+        heff_flop += heff_flops(s) * r.matvecs;
+        theta = r.theta;
+        theta2 = r.theta2;
+        ++fallbacks;
+    }
+    if (!rm.converged) ++not_converged;
+    iterDE[ia] = theta - Emin[ia];
+    Emin[ia] = theta;
+    gapE[ia] = theta2 - theta;
+    return TN_OK;
+}
+
 // MPSSite::Refine (MPSSite_Variational.C:18-44) with the device eigensolver.
 int MPSState::refine_site(int ia, double epsEigen) {
     const SiteMPO& op = H->ops[ia];
     ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+    if (opt.precision != TN_PREC_FP64 && mixed_supported(s)) return refine_site_mixed(ia, epsEigen);
     const long long N = (long long)d * D1[ia] * D2[ia];
-    size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(ctx->P.ensure(scr));
     TN_CHECK(ctx->Q.ensure(scr));
     const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;
@@ -565,7 +630,7 @@ int MPSState::expectation(const std::vector<SiteMPO>& ops, double* E) {
         const SiteMPO& op = ops[ia];
         ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
         TN_CHECK(nxt->ensure(sizeof(double) * (size_t)op.Dw2 * D2[ia] * D2[ia]));
-        size_t scr = sizeof(double) * (size_t)d * std::max(op.Dw1, op.Dw2) * D1[ia] * D2[ia];
+        size_t scr = sizeof(double) * contract_scratch_doubles(s);
         TN_CHECK(ctx->P.ensure(scr));
         TN_CHECK(ctx->Q.ensure(scr));
         const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;

@@ -5,6 +5,7 @@
 
 #include "contract.h"
 #include "lanczos.h"
+#include "mixed.h"
 #include "qr.h"
 
 namespace tnb {
@@ -43,7 +44,8 @@ struct MPSState {
     std::vector<int> bondK;                   // current bond dimension (Bond::GetD)
     std::vector<char> bondDirty;
     std::vector<double> Emin, iterDE, gapE;
-    DevBuf tmp, Wqr, Qqr, svdw, envA, envB;
+    DevBuf tmp, Wqr, Qqr, svdw, envA, envB, yvec;
+    MixedSite msite;
     long long matvecs = 0, matvecs_fp64 = 0;
     double heff_flop = 0;
     int not_converged = 0, fallbacks = 0;
@@ -61,6 +63,7 @@ struct MPSState {
     int compute_right_env(int ia);
     int load_heff_caches();
     int refine_site(int ia, double epsEigen);
+    int refine_site_mixed(int ia, double epsEigen);
     int sweep(bool left, double epsEigen);
     int increase_bond_dims(int D);
     int expectation(const std::vector<SiteMPO>& ops, double* E);

@@ -381,6 +381,66 @@ __global__ void lz_ritz_vector_kernel(const double* __restrict__ V, double* __re
     }
 }
 
+// Rayleigh quotient theta = x.y / x.x and residual |y - theta x| / |x|.
+__global__ void rq_dots_kernel(const double* __restrict__ x, const double* __restrict__ y, long long N,
+                               double* partial, LzState* st) {
+    __shared__ double sh[KCHUNK * 32];
+    __shared__ double res[KCHUNK];
+    __shared__ bool last;
+    double v[KCHUNK] = {0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        double a = x[i];
+        v[0] = fma(a, y[i], v[0]);
+        v[1] = fma(a, a, v[1]);
+    }
+    block_sum_chunk(v, res, sh);
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = res[0];
+        partial[2 * blockIdx.x + 1] = res[1];
+        __threadfence();
+        unsigned int prev = atomicAdd(&st->counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        double xy = 0, xx = 0;
+        for (int b = 0; b < (int)gridDim.x; ++b) {
+            xy += __ldcg(partial + 2 * b);
+            xx += __ldcg(partial + 2 * b + 1);
+        }
+        st->theta = xx > 0 ? xy / xx : 0.0;
+        st->xnorm = sqrt(xx);
+        st->counter = 0;
+    }
+}
+
+__global__ void rq_resid_kernel(const double* __restrict__ x, const double* __restrict__ y, long long N,
+                                double* partial, LzState* st) {
+    __shared__ double sh[KCHUNK * 32];
+    __shared__ double res[KCHUNK];
+    __shared__ bool last;
+    const double th = st->theta;
+    double v[KCHUNK] = {0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        double r = y[i] - th * x[i];
+        v[0] = fma(r, r, v[0]);
+    }
+    block_sum_chunk(v, res, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = res[0];
+        __threadfence();
+        unsigned int prev = atomicAdd(&st->counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        double s = 0;
+        for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + b);
+        st->resid = st->xnorm > 0 ? sqrt(s) / st->xnorm : 0.0;
+        st->counter = 0;
+    }
+}
+
 inline int vec_grid(long long N, int sm) {
     long long b = (N + LZ_THREADS - 1) / LZ_THREADS;
     long long cap = (long long)sm * 2;
@@ -460,6 +520,26 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         set_error("lanczos: non-finite Ritz value");
         return TN_NAN_DETECTED;
     }
+    return TN_OK;
+}
+
+int rayleigh_residual(Ctx& c, long long N, const double* x, const double* y, double* theta, double* resid) {
+    cudaStream_t st = c.stream;
+    const int grid = vec_grid(N, c.sm_count);
+    TN_CHECK(c.rq.ensure(sizeof(double) * (2 * (size_t)grid + 8) + sizeof(LzState)));
+    LzState* s = reinterpret_cast<LzState*>(c.rq.p);
+    double* partial = reinterpret_cast<double*>(c.rq.as<char>() + sizeof(LzState));
+    TN_CHECK(c.pinned.ensure(sizeof(LzState)));
+    TN_CUDA_CHECK(cudaMemsetAsync(&s->counter, 0, sizeof(unsigned int), st));
+    rq_dots_kernel<<<grid, LZ_THREADS, 0, st>>>(x, y, N, partial, s);
+    TN_LAUNCH_CHECK();
+    rq_resid_kernel<<<grid, LZ_THREADS, 0, st>>>(x, y, N, partial, s);
+    TN_LAUNCH_CHECK();
+    LzState* hs = reinterpret_cast<LzState*>(c.pinned.p);
+    TN_CUDA_CHECK(cudaMemcpyAsync(hs, s, sizeof(LzState), cudaMemcpyDeviceToHost, st));
+    TN_CUDA_CHECK(cudaStreamSynchronize(st));
+    *theta = hs->theta;
+    *resid = hs->resid;
     return TN_OK;
 }
 

@@ -30,6 +30,9 @@ struct LzResult {
 // do nothing when *skip != 0 (device flag).
 using MatvecFn = std::function<int(const double*, double*, const int*)>;
 
+// theta = x.y/x.x and |y - theta x|/|x| (device vectors; synchronises).
+int rayleigh_residual(Ctx& c, long long N, const double* x, const double* y, double* theta, double* resid);
+
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
                   LzResult* out);
 

@@ -111,19 +111,26 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(double* __restrict
         if (lane == 0) G[c * b + r] = s;
     }
     __syncthreads();
-    // T (dlarft, forward, columnwise): T(jj,jj)=tau_jj, T(0:jj,jj) = -tau_jj T(0:jj,0:jj) G(0:jj,jj)
+    // T (dlarft, forward, columnwise): T(jj,jj)=tau_jj, T(0:jj,jj) = -tau_jj T(0:jj,0:jj) G(0:jj,jj).
+    // Row i of T depends only on row i, so thread i builds it in shared memory.
+    __shared__ double Ts[32 * 32];
     if (tid < b) {
         const int i = tid;
         for (int jj = 0; jj < b; ++jj) {
             double v;
             if (i < jj) {
                 double s = 0;
-                for (int l = i; l < jj; ++l) s = fma(T[(size_t)l * ldt + i], G[jj * b + l], s);
+                for (int l = i; l < jj; ++l) s = fma(Ts[l * 32 + i], G[jj * b + l], s);
                 v = -tau[jj] * s;
             } else if (i == jj) v = tau[jj];
             else v = 0.0;
-            T[(size_t)jj * ldt + i] = v;
+            Ts[jj * 32 + i] = v;
         }
+    }
+    __syncthreads();
+    for (int e = tid; e < b * b; e += blockDim.x) {
+        int i = e % b, jj = e / b;
+        T[(size_t)jj * ldt + i] = Ts[jj * 32 + i];
     }
 }
 

@@ -115,6 +115,7 @@ struct Ctx {
     DevBuf P, Q;           // contraction intermediates
     DevBuf lz;             // Lanczos basis + work vectors
     DevBuf lzstate;        // Lanczos device state
+    DevBuf rq;             // Rayleigh-quotient state + partials
     DevBuf qrw;            // QR workspace
     DevBuf svdw;           // SVD workspace
     DevBuf wterms;         // MPO term lists
