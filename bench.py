@@ -146,8 +146,10 @@ def heff_flops(d, Dw1, Dw2, D1, D2):
 
 
 def matvec_microbench(T, ctx, torch, D, precision, reps=50):
-    """Average device time of one bulk Heff application at D x D (d=2, Dw=5) on the
-    library's launch stream (set to torch's current stream so torch events see it)."""
+    """Average device time of one bulk Heff application at D x D (d=2, Dw=5) through
+    the operator handle, on a torch stream that the library launches on, so that the
+    torch events bracket exactly these launches."""
+    import ctypes as C
     import numpy as np
     lib = ctx._lib
     H = T.Factory(ctx).Make1D_NN_HeisenbergHamiltonian(10, 0.5, T.RegularLower, 1.0, 1.0, 0.0)
@@ -158,22 +160,26 @@ def matvec_microbench(T, ctx, torch, D, precision, reps=50):
     G = torch.rand(Dw * D * D, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
     x = torch.rand(d * D * D, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
     y = torch.empty_like(x)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a real (non-default) stream shared by the library and the events
+    torch.cuda.synchronize()
     lib.tn_ctx_set_stream(ctx.handle, stream.cuda_stream)
     try:
+      with torch.cuda.stream(stream):
         prec = {"fp64": 0, "mixed": 1, "mixed_hi": 2}[precision]
+        h = C.c_void_p()
+        T._capi.check(lib.tn_heff_create(ctx.handle, prec, d, Dw, Dw, D, D, W.ctypes.data, F.data_ptr(),
+                                         G.data_ptr(), C.byref(h)), "tn_heff_create")
         for _ in range(5):
-            T._capi.check(lib.tn_heff_matvec(ctx.handle, prec, d, Dw, Dw, D, D, W.ctypes.data, F.data_ptr(),
-                                             G.data_ptr(), x.data_ptr(), y.data_ptr()), "matvec")
+            T._capi.check(lib.tn_heff_apply(h, x.data_ptr(), y.data_ptr()), "tn_heff_apply")
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
+        s.record(stream)
         for _ in range(reps):
-            lib.tn_heff_matvec(ctx.handle, prec, d, Dw, Dw, D, D, W.ctypes.data, F.data_ptr(), G.data_ptr(),
-                               x.data_ptr(), y.data_ptr())
-        e.record()
+            T._capi.check(lib.tn_heff_apply(h, x.data_ptr(), y.data_ptr()), "tn_heff_apply")
+        e.record(stream)
         e.synchronize()
         t = s.elapsed_time(e) / 1e3 / reps
+        T._capi.check(lib.tn_heff_destroy(h), "tn_heff_destroy")
     finally:
         lib.tn_ctx_set_stream(ctx.handle, None)
     return t, heff_flops(d, Dw, Dw, D, D)

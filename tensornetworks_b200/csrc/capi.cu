@@ -319,7 +319,7 @@ int tn_mps_find_variational_ground_state(tn_mps m, tn_hamiltonian h, const tn_sc
             set_error("schedule line %d invalid", i);
             return TN_BAD_ARG;
         }
-    if (opt && opt->precision != TN_PREC_FP64 && opt->precision != TN_PREC_MIXED) return TN_BAD_ARG;
+    if (opt && (opt->precision < TN_PREC_FP64 || opt->precision > TN_PREC_MIXED_HI)) return TN_BAD_ARG;
     m->m.H = &h->h;
     tn_sweep_stats st{};
     TN_CHECK(m->m.find_ground_state(lines, nlines, opt, &st));

@@ -17,6 +17,7 @@
 //   * the eigensolver is matrix-free (Lanczos/Davidson) instead of a dense
 //     zheevx on the materialised Heff.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -564,20 +565,35 @@ int MPSState::refine_site(int ia, double epsEigen) {
 
 // MPSImp::Sweep / MPSImp::Refine (MPSImp_Variational.C:64-99).
 int MPSState::sweep(bool left, double epsEigen) {
-    if (left) {
-        for (int ia = 1; ia <= L; ++ia) {
-            TN_CHECK(refine_site(ia, epsEigen));
-            TN_CHECK(normalize_site(ia, true));
-            if (ia < L) TN_CHECK(compute_left_env(ia));
-        }
-    } else {
-        for (int ia = L; ia >= 1; --ia) {
-            TN_CHECK(refine_site(ia, epsEigen));
-            TN_CHECK(normalize_site(ia, false));
-            if (ia > 1) TN_CHECK(compute_right_env(ia));
+    const bool prof = opt.verbose >= 2;
+    auto now = [&]() {
+        if (prof) cudaStreamSynchronize(ctx->stream);
+        return std::chrono::steady_clock::now();
+    };
+    auto secs = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+        return std::chrono::duration<double>(b - a).count();
+    };
+    for (int step = 0; step < L; ++step) {
+        const int ia = left ? 1 + step : L - step;
+        auto t0 = now();
+        TN_CHECK(refine_site(ia, epsEigen));
+        auto t1 = now();
+        TN_CHECK(normalize_site(ia, left));
+        auto t2 = now();
+        if (left && ia < L) TN_CHECK(compute_left_env(ia));
+        if (!left && ia > 1) TN_CHECK(compute_right_env(ia));
+        auto t3 = now();
+        if (prof) {
+            t_refine += secs(t0, t1);
+            t_gauge += secs(t1, t2);
+            t_env += secs(t2, t3);
         }
     }
-    return bond_values_update(false);
+    auto b0 = now();
+    TN_CHECK(bond_values_update(false));
+    auto b1 = now();
+    if (prof) t_bond += secs(b0, b1);
+    return TN_OK;
 }
 
 // MPSImp::IncreaseBondDimensions (MPSImp.C:123-147) with Bond::NewBondDimension (Bond.C:60-84).
@@ -652,6 +668,7 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
     matvecs = matvecs_fp64 = 0;
     heff_flop = 0;
     not_converged = fallbacks = 0;
+    t_refine = t_gauge = t_env = t_bond = 0;
     TN_CUDA_CHECK(cudaEventRecord(ctx->ev_a, st));
     double dE = 0, dl = 0;
     for (int in = 0; in < nsweeps; ++in) {
@@ -666,6 +683,9 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
     TN_CUDA_CHECK(cudaEventSynchronize(ctx->ev_b));
     float ms = 0;
     TN_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b));
+    if (opt.verbose >= 2)
+        std::printf("phase seconds: refine %.4f gauge %.4f env %.4f bond-values %.4f (matvecs %lld, fp64 %lld)\n",
+                    t_refine, t_gauge, t_env, t_bond, matvecs, matvecs_fp64);
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         double e = 0;

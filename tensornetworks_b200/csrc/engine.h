@@ -50,6 +50,8 @@ struct MPSState {
     double heff_flop = 0;
     int not_converged = 0, fallbacks = 0;
     tn_solver_options opt{};
+    // phase timing (verbose >= 2): seconds in refine / gauge / environment / bond values
+    double t_refine = 0, t_gauge = 0, t_env = 0, t_bond = 0;
 
     ~MPSState();
     int init(Hamiltonian* h, int D);

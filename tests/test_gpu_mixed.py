@@ -2,7 +2,8 @@
 
 Tolerances (normwise relative error of Heff x, random environments):
   MIXED    (2 BF16 pieces, 3 products):  <= 2e-4
-  MIXED_HI (3 BF16 pieces, 6 products):  <= 5e-6
+  MIXED_HI (3 BF16 pieces, 6 products):  <= 2e-5 (FP32 accumulation and FP32
+                                         stage-2 intermediates set this floor)
 """
 import ctypes as C
 
@@ -11,7 +12,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL = {1: 2e-4, 2: 5e-6}
+TOL = {1: 2e-4, 2: 2e-5}
 
 
 @pytest.fixture(scope="module")
