@@ -88,7 +88,8 @@ typedef struct {
     int use_learned;     /* 1: learned preconditioner (Davidson only)      */
     int verbose;         /* 1: print the reference's per-sweep log line     */
     double mixed_tol;    /* residual target of the split-precision Krylov
-                            phase (0: 1e-6 for MIXED, 1e-9 for MIXED_HI)   */
+                            phase relative to the norm of its tridiagonal
+                            matrix (0: 3e-5 for MIXED, 2e-6 for MIXED_HI) */
     double refine_tol;   /* FP64 residual above which an FP64 Lanczos
                             continuation follows the split-precision solve
                             (0: never; the FP64 Rayleigh quotient always

@@ -282,6 +282,7 @@ int tn_mps_set_site(tn_mps m, int site, int D1, int D2, const double* A) {
 
 int tn_mps_get_bond(tn_mps m, int bond, int* D, double* s_host) {
     if (!m || bond < 1 || bond >= m->m.L) return TN_BAD_ARG;
+    TN_CHECK(m->m.ensure_bond_values());
     const auto& s = m->m.bond_s[bond];
     if (D) *D = (int)s.size();
     if (s_host) std::memcpy(s_host, s.data(), sizeof(double) * s.size());

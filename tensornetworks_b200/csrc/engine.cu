@@ -180,7 +180,8 @@ MPSState::~MPSState() {
     for (auto p : A) delete p;
     for (auto p : Lenv) delete p;
     for (auto p : Renv) delete p;
-    for (auto p : bondR) delete p;
+    for (int q = 0; q < 2; ++q)
+        for (auto p : bondR[q]) delete p;
 }
 
 // MPSImp::InitSitesAndBonds (MPSImp.C:69-90); Bond ctor fills s = 1/D (Bond.C:11-25).
@@ -198,18 +199,26 @@ int MPSState::init(Hamiltonian* h, int D) {
     A.assign(L + 2, nullptr);
     Lenv.assign(L + 2, nullptr);
     Renv.assign(L + 2, nullptr);
-    bondR.assign(L + 1, nullptr);
+    for (int q = 0; q < 2; ++q) {
+        bondR[q].assign(L + 1, nullptr);
+        bondRm[q].assign(L + 1, 0);
+        bondRn[q].assign(L + 1, 0);
+        bondHave[q].assign(L + 1, 0);
+    }
+    bondLatest.assign(L + 1, -1);
     for (int i = 0; i <= L + 1; ++i) {
         A[i] = new DevBuf();
         Lenv[i] = new DevBuf();
         Renv[i] = new DevBuf();
-        if (i <= L) bondR[i] = new DevBuf();
+        if (i <= L) {
+            bondR[0][i] = new DevBuf();
+            bondR[1][i] = new DevBuf();
+        }
     }
     LenvDw.assign(L + 2, 1); LenvD.assign(L + 2, 1);
     RenvDw.assign(L + 2, 1); RenvD.assign(L + 2, 1);
     bond_s.assign(L + 1, std::vector<double>());
     bond_maxDelta.assign(L + 1, 0.0);
-    bondRm.assign(L + 1, 0); bondRn.assign(L + 1, 0);
     bondK.assign(L + 1, D);
     bondDirty.assign(L + 1, 0);
     for (int b = 1; b < L; ++b) bond_s[b].assign(D, 1.0 / D);
@@ -320,10 +329,11 @@ int MPSState::normalize_site(int ia, bool left) {
         const int m = d * a1, n = a2, k = std::min(m, n);
         TN_CHECK(Wqr.ensure(sizeof(double) * (size_t)m * n));
         TN_CHECK(Qqr.ensure(sizeof(double) * (size_t)m * k));
-        TN_CHECK(bondR[ia]->ensure(sizeof(double) * (size_t)k * n));
+        DevBuf* Rb = bondR[0][ia];
+        TN_CHECK(Rb->ensure(sizeof(double) * (size_t)k * n));
         // W(r=(n_,i1), c=i2) = A(n_,i1,i2)
         TN_CHECK(copy2d(m, n, Aia, idx2(1, a1, blk), idx(a1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
-        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, bondR[ia]->as<double>(), k));
+        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, Rb->as<double>(), k));
         // site := Q with D2 = k
         TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(1, a1, (long long)a1 * k), idx(a1), 1.0, st));
         D2[ia] = k;
@@ -332,23 +342,25 @@ int MPSState::normalize_site(int ia, bool left) {
         TN_CHECK(tmp.ensure(sizeof(double) * (size_t)d * k * nb2));
         GemmArgs g;
         g.M = k; g.N = nb2; g.K = nb1; g.nb0 = d;
-        g.A.ptr = bondR[ia]->as<double>(); g.A.mn = idx(1); g.A.k = idx(k);
+        g.A.ptr = Rb->as<double>(); g.A.mn = idx(1); g.A.k = idx(k);
         g.B.ptr = A[ia + 1]->as<double>(); g.B.k = idx(1); g.B.mn = idx(nb1); g.B.sb0 = (long long)nb1 * nb2;
         g.C.ptr = tmp.as<double>(); g.C.m = idx(1); g.C.n = idx(k); g.C.sb0 = (long long)k * nb2;
         TN_CHECK(gemm_f64(g, st));
         TN_CUDA_CHECK(cudaMemcpyAsync(A[ia + 1]->p, tmp.p, sizeof(double) * (size_t)d * k * nb2,
                                       cudaMemcpyDeviceToDevice, st));
         D1[ia + 1] = k;
-        bondRm[ia] = k; bondRn[ia] = n; bondDirty[ia] = 1; bondK[ia] = k;
+        bondRm[0][ia] = k; bondRn[0][ia] = n; bondHave[0][ia] = 1; bondLatest[ia] = 0;
+        bondDirty[ia] = 1; bondK[ia] = k;
     } else {
         // LQ of the D1 x (d*D2) matrix as QR of its transpose (m = d*D2 rows, n = D1 cols)
         const int m = d * a2, n = a1, k = std::min(m, n);
         TN_CHECK(Wqr.ensure(sizeof(double) * (size_t)m * n));
         TN_CHECK(Qqr.ensure(sizeof(double) * (size_t)m * k));
-        TN_CHECK(bondR[ia - 1]->ensure(sizeof(double) * (size_t)k * n));
+        DevBuf* Rb = bondR[1][ia - 1];
+        TN_CHECK(Rb->ensure(sizeof(double) * (size_t)k * n));
         // W(r=(n_,i2), c=i1) = A(n_,i1,i2)
         TN_CHECK(copy2d(m, n, Aia, idx2(a1, a2, blk), idx(1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
-        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, bondR[ia - 1]->as<double>(), k));
+        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, Rb->as<double>(), k));
         // site := Q^T with D1 = k: element (n_, i1', i2) = Q(n_*D2+i2, i1')
         TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(k, a2, (long long)k * a2), idx(1), 1.0, st));
         D1[ia] = k;
@@ -358,40 +370,41 @@ int MPSState::normalize_site(int ia, bool left) {
         GemmArgs g;
         g.M = pb1; g.N = k; g.K = pb2; g.nb0 = d;
         g.A.ptr = A[ia - 1]->as<double>(); g.A.mn = idx(1); g.A.k = idx(pb1); g.A.sb0 = (long long)pb1 * pb2;
-        g.B.ptr = bondR[ia - 1]->as<double>(); g.B.k = idx(k); g.B.mn = idx(1);
+        g.B.ptr = Rb->as<double>(); g.B.k = idx(k); g.B.mn = idx(1);
         g.C.ptr = tmp.as<double>(); g.C.m = idx(1); g.C.n = idx(pb1); g.C.sb0 = (long long)pb1 * k;
         TN_CHECK(gemm_f64(g, st));
         TN_CUDA_CHECK(cudaMemcpyAsync(A[ia - 1]->p, tmp.p, sizeof(double) * (size_t)d * pb1 * k,
                                       cudaMemcpyDeviceToDevice, st));
         D2[ia - 1] = k;
-        bondRm[ia - 1] = k; bondRn[ia - 1] = n; bondDirty[ia - 1] = 1; bondK[ia - 1] = k;
+        bondRm[1][ia - 1] = k; bondRn[1][ia - 1] = n; bondHave[1][ia - 1] = 1; bondLatest[ia - 1] = 1;
+        bondDirty[ia - 1] = 1; bondK[ia - 1] = k;
     }
     return TN_OK;
 }
 
-// Singular values of every bond normalised since the last call, in one
-// batched Jacobi launch, then Bond::SetSingularValues (Bond.C:86-106).
-int MPSState::bond_values_update(bool initial) {
-    std::vector<int> bonds;
+// Singular values (descending, un-normalised) of the stored triangular factors
+// (dir, bond) in `which`, in one batched Jacobi launch.
+int MPSState::bond_values(const std::vector<std::pair<int, int>>& which, std::vector<std::vector<double>>& out) {
+    out.assign(which.size(), std::vector<double>());
+    if (which.empty()) return TN_OK;
     size_t total = 0;
-    for (int b = 1; b < L; ++b)
-        if (bondDirty[b]) {
-            bonds.push_back(b);
-            total += (size_t)bondRm[b] * bondRn[b] + std::min(bondRm[b], bondRn[b]);
-        }
-    if (bonds.empty()) return TN_OK;
+    for (auto& w : which) {
+        int r = bondRm[w.first][w.second], c = bondRn[w.first][w.second];
+        total += (size_t)r * c + std::min(r, c);
+    }
     TN_CHECK(svdw.ensure(sizeof(double) * total));
     std::vector<SvdJob> jobs;
     std::vector<size_t> soff;
     size_t off = 0;
-    for (int b : bonds) {
-        int r = bondRm[b], c = bondRn[b];
+    for (auto& w : which) {
+        int r = bondRm[w.first][w.second], c = bondRn[w.first][w.second];
         int tm = std::max(r, c), tn = std::min(r, c);
         double* Wb = svdw.as<double>() + off;
+        const double* R = bondR[w.first][w.second]->as<double>();
         if (r >= c)
-            TN_CHECK(copy2d(r, c, bondR[b]->as<double>(), idx(1), idx(r), Wb, idx(1), idx(r), 1.0, ctx->stream));
+            TN_CHECK(copy2d(r, c, R, idx(1), idx(r), Wb, idx(1), idx(r), 1.0, ctx->stream));
         else
-            TN_CHECK(copy2d(r, c, bondR[b]->as<double>(), idx(1), idx(r), Wb, idx(c), idx(1), 1.0, ctx->stream));
+            TN_CHECK(copy2d(r, c, R, idx(1), idx(r), Wb, idx(c), idx(1), 1.0, ctx->stream));
         off += (size_t)tm * tn;
         SvdJob j{};
         j.W = Wb; j.m = tm; j.n = tn; j.s = svdw.as<double>() + off;
@@ -402,14 +415,30 @@ int MPSState::bond_values_update(bool initial) {
     TN_CHECK(svd_batched(*ctx, jobs, false));
     std::vector<double> hs(total);
     TN_CUDA_CHECK(cudaMemcpy(hs.data(), svdw.p, sizeof(double) * total, cudaMemcpyDeviceToHost));
-    for (size_t q = 0; q < bonds.size(); ++q) {
-        int b = bonds[q];
-        int k = jobs[q].n;
-        std::vector<double> s(hs.begin() + soff[q], hs.begin() + soff[q] + k);
-        double nrm = 0;
-        for (double v : s) nrm += v * v;
-        nrm = std::sqrt(nrm);
-        for (double& v : s) v = nrm > 0 ? v / nrm : 0.0;
+    for (size_t q = 0; q < which.size(); ++q)
+        out[q].assign(hs.begin() + soff[q], hs.begin() + soff[q] + jobs[q].n);
+    return TN_OK;
+}
+
+static std::vector<double> normalised(std::vector<double> s) {
+    double nrm = 0;
+    for (double v : s) nrm += v * v;
+    nrm = std::sqrt(nrm);
+    for (double& v : s) v = nrm > 0 ? v / nrm : 0.0;
+    return s;
+}
+
+// Bond::SetSingularValues (Bond.C:86-106) for every bond whose latest factor
+// has not been evaluated yet; maxDelta against the previously stored values.
+int MPSState::ensure_bond_values() {
+    std::vector<std::pair<int, int>> which;
+    for (int b = 1; b < L; ++b)
+        if (bondDirty[b] && bondLatest[b] >= 0) which.push_back({bondLatest[b], b});
+    std::vector<std::vector<double>> vals;
+    TN_CHECK(bond_values(which, vals));
+    for (size_t q = 0; q < which.size(); ++q) {
+        int b = which[q].second;
+        std::vector<double> s = normalised(vals[q]);
         std::vector<double> old = bond_s[b];
         old.resize(s.size(), 0.0);
         double md = 0;
@@ -419,7 +448,35 @@ int MPSState::bond_values_update(bool initial) {
         bondK[b] = (int)s.size();
         bondDirty[b] = 0;
     }
-    (void)initial;
+    return TN_OK;
+}
+
+// MPSImp::GetMaxDeltal (MPSImp_Variational.C:162-173) after a sweep pair: every
+// bond was last set by the right-to-left half-sweep and before that by the
+// left-to-right one, so maxDelta compares the singular values of those two factors.
+int MPSState::sweep_pair_dlambda(double* dl) {
+    std::vector<std::pair<int, int>> which;
+    for (int b = 1; b < L; ++b)
+        if (bondHave[0][b] && bondHave[1][b]) {
+            which.push_back({0, b});
+            which.push_back({1, b});
+        }
+    std::vector<std::vector<double>> vals;
+    TN_CHECK(bond_values(which, vals));
+    double m = 0;
+    for (size_t q = 0; q + 1 < which.size(); q += 2) {
+        int b = which[q].second;
+        std::vector<double> sl = normalised(vals[q]), sr = normalised(vals[q + 1]);
+        sl.resize(sr.size(), 0.0);
+        double md = 0;
+        for (size_t i = 0; i < sr.size(); ++i) md = std::max(md, std::fabs(sr[i] - sl[i]));
+        bond_maxDelta[b] = md;
+        bond_s[b] = sr;
+        bondK[b] = (int)sr.size();
+        bondDirty[b] = 0;
+        m = std::max(m, md);
+    }
+    *dl = m;
     return TN_OK;
 }
 
@@ -458,7 +515,7 @@ int MPSState::compute_right_env(int ia) {
 int MPSState::normalize_all(bool left) {
     if (left) for (int ia = 1; ia <= L; ++ia) TN_CHECK(normalize_site(ia, true));
     else for (int ia = L; ia >= 1; --ia) TN_CHECK(normalize_site(ia, false));
-    return bond_values_update(true);
+    return TN_OK;
 }
 
 // MPSImp::LoadHeffCaches -> CalcHeffRight (MPSImp_Variational.C:120-149).
@@ -495,10 +552,11 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     };
     int krylov = opt.krylov > 0 ? opt.krylov : 20;
     int restarts = opt.max_restarts > 0 ? opt.max_restarts : 10;
-    double tolm = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-6);
-    tolm = std::max(tolm, epsEigen);
+    // residual target: the requested tolerance, but not below the split operator's
+    // noise floor relative to |T| (BF16x3 ~ 2^-16, BF16x6 ~ FP32 accumulation)
+    const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 2e-6 : 3e-5);
     LzResult rm{};
-    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, tolm, mvm, &rm));
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel));
     TN_CHECK(mixed_check_error(msite, st));
     matvecs += rm.matvecs;
     heff_flop += heff_flops(s) * rm.matvecs;
@@ -589,10 +647,6 @@ int MPSState::sweep(bool left, double epsEigen) {
             t_env += secs(t2, t3);
         }
     }
-    auto b0 = now();
-    TN_CHECK(bond_values_update(false));
-    auto b1 = now();
-    if (prof) t_bond += secs(b0, b1);
     return TN_OK;
 }
 
@@ -676,8 +730,7 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
         TN_CHECK(sweep(false, epsEigen));
         dE = 0;
         for (int ia = 1; ia <= L; ++ia) dE = std::max(dE, std::fabs(iterDE[ia]));
-        dl = 0;
-        for (int b = 1; b < L; ++b) dl = std::max(dl, bond_maxDelta[b]);
+        dl = -1;  // not evaluated (no convergence test here)
     }
     TN_CUDA_CHECK(cudaEventRecord(ctx->ev_b, st));
     TN_CUDA_CHECK(cudaEventSynchronize(ctx->ev_b));
@@ -741,8 +794,13 @@ int MPSState::find_ground_state(const tn_sched_line* lines, int nlines, const tn
                 ++total;
                 dE = 0;
                 for (int ia = 1; ia <= L; ++ia) dE = std::max(dE, std::fabs(iterDE[ia]));
-                dl = 0;
-                for (int b = 1; b < L; ++b) dl = std::max(dl, bond_maxDelta[b]);
+                // dE < eps_E && dl < eps_lambda: dl is only needed when the first test holds
+                dl = -1;
+                if (dE < isl.eps_energy || opt.verbose) {
+                    auto b0 = std::chrono::steady_clock::now();
+                    TN_CHECK(sweep_pair_dlambda(&dl));
+                    t_bond += std::chrono::duration<double>(std::chrono::steady_clock::now() - b0).count();
+                }
                 if (opt.verbose) std::printf("%4d %4d %.1e %.1e\n", in, D, dE, dl);
                 if (dE < isl.eps_energy && dl < isl.eps_lambda) break;
             }

@@ -39,10 +39,17 @@ struct MPSState {
     std::vector<int> LenvDw, LenvD, RenvDw, RenvD;
     std::vector<std::vector<double>> bond_s;  // 1..L-1, normalised
     std::vector<double> bond_maxDelta;
-    std::vector<DevBuf*> bondR;               // R / L factor of the last normalisation
-    std::vector<int> bondRm, bondRn;          // its dims (rows, cols)
+    // Triangular factor of the last gauge move of each bond, kept per direction
+    // (0: left-to-right half-sweep, 1: right-to-left), with its dims.  The bond
+    // singular values are the singular values of these factors and are computed
+    // only when something reads them (the dlambda test of the sweep loop runs
+    // only when dE is already below its epsilon; accessors).
+    std::vector<DevBuf*> bondR[2];
+    std::vector<int> bondRm[2], bondRn[2];
+    std::vector<char> bondHave[2];
+    std::vector<int> bondLatest;              // direction of the most recent gauge move
     std::vector<int> bondK;                   // current bond dimension (Bond::GetD)
-    std::vector<char> bondDirty;
+    std::vector<char> bondDirty;              // bond_s lags behind the latest factor
     std::vector<double> Emin, iterDE, gapE;
     DevBuf tmp, Wqr, Qqr, svdw, envA, envB, yvec;
     MixedSite msite;
@@ -60,7 +67,9 @@ struct MPSState {
     int ensure_capacity(int D);
     int normalize_site(int ia, bool left);
     int normalize_all(bool left);
-    int bond_values_update(bool initial);
+    int bond_values(const std::vector<std::pair<int, int>>& which, std::vector<std::vector<double>>& out);
+    int ensure_bond_values();           // bond_s from the latest factor of every dirty bond
+    int sweep_pair_dlambda(double* dl); // Bond::GetMaxDelta over the last two half-sweeps
     int compute_left_env(int ia);
     int compute_right_env(int ia);
     int load_heff_caches();

@@ -150,7 +150,7 @@ __device__ void tri_solve(int n, const double* a, const double* b, double shift,
 
 // ---- kernels ---------------------------------------------------------------
 
-__global__ void lz_reset_kernel(LzState* st, double tol, int first) {
+__global__ void lz_reset_kernel(LzState* st, double tol, double tol_rel, int first) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         st->done = 0;
         st->nb = 0;
@@ -159,6 +159,7 @@ __global__ void lz_reset_kernel(LzState* st, double tol, int first) {
             st->matvecs = 0;
             st->converged = 0;
             st->tol = tol;
+            st->tol_rel = tol_rel;
             st->theta = 0;
             st->theta2 = 0;
             st->resid = 1e300;
@@ -311,6 +312,12 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
         double bj = b[j];
         double resid = bj * yl;
         double tolEff = fmax(st->tol, 1e-13 * fmax(1.0, fabs(th)));
+        if (st->tol_rel > 0) {
+            double tn = 0;
+            for (int i = 0; i < nk; ++i)
+                tn = fmax(tn, fabs(a[i]) + fabs(b[i]) + (i > 0 ? fabs(b[i - 1]) : 0.0));
+            tolEff = fmax(tolEff, st->tol_rel * tn);
+        }
         st->theta = th;
         st->resid = resid;
         st->nb = nk;
@@ -452,7 +459,7 @@ inline int vec_grid(long long N, int sm) {
 }  // namespace
 
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                  LzResult* out) {
+                  LzResult* out, double tol_rel) {
     cudaStream_t st = c.stream;
     if (N <= 0) return TN_BAD_SHAPE;
     int mm = m;
@@ -473,8 +480,9 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
 
     int restarts = 0;
     bool converged = false;
+    double prev_resid = 1e300;
     for (restarts = 0; restarts < (maxRestarts > 0 ? maxRestarts : 1); ++restarts) {
-        lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, restarts == 0);
+        lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, restarts == 0);
         TN_LAUNCH_CHECK();
         lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
         TN_LAUNCH_CHECK();
@@ -500,9 +508,14 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         TN_CUDA_CHECK(cudaStreamSynchronize(st));
         if (hs->converged) { converged = true; ++restarts; break; }
         if ((long long)mm >= N) { converged = true; ++restarts; break; }  // full space spanned: exact
+        if (tol_rel > 0) {
+            // split-precision operator: stop at its noise floor (no real progress)
+            if (restarts > 0 && hs->resid > 0.5 * prev_resid) { ++restarts; break; }
+            prev_resid = hs->resid;
+        }
     }
     // final normalisation of the Ritz vector
-    lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, 0);
+    lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0);
     TN_LAUNCH_CHECK();
     lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
     TN_LAUNCH_CHECK();

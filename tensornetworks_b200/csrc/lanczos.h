@@ -16,6 +16,7 @@ struct LzState {
     unsigned int counter;  // last-block reduction ticket
     int pad;
     double tol, theta, theta2, resid, xnorm;
+    double tol_rel;        // additional residual target relative to |T| (split-precision operators)
     double alpha[LZ_MAXK], beta[LZ_MAXK];
     double h[LZ_MAXK], h2[LZ_MAXK];
     double y[LZ_MAXK];
@@ -33,7 +34,11 @@ using MatvecFn = std::function<int(const double*, double*, const int*)>;
 // theta = x.y/x.x and |y - theta x|/|x| (device vectors; synchronises).
 int rayleigh_residual(Ctx& c, long long N, const double* x, const double* y, double* theta, double* resid);
 
+// tol: absolute residual target; tol_rel (>= 0): residual target relative to
+// the norm of the tridiagonal matrix (the operator's noise floor for the
+// split-precision matvec).  With tol_rel > 0 the restarts also stop once the
+// residual no longer drops by half between restarts.
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                  LzResult* out);
+                  LzResult* out, double tol_rel = 0.0);
 
 }  // namespace tnb

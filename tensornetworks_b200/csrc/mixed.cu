@@ -10,9 +10,12 @@
 // Heff - sigma I, which has the same eigenvectors; energies are recomputed in
 // FP64).  Per matvec: split x (FP64 -> BF16 pairs), stage 1 on the tensor
 // cores (P[w1,n] = F_w1 x_n, FP32 out), stage 2 on CUDA cores (the sparse W
-// combination, FP32, re-split to BF16 pairs), stage 3 on the tensor cores
-// (y_m = sum_{w2} Q[m,w2] G_w2^T with K = (w2, j2) accumulated in TMEM, FP64 out).
+// combination, FP32, re-split to BF16 pieces), stage 3 on the tensor cores
+// split over w2 for parallelism (Yp[m,w2] = Q[m,w2] G_w2^T, FP32 partials) and a
+// deterministic FP64 sum over w2 into y.
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "mixed.h"
 
@@ -51,8 +54,9 @@ __global__ void block_trace_kernel(const double* __restrict__ E, int D, int w, d
     }
 }
 
-// F (Dw x D x D, column-major blocks: (w,i,j) at w*D*D + j*D + i) ->
-// Fs[w][i][j] (j contiguous), block wshift shifted by -(*shift) on the diagonal.
+// Environment E (Dw x D x D, column-major blocks: (w,i,j) at w*D*D + j*D + i) ->
+// Es[w][i][j] (j contiguous: K-major rows), block wshift shifted by -(*shift) on
+// the diagonal.  Used for both F (rows i1, K = j1) and G (rows i2, K = j2).
 __global__ void split_env_left_kernel(const double* __restrict__ F, int Dw, int D, int wshift,
                                       const double* __restrict__ shift, uint16_t* __restrict__ out, int ns,
                                       long long pstride) {
@@ -69,23 +73,6 @@ __global__ void split_env_left_kernel(const double* __restrict__ F, int Dw, int 
     }
 }
 
-// G (Dw x D x D, (w,i,j) at w*D*D + j*D + i) -> Gs[i][w][j] (K = (w, j) contiguous per row i).
-__global__ void split_env_right_kernel(const double* __restrict__ G, int Dw, int D, int wshift,
-                                       const double* __restrict__ shift, uint16_t* __restrict__ out, int ns,
-                                       long long pstride) {
-    const long long total = (long long)Dw * D * D;
-    const double sft = shift ? *shift : 0.0;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(e % D);
-        const int w = (int)((e / D) % Dw);
-        const int i = (int)(e / ((long long)D * Dw));
-        double v = G[(long long)w * D * D + (long long)j * D + i];
-        if (w == wshift && i == j) v -= sft;
-        split_bf16((float)v, ns, out, pstride, e);
-    }
-}
-
 __global__ void split_vec_kernel(const double* __restrict__ x, long long n, uint16_t* __restrict__ out, int ns,
                                  long long pstride, const int* skip) {
     if (skip && *skip) return;
@@ -93,7 +80,7 @@ __global__ void split_vec_kernel(const double* __restrict__ x, long long n, uint
         split_bf16((float)x[e], ns, out, pstride, e);
 }
 
-// Q[m][i1][w2][j2] = sum_terms c * P[(w1,n)][i1][j2], split into BF16 pairs.
+// Q[m][w2][i1][j2] = sum_terms c * P[(w1,n)][i1][j2], split into BF16 pieces.
 __global__ void wcombine_split_kernel(const float* __restrict__ P, uint16_t* __restrict__ qout, int ns,
                                       long long pstride, const WTermDev* __restrict__ terms, int nterms,
                                       int D1, int D2, int Dwout, const int* skip) {
@@ -101,15 +88,13 @@ __global__ void wcombine_split_kernel(const float* __restrict__ P, uint16_t* __r
     const long long blk = (long long)D1 * D2;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < blk;
          e += (long long)gridDim.x * blockDim.x) {
-        const int j2 = (int)(e % D2);
-        const int i1 = (int)(e / D2);
         int cur = terms[0].out;
         float acc = 0.0f;
         for (int t = 0; t <= nterms; ++t) {
             const bool flush = (t == nterms) || (terms[t].out != cur);
             if (flush) {
-                const int m = cur / Dwout, w2 = cur - m * Dwout;
-                const long long o = (((long long)m * D1 + i1) * Dwout + w2) * D2 + j2;
+                // out slab cur = m*Dwout + w2; Q layout [m][w2][i1][j2]
+                const long long o = (long long)cur * blk + e;
                 split_bf16(acc, ns, qout, pstride, o);
                 if (t == nterms) break;
                 acc = 0.0f;
@@ -117,6 +102,20 @@ __global__ void wcombine_split_kernel(const float* __restrict__ P, uint16_t* __r
             }
             acc = fmaf((float)terms[t].c, P[(long long)terms[t].in * blk + e], acc);
         }
+    }
+}
+
+// y[m][e] = sum_w2 Yp[(m*Dw2 + w2)][e]   (FP32 partials -> FP64 site layout)
+__global__ void reduce_w2_kernel(const float* __restrict__ Yp, int d, int Dw2, long long blk, double* __restrict__ y,
+                                 const int* skip) {
+    if (skip && *skip) return;
+    const long long total = (long long)d * blk;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long m = e / blk, r = e - m * blk;
+        double s = 0.0;
+        for (int w = 0; w < Dw2; ++w) s += (double)Yp[((long long)m * Dw2 + w) * blk + r];
+        y[e] = s;
     }
 }
 
@@ -136,7 +135,7 @@ int mixed_prepare_site(Ctx& c, MixedSite& ms, const ContractShape& s, const WTer
     const int ns = nsplit;
     const long long blk = (long long)D1 * D2;
     const size_t nF = pad8((size_t)Dw1 * D1 * D1), nG = pad8((size_t)Dw2 * D2 * D2), nX = pad8((size_t)d * blk);
-    const size_t nP = (size_t)Dw1 * d * blk, nQ = pad8((size_t)d * D1 * Dw2 * D2);
+    const size_t nP = (size_t)std::max(Dw1, Dw2) * d * blk, nQ = pad8((size_t)d * D1 * Dw2 * D2);
     TN_CHECK(ms.Fs.ensure(2 * ns * nF));
     TN_CHECK(ms.Gs.ensure(2 * ns * nG));
     TN_CHECK(ms.Xs.ensure(2 * ns * nX));
@@ -156,7 +155,7 @@ int mixed_prepare_site(Ctx& c, MixedSite& ms, const ContractShape& s, const WTer
     TN_LAUNCH_CHECK();
     split_env_left_kernel<<<g1d(nF), 256, 0, st>>>(F, Dw1, D1, wF, sh, Fp, ns, (long long)nF);
     TN_LAUNCH_CHECK();
-    split_env_right_kernel<<<g1d(nG), 256, 0, st>>>(G, Dw2, D2, wG, sh + 1, Gp, ns, (long long)nG);
+    split_env_left_kernel<<<g1d(nG), 256, 0, st>>>(G, Dw2, D2, wG, sh + 1, Gp, ns, (long long)nG);
     TN_LAUNCH_CHECK();
     ms.shape = s;
     ms.termsLR = termsLR;
@@ -176,16 +175,17 @@ int mixed_prepare_site(Ctx& c, MixedSite& ms, const ContractShape& s, const WTer
     a1.out_mode = TC_OUT_F32_ROWMAJOR; a1.c32 = ms.P32.as<float>(); a1.ldc = D2; a1.c_batch = blk;
     a1.err = ms.err.as<int>();
     TN_CHECK(tc_gemm_plan(a1, &ms.plan1));
-    // stage 3: y_m(i1, i2) = sum_{(w2,j2)} Qs[m](i1, (w2,j2)) Gs(i2, (w2,j2)), FP64 column-major out
+    // stage 3, split over w2: Yp[(m,w2)](i1, i2) = sum_j2 Qs[(m,w2)](i1, j2) Gs[w2](i2, j2)
+    // (FP32 column-major partials), then y_m = sum_w2 Yp[(m,w2)] in FP64
     TcGemmArgs a3;
-    a3.M = D1; a3.N = D2; a3.K = Dw2 * D2; a3.batch = d; a3.nsplit = ns;
+    a3.M = D1; a3.N = D2; a3.K = D2; a3.batch = d * Dw2; a3.nsplit = ns;
     for (int q = 0; q < ns; ++q) {
         a3.a[q] = ms.Qs.as<uint16_t>() + q * nQ;
         a3.b[q] = Gp + q * nG;
     }
-    a3.lda = (long long)Dw2 * D2; a3.a_batch = (long long)D1 * Dw2 * D2; a3.a_nbatch = d; a3.a_bdiv = 1; a3.a_bmod = d;
-    a3.ldb = (long long)Dw2 * D2; a3.b_batch = 0; a3.b_nbatch = 1; a3.b_bdiv = 1; a3.b_bmod = 1;
-    a3.out_mode = TC_OUT_F64_COLMAJOR; a3.ldc = D1; a3.c_batch = blk;
+    a3.lda = D2; a3.a_batch = blk; a3.a_nbatch = d * Dw2; a3.a_bdiv = 1; a3.a_bmod = d * Dw2;
+    a3.ldb = D2; a3.b_batch = (long long)D2 * D2; a3.b_nbatch = Dw2; a3.b_bdiv = 1; a3.b_bmod = Dw2;
+    a3.out_mode = TC_OUT_F32_COLMAJOR; a3.c32 = ms.P32.as<float>(); a3.ldc = D1; a3.c_batch = blk;
     a3.err = ms.err.as<int>();
     TN_CHECK(tc_gemm_plan(a3, &ms.plan3));
     ms.ready = true;
@@ -207,8 +207,9 @@ int heff_matvec_mixed(Ctx& c, MixedSite& ms, const double* x, double* y, const i
     TN_LAUNCH_CHECK();
     TcGemmPlan p3 = ms.plan3;
     p3.args.skip = skip;
-    p3.args.c64 = y;
     TN_CHECK(tc_gemm_run(p3, st));
+    reduce_w2_kernel<<<g1d(nX), 256, 0, st>>>(ms.P32.as<float>(), s.d, s.Dw2, blk, y, skip);
+    TN_LAUNCH_CHECK();
     return TN_OK;
 }
 

@@ -217,7 +217,14 @@ __global__ void __launch_bounds__(THREADS, 1)
                 float v[16];
                 tmem_ld16(tbase + (uint32_t)c0, v);
                 if (row < p.M) {
-                    if (p.out_mode == TC_OUT_F32_ROWMAJOR) {
+                    if (p.out_mode == TC_OUT_F32_COLMAJOR) {
+                        float* dst = p.c32 + (long long)b * p.c_batch + row;
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const int col = n0 + c0 + i;
+                            if (col < p.N) dst[(long long)col * p.ldc] = v[i] * p.alpha;
+                        }
+                    } else if (p.out_mode == TC_OUT_F32_ROWMAJOR) {
                         float* dst = p.c32 + (long long)b * p.c_batch + (long long)row * p.ldc + n0 + c0;
 #pragma unroll
                         for (int i = 0; i < 16; ++i)
@@ -307,7 +314,8 @@ int tc_gemm_plan(const TcGemmArgs& p, TcGemmPlan* plan) {
         return TN_BAD_ARG;
     }
     plan->args = p;
-    plan->bn = p.N <= 64 ? 64 : 128;
+    const long long tiles128 = (long long)((p.N + 127) / 128) * ((p.M + BM - 1) / BM) * p.batch;
+    plan->bn = (p.N <= 64 || tiles128 < 148) ? 64 : 128;
     for (int q = 0; q < p.nsplit; ++q) {
         TN_CHECK(make_map(&plan->maps.a[q], p.a[q], p.K, p.M, p.a_nbatch, p.lda, p.a_batch, BM));
         TN_CHECK(make_map(&plan->maps.b[q], p.b[q], p.K, p.N, p.b_nbatch, p.ldb, p.b_batch, plan->bn));

@@ -6,7 +6,7 @@
 
 namespace tnb {
 
-enum { TC_OUT_F32_ROWMAJOR = 0, TC_OUT_F64_COLMAJOR = 1, TC_OUT_F64_COLMAJOR_ACC = 2 };
+enum { TC_OUT_F32_ROWMAJOR = 0, TC_OUT_F64_COLMAJOR = 1, TC_OUT_F64_COLMAJOR_ACC = 2, TC_OUT_F32_COLMAJOR = 3 };
 
 // C[b](m,n) = alpha * sum_k A[b](m,k) B[b](n,k); A rows are K-contiguous BF16 pieces
 // (hi, lo[, lo2]) with row pitch lda and batch pitch a_batch (elements); same for B.
