@@ -303,6 +303,22 @@ int MPSState::rescale_site(int ia) {
     return TN_OK;
 }
 
+// Thin QR of the gauge matrix W (m x n, ld m): Cholesky-QR2 when the shape allows
+// and the factor is well conditioned, Householder otherwise.  W is preserved by
+// the Cholesky path and overwritten by the Householder path.
+int MPSState::gauge_qr(int m, int n, double* W, double* Q, double* R, int ldr) {
+    if (cholqr_supported(m, n)) {
+        bool ok = false;
+        TN_CHECK(cholqr2_dense(*ctx, m, n, W, Q, m, R, ldr, &ok));
+        if (ok) {
+            ++gauge_cholqr;
+            return TN_OK;
+        }
+    }
+    ++gauge_householder;
+    return qr_dense(*ctx, m, n, W, Q, m, R, ldr);
+}
+
 // MPSSite::SVDNormalize / NormalizeQR + Bond::SVDTransfer / TransferQR
 // (MPSSite_Normalization.C:20-107, Bond.C:162-176, MPSSite_Contractions.C:402-513).
 int MPSState::normalize_site(int ia, bool left) {
@@ -333,7 +349,7 @@ int MPSState::normalize_site(int ia, bool left) {
         TN_CHECK(Rb->ensure(sizeof(double) * (size_t)k * n));
         // W(r=(n_,i1), c=i2) = A(n_,i1,i2)
         TN_CHECK(copy2d(m, n, Aia, idx2(1, a1, blk), idx(a1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
-        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, Rb->as<double>(), k));
+        TN_CHECK(gauge_qr(m, n, Wqr.as<double>(), Qqr.as<double>(), Rb->as<double>(), k));
         // site := Q with D2 = k
         TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(1, a1, (long long)a1 * k), idx(a1), 1.0, st));
         D2[ia] = k;
@@ -360,7 +376,7 @@ int MPSState::normalize_site(int ia, bool left) {
         TN_CHECK(Rb->ensure(sizeof(double) * (size_t)k * n));
         // W(r=(n_,i2), c=i1) = A(n_,i1,i2)
         TN_CHECK(copy2d(m, n, Aia, idx2(a1, a2, blk), idx(1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
-        TN_CHECK(qr_dense(*ctx, m, n, Wqr.as<double>(), Qqr.as<double>(), m, Rb->as<double>(), k));
+        TN_CHECK(gauge_qr(m, n, Wqr.as<double>(), Qqr.as<double>(), Rb->as<double>(), k));
         // site := Q^T with D1 = k: element (n_, i1', i2) = Q(n_*D2+i2, i1')
         TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(k, a2, (long long)k * a2), idx(1), 1.0, st));
         D1[ia] = k;
@@ -554,7 +570,7 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     int restarts = opt.max_restarts > 0 ? opt.max_restarts : 10;
     // residual target: the requested tolerance, but not below the split operator's
     // noise floor relative to |T| (BF16x3 ~ 2^-16, BF16x6 ~ FP32 accumulation)
-    const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 2e-6 : 3e-5);
+    const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-7);
     LzResult rm{};
     TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel));
     TN_CHECK(mixed_check_error(msite, st));
@@ -582,6 +598,9 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
         theta2 = r.theta2;
         ++fallbacks;
     }
+    if (opt.verbose >= 3)
+        std::printf("site %3d D %3dx%3d mixed: %d matvecs resid %.2e | fp64 RQ resid %.2e theta %.12f\n", ia,
+                    D1[ia], D2[ia], rm.matvecs, rm.resid, resid, theta);
     if (!rm.converged) ++not_converged;
     iterDE[ia] = theta - Emin[ia];
     Emin[ia] = theta;

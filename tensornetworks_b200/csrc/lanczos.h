@@ -20,6 +20,7 @@ struct LzState {
     double alpha[LZ_MAXK], beta[LZ_MAXK];
     double h[LZ_MAXK], h2[LZ_MAXK];
     double y[LZ_MAXK];
+    double rhist[LZ_MAXK];  // residual estimate after each step of the current restart
 };
 
 struct LzResult {

@@ -117,6 +117,7 @@ struct Ctx {
     DevBuf lzstate;        // Lanczos device state
     DevBuf rq;             // Rayleigh-quotient state + partials
     DevBuf qrw;            // QR workspace
+    DevBuf cqr;            // Cholesky-QR workspace
     DevBuf svdw;           // SVD workspace
     DevBuf wterms;         // MPO term lists
     DevBuf misc;
