@@ -324,9 +324,9 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
         st->rhist[j] = resid;
         bool conv = (resid <= tolEff) || (bj <= 1e-14 * fmax(1.0, fabs(th)));
         if (conv) { st->done = 1; st->converged = 1; }
-        // split-precision operator: a residual that no longer falls (10% over 4
-        // steps) has reached the operator's noise floor
-        if (st->tol_rel > 0 && j >= 4 && resid > 0.9 * st->rhist[j - 4]) st->done = 1;
+        // split-precision operator: a residual that no longer halves over two
+        // steps has reached the operator's noise floor
+        if (st->tol_rel > 0 && j >= 2 && resid > 0.5 * st->rhist[j - 2]) st->done = 1;
         if (nk >= mmax) st->done = 1;  // basis exhausted for this restart
     }
 }
