@@ -627,7 +627,7 @@ int tn_qr(tn_ctx c, int m, int n, const double* A, int lda, double* Q, int ldq, 
     const int k = std::min(m, n);
     if (ldq < m || ldr < k) return TN_BAD_ARG;
     Ctx& cx = c->c;
-    DevBuf W;
+    DevBuf& W = cx.apiw[0];
     TN_CHECK(W.ensure(sizeof(double) * (size_t)m * n));
     TN_CHECK(copy2d(m, n, A, idx(1), idx(lda), W.as<double>(), idx(1), idx(m), 1.0, cx.stream));
     TN_CHECK(qr_dense(cx, m, n, W.as<double>(), Q, ldq, R, ldr));
@@ -640,7 +640,7 @@ int tn_lq(tn_ctx c, int m, int n, const double* A, int lda, double* L, int ldl, 
     const int k = std::min(m, n);
     if (ldl < m || ldq < k) return TN_BAD_ARG;
     Ctx& cx = c->c;
-    DevBuf W, Qt, Rt;
+    DevBuf &W = cx.apiw[0], &Qt = cx.apiw[1], &Rt = cx.apiw[2];
     TN_CHECK(W.ensure(sizeof(double) * (size_t)m * n));
     TN_CHECK(Qt.ensure(sizeof(double) * (size_t)n * k));
     TN_CHECK(Rt.ensure(sizeof(double) * (size_t)k * m));

@@ -303,19 +303,9 @@ int MPSState::rescale_site(int ia) {
     return TN_OK;
 }
 
-// Thin QR of the gauge matrix W (m x n, ld m): Cholesky-QR2 when the shape allows
-// and the factor is well conditioned, Householder otherwise.  W is preserved by
-// the Cholesky path and overwritten by the Householder path.
+// Thin QR of the gauge matrix W (m x n, ld m; overwritten) into Q (m x k, ld m)
+// and R (k x n, ld ldr): blocked Householder.
 int MPSState::gauge_qr(int m, int n, double* W, double* Q, double* R, int ldr) {
-    if (cholqr_supported(m, n)) {
-        bool ok = false;
-        TN_CHECK(cholqr2_dense(*ctx, m, n, W, Q, m, R, ldr, &ok));
-        if (ok) {
-            ++gauge_cholqr;
-            return TN_OK;
-        }
-    }
-    ++gauge_householder;
     return qr_dense(*ctx, m, n, W, Q, m, R, ldr);
 }
 

@@ -6,7 +6,6 @@
 #include "contract.h"
 #include "lanczos.h"
 #include "mixed.h"
-#include "cholqr.h"
 #include "qr.h"
 
 namespace tnb {
@@ -57,7 +56,6 @@ struct MPSState {
     long long matvecs = 0, matvecs_fp64 = 0;
     double heff_flop = 0;
     int not_converged = 0, fallbacks = 0;
-    long long gauge_cholqr = 0, gauge_householder = 0;
     tn_solver_options opt{};
     // phase timing (verbose >= 2): seconds in refine / gauge / environment / bond values
     double t_refine = 0, t_gauge = 0, t_env = 0, t_bond = 0;

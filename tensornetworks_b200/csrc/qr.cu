@@ -134,6 +134,308 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(double* __restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident panel (m <= 1024 rows).  Thread t owns rows t + k*256
+// (R rows of B columns in registers), so each column step costs two block
+// reductions and two barriers: the norm of the sub-column, then one
+// reduce-scatter of v^T P over every other column of the panel.  The same
+// reduce-scatter yields V(:,0:jj)^T v_jj, from which warp 0 appends column jj
+// of the dlarft T factor.  Reflectors follow the dlarfg convention as above.
+//
+// Register indices must be compile-time, but unrolling all B column steps is
+// instruction-fetch bound; so the loop runs over groups of QRP_U steps and
+// the register window rotates by QRP_U columns per group.  At the start of a
+// group (first column jj0) slot i holds column jj0 + i for i < B - jj0 and
+// the finished reflector l < jj0 sits in slot B - jj0 + l.
+constexpr int QRP_THREADS = 256;
+constexpr int QRP_WARPS = QRP_THREADS / 32;
+constexpr int QRP_U = 2;
+
+// Reduce-scatter of B per-lane values over the warp: afterwards lane l holds
+// the warp's sum for slot (l mod B).  B is 16 or 32; f(i) yields slot i.
+template <int B, class F>
+__device__ __forceinline__ double warp_reduce_scatter(F f) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    double h[16];
+    if (B == 32) {
+        const bool up = lane & 16;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const double a = f(i), b = f(i + 16);
+            const double send = up ? a : b, keep = up ? b : a;
+            h[i] = keep + __shfl_xor_sync(full, send, 16);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const double a = f(i);
+            h[i] = a + __shfl_xor_sync(full, a, 16);
+        }
+    }
+#pragma unroll
+    for (int k = 8; k >= 1; k >>= 1) {
+        const bool up = lane & k;
+#pragma unroll
+        for (int i = 0; i < k; ++i) {
+            const double send = up ? h[i] : h[i + k], keep = up ? h[i + k] : h[i];
+            h[i] = keep + __shfl_xor_sync(full, send, k);
+        }
+    }
+    return h[0];
+}
+
+template <int R, int B>
+__global__ void __launch_bounds__(QRP_THREADS) qr_panel_reg_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                                                     double* __restrict__ V, int ldv,
+                                                                     double* __restrict__ T, int ldt) {
+    static_assert(B % QRP_U == 0, "panel width must be a multiple of the group size");
+    __shared__ double redN[QRP_WARPS];
+    __shared__ double redD[QRP_WARPS][32];
+    __shared__ double gsh[QRP_WARPS][32];
+    __shared__ double alpha_sh;
+    __shared__ double Gs[B][B + 1];   // Gs[l][jj] = v_l^T v_jj, l < jj
+    __shared__ double taus[B];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int mp = m - j0;
+    double p[R][B];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int r = tid + k * QRP_THREADS;
+#pragma unroll
+        for (int c = 0; c < B; ++c)
+            p[k][c] = (r < mp && c < b) ? W[(size_t)(j0 + c) * ldw + j0 + r] : 0.0;
+    }
+#pragma unroll 1
+    for (int jj0 = 0; jj0 < b; jj0 += QRP_U) {
+        const int last_trail = B - 1 - jj0;  // slots u+1 .. last_trail are trailing columns
+#pragma unroll
+        for (int u = 0; u < QRP_U; ++u) {
+            const int jj = jj0 + u;
+            if (jj >= b) break;
+            double part = 0;
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int r = tid + k * QRP_THREADS;
+                if (r > jj && r < mp) part = fma(p[k][u], p[k][u], part);
+            }
+            part = wsum(part);
+            if (lane == 0) redN[wid] = part;
+            if (tid == jj) alpha_sh = p[0][u];
+            __syncthreads();
+            double xn2 = 0;
+#pragma unroll
+            for (int w = 0; w < QRP_WARPS; ++w) xn2 += redN[w];
+            const double alpha = alpha_sh;
+            double t = 0, beta = alpha, scal = 0;
+            if (xn2 > 0.0) {
+                const double nrm = sqrt(alpha * alpha + xn2);
+                beta = alpha >= 0 ? -nrm : nrm;
+                const double amb = alpha - beta;
+                const double rinv = 1.0 / (beta * amb);  // tau = -amb / beta, scal = 1 / amb
+                t = -amb * amb * rinv;
+                scal = beta * rinv;
+            }
+            double v[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int r = tid + k * QRP_THREADS;
+                if (r == jj) {
+                    v[k] = 1.0;
+                    p[k][u] = beta;
+                } else if (r > jj && r < mp) {
+                    if (t != 0.0) p[k][u] *= scal;
+                    v[k] = p[k][u];
+                } else {
+                    v[k] = 0.0;
+                }
+            }
+            // every slot but u: v_jj^T (trailing column or finished reflector)
+            const double red = warp_reduce_scatter<B>([&](int i) {
+                double sacc = 0;
+                if (i != u) {
+#pragma unroll
+                    for (int k = 0; k < R; ++k) sacc = fma(v[k], p[k][i], sacc);
+                }
+                return sacc;
+            });
+            redD[wid][lane] = red;
+            __syncthreads();
+            double g = 0;
+#pragma unroll
+            for (int w = 0; w < QRP_WARPS; ++w) g += redD[w][lane];
+            gsh[wid][lane] = g;
+            __syncwarp();
+            if (t != 0.0) {
+#pragma unroll
+                for (int i = u + 1; i < B; ++i) {
+                    if (i <= last_trail) {
+                        const double ts = t * gsh[wid][i];
+#pragma unroll
+                        for (int k = 0; k < R; ++k) p[k][i] = fma(-ts, v[k], p[k][i]);
+                    }
+                }
+            }
+            if (wid == 0) {
+                // column jj of V^T V (reflector l sits in slot B - jj0 + l or l - jj0)
+                if (lane < jj) Gs[lane][jj] = gsh[0][lane < jj0 ? B - jj0 + lane : lane - jj0];
+                if (lane == 0) taus[jj] = t;
+            }
+        }
+        // rotate the window left by QRP_U columns
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            double keep[QRP_U];
+#pragma unroll
+            for (int i = 0; i < QRP_U; ++i) keep[i] = p[k][i];
+#pragma unroll
+            for (int i = 0; i < B - QRP_U; ++i) p[k][i] = p[k][i + QRP_U];
+#pragma unroll
+            for (int i = 0; i < QRP_U; ++i) p[k][B - QRP_U + i] = keep[i];
+        }
+    }
+    // after the groups slot i holds column (i + rb) mod B, rb = b rounded up to the group size
+    const int rb = ((b + QRP_U - 1) / QRP_U) * QRP_U;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int r = tid + k * QRP_THREADS;
+        if (r < mp) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                const int c = (i + rb) % B;
+                if (c < b) {
+                    W[(size_t)(j0 + c) * ldw + j0 + r] = p[k][i];
+                    V[(size_t)c * ldv + r] = (r < c) ? 0.0 : (r == c ? 1.0 : p[k][i]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // dlarft (forward, columnwise): T(i, jj) = -tau_jj sum_{l=i}^{jj-1} T(i, l) G(l, jj),
+    // T(i, i) = tau_i.  Row i needs only row i, so lane i builds it in registers.
+    if (wid == 0 && lane < B) {
+        const int i = lane;
+        double trow[B];
+#pragma unroll
+        for (int jj = 0; jj < B; ++jj) {
+            double a0 = 0, a1 = 0;
+#pragma unroll
+            for (int l = 0; l < jj; ++l) {
+                const double term = (l >= i) ? trow[l] * Gs[l][jj] : 0.0;
+                if (l & 1) a1 += term; else a0 += term;
+            }
+            const double tj = jj < b ? taus[jj] : 0.0;
+            trow[jj] = (jj < i) ? 0.0 : (jj == i ? tj : -tj * (a0 + a1));
+        }
+#pragma unroll
+        for (int jj = 0; jj < B; ++jj)
+            if (i < b && jj < b) T[(size_t)jj * ldt + i] = trow[jj];
+    }
+}
+
+// C (mp x nc, ld ldc) <- (I - V T' V^T) C with T' = T^T (TRANS: applying Q^T,
+// the trailing update) or T (forming Q).  V is mp x b (ld ldv, unit lower
+// trapezoidal, explicit), T is b x b upper triangular (ld ldt), b <= B.
+// One CTA per 8 columns of C.  The whole of V and the CTA's columns of C are
+// staged in shared memory by asynchronous copies (all in flight at once; the
+// kernel is latency bound otherwise), then Z = V^T C, Z2 = T' Z, C -= V Z2.
+// Shared layout: column-major with the odd stride mp + 1, so that both the
+// lane-per-column reads of the Z reduction and the lane-per-row reads of the
+// update are free of bank conflicts.
+constexpr int WY_COLS = 8;
+constexpr int WY_THREADS = 256;
+
+inline size_t wy_smem_bytes(int mp, int B) { return sizeof(double) * (size_t)(mp + 1) * (B + WY_COLS); }
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int B, bool TRANS>
+__global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __restrict__ V, int ldv,
+                                                              const double* __restrict__ T, int ldt, int b,
+                                                              double* __restrict__ C, int ldc, int mp, int nc) {
+    constexpr int NPART = WY_THREADS / (B * WY_COLS);  // row partitions of the Z reduction
+    extern __shared__ double wsm[];
+    const int ld = mp + 1;
+    double* Vs = wsm;                  // B columns of length ld
+    double* Cs = Vs + (size_t)ld * B;  // WY_COLS columns of length ld
+    __shared__ double Zp[NPART][B][WY_COLS];
+    __shared__ double Z2[B][WY_COLS];
+    const int tid = threadIdx.x;
+    const int c0 = blockIdx.x * WY_COLS;
+    const int ncol = min(WY_COLS, nc - c0);
+    for (int e = tid; e < mp * B; e += WY_THREADS) {
+        const int r = e % mp, col = e / mp;
+        if (col < b) cp_async8(Vs + (size_t)col * ld + r, V + (size_t)col * ldv + r);
+        else Vs[(size_t)col * ld + r] = 0.0;
+    }
+    for (int e = tid; e < mp * WY_COLS; e += WY_THREADS) {
+        const int r = e % mp, col = e / mp;
+        if (col < ncol) cp_async8(Cs + (size_t)col * ld + r, C + (size_t)(c0 + col) * ldc + r);
+        else Cs[(size_t)col * ld + r] = 0.0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    {
+        const int bb = tid % B, cc = (tid / B) % WY_COLS, part = tid / (B * WY_COLS);
+        const double* vcol = Vs + (size_t)bb * ld;
+        const double* ccol = Cs + (size_t)cc * ld;
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        int r = part;
+        for (; r + 3 * NPART < mp; r += 4 * NPART) {
+            a0 = fma(vcol[r], ccol[r], a0);
+            a1 = fma(vcol[r + NPART], ccol[r + NPART], a1);
+            a2 = fma(vcol[r + 2 * NPART], ccol[r + 2 * NPART], a2);
+            a3 = fma(vcol[r + 3 * NPART], ccol[r + 3 * NPART], a3);
+        }
+        for (; r < mp; r += NPART) a0 = fma(vcol[r], ccol[r], a0);
+        Zp[part][bb][cc] = (a0 + a1) + (a2 + a3);
+    }
+    __syncthreads();
+    if (tid < B * WY_COLS) {
+        const int bb = tid % B, cc = tid / B;
+        double s = 0;
+        if (bb < b) {
+            if (TRANS) {
+                for (int l = 0; l <= bb; ++l) {
+                    double z = 0;
+#pragma unroll
+                    for (int pp = 0; pp < NPART; ++pp) z += Zp[pp][l][cc];
+                    s = fma(T[(size_t)bb * ldt + l], z, s);
+                }
+            } else {
+                for (int l = bb; l < b; ++l) {
+                    double z = 0;
+#pragma unroll
+                    for (int pp = 0; pp < NPART; ++pp) z += Zp[pp][l][cc];
+                    s = fma(T[(size_t)l * ldt + bb], z, s);
+                }
+            }
+        }
+        Z2[bb][cc] = s;
+    }
+    __syncthreads();
+    for (int r = tid; r < mp; r += WY_THREADS) {
+        double acc[WY_COLS];
+#pragma unroll
+        for (int q = 0; q < WY_COLS; ++q) acc[q] = Cs[(size_t)q * ld + r];
+#pragma unroll 4
+        for (int l = 0; l < B; ++l) {
+            const double vl = Vs[(size_t)l * ld + r];
+#pragma unroll
+            for (int q = 0; q < WY_COLS; ++q) acc[q] = fma(-vl, Z2[l][q], acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < WY_COLS; ++q)
+            if (q < ncol) C[(size_t)(c0 + q) * ldc + r] = acc[q];
+    }
+}
+
 __global__ void set_identity_kernel(double* Q, int m, int k, int ldq) {
     long long total = (long long)m * k;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
@@ -165,9 +467,66 @@ int panel_width(int m) {
 
 }  // namespace
 
+namespace {
+
+template <int R, int B>
+int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
+    cudaStream_t st = c.stream;
+    const int k = std::min(m, n);
+    static thread_local int attr_set[2] = {-1, -1};  // device whose attributes are set
+    int dev = 0;
+    TN_CUDA_CHECK(cudaGetDevice(&dev));
+    if (attr_set[B == 32] != dev) {
+        const int bytes = (int)wy_smem_bytes(B == 32 ? 2 * QRP_THREADS : 4 * QRP_THREADS, B);
+        TN_CUDA_CHECK(cudaFuncSetAttribute(wy_apply_kernel<B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        TN_CUDA_CHECK(cudaFuncSetAttribute(wy_apply_kernel<B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        attr_set[B == 32] = dev;
+    }
+    size_t need = sizeof(double) * ((size_t)m * k + (size_t)B * k + 16);
+    TN_CHECK(c.qrw.ensure(need));
+    double* Vall = c.qrw.as<double>();
+    double* Tall = Vall + (size_t)m * k;
+    for (int j0 = 0; j0 < k; j0 += B) {
+        const int b = std::min(B, k - j0);
+        const int mp = m - j0;
+        double* Vp = Vall + (size_t)j0 * m + j0;  // ld m
+        double* Tp = Tall + (size_t)j0 * B;        // ld B
+        qr_panel_reg_kernel<R, B><<<1, QRP_THREADS, 0, st>>>(W, m, m, j0, b, Vp, m, Tp, B);
+        TN_LAUNCH_CHECK();
+        const int nt = n - j0 - b;
+        if (nt > 0) {
+            wy_apply_kernel<B, true><<<(nt + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(mp, B), st>>>(
+                Vp, m, Tp, B, b, W + (size_t)(j0 + b) * m + j0, m, mp, nt);
+            TN_LAUNCH_CHECK();
+        }
+    }
+    if (Rout) {
+        extract_r_kernel<<<g1d((long long)k * n), 256, 0, st>>>(W, m, k, n, Rout, ldr);
+        TN_LAUNCH_CHECK();
+    }
+    if (Qout) {
+        set_identity_kernel<<<g1d((long long)m * k), 256, 0, st>>>(Qout, m, k, ldq);
+        TN_LAUNCH_CHECK();
+        const int last = ((k - 1) / B) * B;
+        for (int j0 = last; j0 >= 0; j0 -= B) {
+            const int b = std::min(B, k - j0);
+            const int nq = k - j0;
+            wy_apply_kernel<B, false><<<(nq + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(m - j0, B), st>>>(
+                Vall + (size_t)j0 * m + j0, m, Tall + (size_t)j0 * B, B, b, Qout + (size_t)j0 * ldq + j0, ldq,
+                m - j0, nq);
+            TN_LAUNCH_CHECK();
+        }
+    }
+    return TN_OK;
+}
+
+}  // namespace
+
 int qr_dense(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
     cudaStream_t st = c.stream;
     if (m <= 0 || n <= 0) return TN_BAD_SHAPE;
+    if (m <= 2 * QRP_THREADS) return qr_dense_reg<2, 32>(c, m, n, W, Qout, ldq, Rout, ldr);
+    if (m <= 4 * QRP_THREADS) return qr_dense_reg<4, 16>(c, m, n, W, Qout, ldq, Rout, ldr);
     const int k = std::min(m, n);
     const int bmax = panel_width(m);
     if ((size_t)m * bmax * 8 > 200 * 1024 || bmax < 1) {

@@ -117,10 +117,10 @@ struct Ctx {
     DevBuf lzstate;        // Lanczos device state
     DevBuf rq;             // Rayleigh-quotient state + partials
     DevBuf qrw;            // QR workspace
-    DevBuf cqr;            // Cholesky-QR workspace
     DevBuf svdw;           // SVD workspace
     DevBuf wterms;         // MPO term lists
     DevBuf misc;
+    DevBuf apiw[3];        // staging copies of the dense-solver entry points
     HostBuf pinned;
     int sm_count = 148;
     // cache of the last MPO term list uploaded through the C ABI

@@ -117,7 +117,8 @@ def test_lanczos_heff(T, ctx, oracle, d, D1, D2, site):
     assert abs(th.value - tho) < 1e-10 * max(1, abs(tho))
 
 
-@pytest.mark.parametrize("m,n", [(7, 5), (5, 7), (64, 32), (32, 64), (512, 256), (130, 130), (1, 5), (9, 1)])
+@pytest.mark.parametrize("m,n", [(7, 5), (5, 7), (64, 32), (32, 64), (512, 256), (130, 130), (1, 5), (9, 1),
+                                 (700, 700), (1024, 300), (600, 40), (2000, 64)])
 def test_qr_lq(T, ctx, oracle, m, n):
     rng = np.random.default_rng(m * 1000 + n)
     A = rng.uniform(-1, 1, size=(m, n))
