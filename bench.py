@@ -12,11 +12,16 @@ A "step" is one sweep pair (Sweep(DLeft) + Sweep(DRight)) of the L=100 chain at
 D = 256, starting from the state the schedule produced.  `value` is device time
 per step (CUDA events on the library's launch stream, max over ranks); the
 schedule itself is run once before the warm-up steps and its wall time and
-final energy are reported too.  Inputs (all site tensors, 25 MB at D = 256
-... 100 MB) are larger than L2 between steps.
+final energy are reported too.  Inputs (site tensors plus environments, about
+0.6 GB at D = 256) are larger than L2 between steps.
+
+The headline path is the split-precision one (--precision mixed, the default).
+Unless --no-fp64-compare is given, the plain FP64 GPU sweep runs the same
+schedule from the same seed and is timed the same way; the line then carries
+its time, the speed-up and the energy difference per site between the two.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                       [--precision fp64|mixed]
+                       [--precision fp64|mixed|mixed_hi] [--no-fp64-compare]
 """
 from __future__ import annotations
 
@@ -44,7 +49,9 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--precision", choices=["fp64", "mixed", "mixed_hi"], default="fp64")
+    p.add_argument("--precision", choices=["fp64", "mixed", "mixed_hi"], default="mixed")
+    p.add_argument("--no-fp64-compare", action="store_true",
+                   help="skip the FP64 GPU sweep on the same schedule (speed-up and energy check)")
     p.add_argument("--L", type=int, default=L_CHAIN)
     p.add_argument("--D", type=int, default=D_FINAL)
     p.add_argument("--cpu-sites", type=int, default=4, help="bulk site updates in the CPU baseline sample")
@@ -52,6 +59,15 @@ def parse():
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
+
+
+def unit_of(args):
+    return f"s per sweep pair (L={args.L}, D={args.D})"
+
+
+def workload_of(args):
+    return (f"Heisenberg S=1/2 L={args.L} open chain, d=2, Dw=5, one sweep pair at D={args.D} after the "
+            f"D 16->{args.D} schedule (2 sweeps/line), Krylov 20, eig tol 1e-10")
 
 
 def schedule_for(D):
@@ -199,52 +215,64 @@ def run_ours(args, rank, world, local_rank):
 
     ctx = T.Context(local_rank)
     lib = ctx._lib
-    prec = {"fp64": T.FP64, "mixed": T.MIXED, "mixed_hi": T.MIXED_HI}[args.precision]
-    opts = T.SolverOptions(precision=prec, krylov=KRYLOV, max_restarts=10)
     f = T.Factory(ctx)
     H = f.Make1D_NN_HeisenbergHamiltonian(args.L, S_SPIN, T.RegularLower, 1.0, 1.0, 0.0)
     lines = schedule_for(args.D)
-    psi = H.CreateMPS(lines[0][1], 1e-12, 1e-12)
-    psi.InitializeWith(T.Random, seed=1234)
-    sched = T.IterationSchedule()
-    for (ms, Dm, dD) in lines:
-        eps = T.Epsilons(1e-12)
-        eps.itsEigenSolverEpsilon = EPS_EIGEN
-        sched.Insert(T.IterationScheduleLine(ms, Dm, dD, eps))
-    t0 = time.perf_counter()
-    var = psi.FindVariationalGroundState(H, sched, opts)
-    schedule_s = time.perf_counter() - t0
-    sched_stats = dict(psi.last_stats)
-    E_sched = psi.GetExpectation(H)
 
-    for _ in range(args.warmup):
-        psi.Sweep(H, 1, EPS_EIGEN, opts)
+    def run_path(precision, sample_clocks):
+        """Schedule from the seed, W warm-up sweep pairs, then K timed sweep pairs."""
+        prec = {"fp64": T.FP64, "mixed": T.MIXED, "mixed_hi": T.MIXED_HI}[precision]
+        opts = T.SolverOptions(precision=prec, krylov=KRYLOV, max_restarts=10)
+        psi = H.CreateMPS(lines[0][1], 1e-12, 1e-12)
+        psi.InitializeWith(T.Random, seed=1234)
+        sched = T.IterationSchedule()
+        for (ms, Dm, dD) in lines:
+            eps = T.Epsilons(1e-12)
+            eps.itsEigenSolverEpsilon = EPS_EIGEN
+            sched.Insert(T.IterationScheduleLine(ms, Dm, dD, eps))
+        t0 = time.perf_counter()
+        var = psi.FindVariationalGroundState(H, sched, opts)
+        schedule_s = time.perf_counter() - t0
+        sched_stats = dict(psi.last_stats)
+        E_sched = psi.GetExpectation(H)
+        for _ in range(args.warmup):
+            psi.Sweep(H, 1, EPS_EIGEN, opts)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local_rank) if sample_clocks else None
+        if clocks:
+            clocks.start()
+        launches0 = lib.tn_launch_count()
+        step_ms, matvecs, flops = [], 0, 0.0
+        if args.profile_region and sample_clocks:
+            torch.cuda.profiler.start()
+        for _ in range(args.steps):
+            st = psi.Sweep(H, 1, EPS_EIGEN, opts)
+            step_ms.append(st["sweep_ms"])
+            matvecs += st["matvecs"]
+            flops += st["heff_flop"]
+        torch.cuda.synchronize()
+        if args.profile_region and sample_clocks:
+            torch.cuda.profiler.stop()
+        launches = lib.tn_launch_count() - launches0
+        if clocks:
+            clocks.stop()
+        t_step = sum(step_ms) / len(step_ms) / 1e3
+        if dist:
+            tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_step = float(tt.item())
+        return dict(psi=psi, opts=opts, var=var, schedule_s=schedule_s, sched_stats=sched_stats, E_sched=E_sched,
+                    t_step=t_step, step_ms=step_ms, matvecs=matvecs, flops=flops, launches=launches,
+                    clocks=clocks, E_after=psi.GetExpectation(H))
 
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    launches0 = lib.tn_launch_count()
-    step_ms, matvecs, flops = [], 0, 0.0
-    if args.profile_region:
-        torch.cuda.profiler.start()
-    for _ in range(args.steps):
-        st = psi.Sweep(H, 1, EPS_EIGEN, opts)
-        step_ms.append(st["sweep_ms"])
-        matvecs += st["matvecs"]
-        flops += st["heff_flop"]
-    torch.cuda.synchronize()
-    if args.profile_region:
-        torch.cuda.profiler.stop()
-    launches = lib.tn_launch_count() - launches0
-    clocks.stop()
-    t_step = sum(step_ms) / len(step_ms) / 1e3
-    if dist:
-        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step = float(tt.item())
-    E_after = psi.GetExpectation(H)
+    main_run = run_path(args.precision, True)
+    psi, opts, var = main_run["psi"], main_run["opts"], main_run["var"]
+    t_step, step_ms, flops = main_run["t_step"], main_run["step_ms"], main_run["flops"]
+    launches, clocks = main_run["launches"], main_run["clocks"]
+    sched_stats, schedule_s = main_run["sched_stats"], main_run["schedule_s"]
+    E_sched, E_after = main_run["E_sched"], main_run["E_after"]
 
     # --- end to end through the C ABI with host buffers (per step: upload all sites,
     #     one sweep pair, download all sites)
@@ -262,6 +290,19 @@ def run_ours(args, rank, world, local_rank):
         e2e_times.append(time.perf_counter() - t0)
     d2h = sum(a.nbytes for a in sites)
     e2e = sum(e2e_times) / len(e2e_times)
+
+    # --- the plain FP64 GPU sweep on the same schedule and seed
+    fp64_cmp = None
+    if args.precision != "fp64" and not args.no_fp64_compare:
+        ref64 = run_path("fp64", False)
+        fp64_cmp = {"value": round(ref64["t_step"], 6), "unit": unit_of(args),
+                    "speedup": round(ref64["t_step"] / t_step, 3),
+                    "schedule_s": round(ref64["schedule_s"], 3),
+                    "energy_per_bond": ref64["E_after"] / (args.L - 1),
+                    "dE_per_site_schedule": abs(E_sched - ref64["E_sched"]) / args.L,
+                    "dE_per_site_after_steps": abs(E_after - ref64["E_after"]) / args.L,
+                    "matvecs_per_step": ref64["matvecs"] / args.steps}
+        del ref64
 
     # --- roofline of the dominant kernel (the bulk Heff contraction chain)
     t_mv, F_mv = matvec_microbench(T, ctx, torch, args.D, args.precision)
@@ -287,7 +328,7 @@ def run_ours(args, rank, world, local_rank):
         out = {
             "metric": METRIC,
             "value": round(t_step, 6),
-            "unit": "s per sweep pair (L=100, D=256)",
+            "unit": unit_of(args),
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
@@ -298,19 +339,18 @@ def run_ours(args, rank, world, local_rank):
             "dtype": {"fp64": "f64", "mixed": "bf16x3 (f32 acc) contractions, f64 Lanczos/QR/SVD/energies",
                       "mixed_hi": "bf16x6 (f32 acc) contractions, f64 Lanczos/QR/SVD/energies"}[args.precision],
             "data": "synthetic (seeded uniform(-1,1) initial MPS)",
-            "config": {"workload": f"Heisenberg S=1/2 L={args.L} open chain, d=2, Dw=5, one sweep pair at "
-                                   f"D={args.D} after the D 16->{args.D} schedule (2 sweeps/line), Krylov 20, "
-                                   f"eig tol 1e-10",
+            "config": {"workload": workload_of(args),
                        "precision": args.precision, "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2 (site tensors + environments ~ 0.6 GB at D=256)"},
             "heff_tflops_sweep": round(flops / (sum(step_ms) / 1e3) / 1e12, 4),
-            "matvecs_per_step": matvecs / args.steps,
+            "matvecs_per_step": main_run["matvecs"] / args.steps,
+            "fp64_gpu": fp64_cmp,
             "schedule_s": round(schedule_s, 3),
             "schedule_sweep_ms": round(sched_stats["sweep_ms"], 1),
             "energy_per_bond": E_after / (args.L - 1),
             "energy_schedule_per_bond": E_sched / (args.L - 1),
             "variance": var,
-            "e2e": {"value": round(e2e, 6), "unit": "s per sweep pair (L=100, D=256)", "h2d_bytes_per_step": h2d,
+            "e2e": {"value": round(e2e, 6), "unit": unit_of(args), "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "roofline": roofline,
@@ -341,7 +381,7 @@ def cpu_baseline_same_state(args, sites, step_ms, psi):
         D1, D2 = a.shape[1], a.shape[2]
         w += heff_flops(d, Dw, Dw, D1, D2) / bulk
     est = per_site * 2.0 * w
-    return {"value": round(est, 3), "unit": "s per sweep pair (L=100, D=256)", "cores": ncores, "kind": "port",
+    return {"value": round(est, 3), "unit": unit_of(args), "cores": ncores, "kind": "port",
             "sample": f"{args.cpu_sites} bulk D={args.D} site updates (Lanczos Krylov 20 tol 1e-10 + QR gauge + "
                       f"environment) of the GPU's converged state in {sec:.2f}s ({nmv} matvecs); scaled by the "
                       f"Heff cost of all 2L site updates of a sweep pair"}
@@ -379,14 +419,14 @@ def run_reference(args, rank, world):
     sample = (f"{args.cpu_sites} bulk D={D} site updates (Lanczos Krylov 20 tol 1e-10 + QR gauge + environment) "
               f"of a random right-canonical L={L} MPS per step, scaled by the Heff cost of the 2L site updates "
               f"of a sweep pair; oracle C++ restatement (reference not buildable here)")
-    out = {"metric": METRIC, "value": round(value, 3), "unit": "s per sweep pair (L=100, D=256)",
+    out = {"metric": METRIC, "value": round(value, 3), "unit": unit_of(args),
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value * 1e3, 1),
            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic", "impl": "reference",
-           "config": {"workload": f"Heisenberg S=1/2 L={L}, one sweep pair at D={D}", "precision": "fp64"},
-           "cpu_baseline": {"value": round(value, 3), "unit": "s per sweep pair", "cores": ncores, "kind": "port",
+           "config": {"workload": workload_of(args), "precision": "fp64 (CPU oracle restatement)"},
+           "cpu_baseline": {"value": round(value, 3), "unit": unit_of(args), "cores": ncores, "kind": "port",
                             "sample": sample},
-           "e2e": {"value": round(value, 3), "unit": "s per sweep pair (L=100, D=256)", "h2d_bytes_per_step": 0,
+           "e2e": {"value": round(value, 3), "unit": unit_of(args), "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return out

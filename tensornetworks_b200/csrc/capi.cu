@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <cstdlib>
 #include <string>
 
 #include "engine.h"
@@ -14,6 +15,7 @@ static thread_local std::string g_last_error;
 static unsigned long long g_launches = 0;
 
 void count_launch() { __atomic_fetch_add(&g_launches, 1ULL, __ATOMIC_RELAXED); }
+unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 void set_error(const char* fmt, ...) {
     char buf[1024];
@@ -24,10 +26,22 @@ void set_error(const char* fmt, ...) {
     g_last_error = buf;
 }
 
+static unsigned long long g_alloc_gen = 0;
+unsigned long long alloc_generation() { return __atomic_load_n(&g_alloc_gen, __ATOMIC_RELAXED); }
+
+void Ctx::clear_graphs() {
+    for (auto& kv : lzgraphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    lzgraphs.clear();
+}
+
 int DevBuf::ensure(size_t nbytes) {
     if (nbytes <= bytes && p) return TN_OK;
     release();
     if (nbytes == 0) nbytes = 8;
+    __atomic_fetch_add(&g_alloc_gen, 1ULL, __ATOMIC_RELAXED);
     cudaError_t e = cudaMalloc(&p, nbytes);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -135,6 +149,7 @@ int tn_ctx_create(int device, tn_ctx* out) {
     tn_ctx c = new tn_ctx_s();
     c->c.device = device;
     c->c.sm_count = prop.multiProcessorCount;
+    if (const char* ng = std::getenv("TN_NO_GRAPHS")) c->c.use_graphs = !(ng[0] == '1');
     TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.own_stream, cudaStreamNonBlocking));
     c->c.stream = c->c.own_stream;
     TN_CUDA_CHECK(cudaEventCreate(&c->c.ev_a));
@@ -147,6 +162,7 @@ int tn_ctx_destroy(tn_ctx c) {
     if (!c) return TN_BAD_ARG;
     cudaSetDevice(c->c.device);
     cudaStreamSynchronize(c->c.stream);
+    c->c.clear_graphs();
     if (c->c.ev_a) cudaEventDestroy(c->c.ev_a);
     if (c->c.ev_b) cudaEventDestroy(c->c.ev_b);
     if (c->c.own_stream) cudaStreamDestroy(c->c.own_stream);

@@ -561,8 +561,16 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     // residual target: the requested tolerance, but not below the split operator's
     // noise floor relative to |T| (BF16x3 ~ 2^-16, BF16x6 ~ FP32 accumulation)
     const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-7);
+    // the operator: everything the recorded matvec launches depend on
+    unsigned long long key = hash_val(HASH_SEED, 0x6d69786564ULL);
+    key = hash_val(key, s);
+    key = hash_val(key, ns);
+    key = hash_val(key, (const void*)t);
+    key = hash_val(key, op.nLR);
+    for (const DevBuf* b : {&msite.Fs, &msite.Gs, &msite.Xs, &msite.P32, &msite.Qs, &msite.shifts, &msite.err})
+        key = hash_val(key, b->p);
     LzResult rm{};
-    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel));
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel, key));
     TN_CHECK(mixed_check_error(msite, st));
     matvecs += rm.matvecs;
     heff_flop += heff_flops(s) * rm.matvecs;
@@ -619,7 +627,12 @@ int MPSState::refine_site(int ia, double epsEigen) {
     LzResult r{};
     int krylov = opt.krylov > 0 ? opt.krylov : 20;
     int restarts = opt.max_restarts > 0 ? opt.max_restarts : 10;
-    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, &r));
+    unsigned long long key = hash_val(HASH_SEED, 0x66703634ULL);
+    key = hash_val(key, s);
+    for (const void* q : {(const void*)t, (const void*)F, (const void*)G, (const void*)P, (const void*)Q})
+        key = hash_val(key, q);
+    key = hash_val(key, op.nLR);
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, &r, 0.0, key));
     matvecs += r.matvecs;
     matvecs_fp64 += r.matvecs;
     heff_flop += heff_flops(s) * r.matvecs;
@@ -643,10 +656,13 @@ int MPSState::sweep(bool left, double epsEigen) {
     for (int step = 0; step < L; ++step) {
         const int ia = left ? 1 + step : L - step;
         auto t0 = now();
+        const unsigned long long n0 = launch_count();
         TN_CHECK(refine_site(ia, epsEigen));
         auto t1 = now();
+        const unsigned long long n1 = launch_count();
         TN_CHECK(normalize_site(ia, left));
         auto t2 = now();
+        const unsigned long long n2 = launch_count();
         if (left && ia < L) TN_CHECK(compute_left_env(ia));
         if (!left && ia > 1) TN_CHECK(compute_right_env(ia));
         auto t3 = now();
@@ -654,6 +670,13 @@ int MPSState::sweep(bool left, double epsEigen) {
             t_refine += secs(t0, t1);
             t_gauge += secs(t1, t2);
             t_env += secs(t2, t3);
+            n_refine += n1 - n0;
+            n_gauge += n2 - n1;
+            n_env += launch_count() - n2;
+            if (opt.verbose >= 3)
+                std::printf("site %d D1 %d D2 %d: refine %.1f us (%llu launches) gauge %.1f us (%llu) env %.1f us (%llu)\n",
+                            ia, D1[ia], D2[ia], 1e6 * secs(t0, t1), n1 - n0, 1e6 * secs(t1, t2), n2 - n1,
+                            1e6 * secs(t2, t3), launch_count() - n2);
         }
     }
     return TN_OK;
@@ -732,6 +755,7 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
     heff_flop = 0;
     not_converged = fallbacks = 0;
     t_refine = t_gauge = t_env = t_bond = 0;
+    n_refine = n_gauge = n_env = 0;
     TN_CUDA_CHECK(cudaEventRecord(ctx->ev_a, st));
     double dE = 0, dl = 0;
     for (int in = 0; in < nsweeps; ++in) {
@@ -746,8 +770,9 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
     float ms = 0;
     TN_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b));
     if (opt.verbose >= 2)
-        std::printf("phase seconds: refine %.4f gauge %.4f env %.4f bond-values %.4f (matvecs %lld, fp64 %lld)\n",
-                    t_refine, t_gauge, t_env, t_bond, matvecs, matvecs_fp64);
+        std::printf("phase seconds: refine %.4f gauge %.4f env %.4f bond-values %.4f (matvecs %lld, fp64 %lld); "
+                    "launches refine %llu gauge %llu env %llu\n",
+                    t_refine, t_gauge, t_env, t_bond, matvecs, matvecs_fp64, n_refine, n_gauge, n_env);
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         double e = 0;

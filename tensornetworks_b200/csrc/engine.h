@@ -59,6 +59,7 @@ struct MPSState {
     tn_solver_options opt{};
     // phase timing (verbose >= 2): seconds in refine / gauge / environment / bond values
     double t_refine = 0, t_gauge = 0, t_env = 0, t_bond = 0;
+    unsigned long long n_refine = 0, n_gauge = 0, n_env = 0;  // launches per phase (verbose >= 2)
 
     ~MPSState();
     int init(Hamiltonian* h, int D);

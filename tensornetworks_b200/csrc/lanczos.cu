@@ -150,11 +150,14 @@ __device__ void tri_solve(int n, const double* a, const double* b, double shift,
 
 // ---- kernels ---------------------------------------------------------------
 
-__global__ void lz_reset_kernel(LzState* st, double tol, double tol_rel, int first) {
+__global__ void lz_reset_kernel(LzState* st, double tol, double tol_rel, int first, int mmax) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         st->done = 0;
         st->nb = 0;
         st->counter = 0;
+        st->j = 0;
+        st->jn = 0;
+        st->mmax = mmax;
         if (first) {
             st->matvecs = 0;
             st->converged = 0;
@@ -193,27 +196,32 @@ __global__ void lz_norm_kernel(const double* __restrict__ x, long long N, double
     }
 }
 
-__global__ void lz_scale_kernel(const double* __restrict__ x, double* __restrict__ v0, long long N,
-                                const LzState* st, int fill_if_zero) {
+// v0 = x / |x| (and the matvec input copy xcur when given).
+__global__ void lz_scale_kernel(const double* x, double* v0, long long N, const LzState* st, int fill_if_zero,
+                                double* xcur) {
     double nr = st->xnorm;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
-        if (nr > 0) v0[i] = x[i] / nr;
+        double v;
+        if (nr > 0) v = x[i] / nr;
         else if (fill_if_zero) {
             // deterministic start vector when x = 0
             unsigned long long h = (unsigned long long)i * 0x9E3779B97F4A7C15ULL;
             h ^= h >> 29;
-            v0[i] = ((double)((h >> 11) & 0xFFFFF) / 1048576.0 - 0.5) / sqrt((double)N / 12.0);
-        } else v0[i] = 0.0;
+            v = ((double)((h >> 11) & 0xFFFFF) / 1048576.0 - 0.5) / sqrt((double)N / 12.0);
+        } else v = 0.0;
+        v0[i] = v;
+        if (xcur) xcur[i] = v;
     }
 }
 
 // h_k = V_k . w for k = 0..j  (partials per block, last block reduces).
-__global__ void lz_dots_kernel(const double* __restrict__ V, const double* __restrict__ w, long long N, int j,
+__global__ void lz_dots_kernel(const double* __restrict__ V, const double* __restrict__ w, long long N,
                                double* partial, LzState* st) {
     if (st->done) return;
     __shared__ double sh[KCHUNK * 32];
     __shared__ double res[KCHUNK];
     __shared__ bool last;
+    const int j = st->j;
     const int nk = j + 1;
     for (int k0 = 0; k0 < nk; k0 += KCHUNK) {
         double v[KCHUNK] = {0};
@@ -246,14 +254,22 @@ __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __res
 }
 
 // w' = w - V h;  h2 = V^T w';  nrm2 = |w'|^2.  The last block forms alpha_j,
-// beta_j, solves the tridiagonal problem and sets the convergence flag.
-__global__ void lz_update_kernel(const double* __restrict__ V, double* __restrict__ w, long long N, int j,
-                                 int mmax, double* partial, LzState* st) {
-    if (st->done) return;
+// beta_j, solves the tridiagonal problem and sets the convergence flag.  Inside
+// a graph loop (cond != 0) it also decides whether the loop runs another step:
+// every step reaches this last block, and it ends the loop at the latest when
+// the basis limit is reached, so the loop always terminates.
+__global__ void lz_update_kernel(const double* __restrict__ V, double* __restrict__ w, long long N,
+                                 double* partial, LzState* st, cudaGraphConditionalHandle cond) {
+    if (st->done) {
+        if (cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+        return;
+    }
     __shared__ double sh[KCHUNK * 32];
     __shared__ double res[KCHUNK];
     __shared__ double hs[LZ_MAXK];
     __shared__ bool last;
+    const int j = st->j;
+    const int mmax = st->mmax;
     const int nk = j + 1;
     for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h[k];
     __syncthreads();
@@ -327,15 +343,21 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
         // split-precision operator: a residual that no longer halves over two
         // steps has reached the operator's noise floor
         if (st->tol_rel > 0 && j >= 2 && resid > 0.5 * st->rhist[j - 2]) st->done = 1;
-        if (nk >= mmax) st->done = 1;  // basis exhausted for this restart
+        if (nk >= mmax || nk >= LZ_MAXK - 1) st->done = 1;  // basis exhausted for this restart
+        st->jn = j + 1;
+        if (cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
     }
 }
 
-// V_{j+1} = (w' - V h2) / beta_j
-__global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N, int j, LzState* st) {
+// V_{j+1} = (w' - V h2) / beta_j, also into the matvec input xcur; the last
+// block advances the step index (the other blocks read only jn).
+__global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N, LzState* st,
+                               double* __restrict__ xcur) {
     if (st->done) return;
     __shared__ double hs[LZ_MAXK];
     __shared__ double inv;
+    __shared__ bool last;
+    const int j = st->jn - 1;
     const int nk = j + 1;
     for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h2[k];
     if (threadIdx.x == 0) inv = 1.0 / st->beta[j];
@@ -344,7 +366,20 @@ __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict_
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         double wi = w[i];
         for (int k = 0; k < nk; ++k) wi = fma(-hs[k], V[(long long)k * N + i], wi);
-        vn[i] = wi * inv;
+        wi *= inv;
+        vn[i] = wi;
+        xcur[i] = wi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int prev = atomicAdd(&st->counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        st->j = j + 1;
+        st->counter = 0;
     }
 }
 
@@ -463,7 +498,7 @@ inline int vec_grid(long long N, int sm) {
 }  // namespace
 
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                  LzResult* out, double tol_rel) {
+                  LzResult* out, double tol_rel, unsigned long long graph_key) {
     cudaStream_t st = c.stream;
     if (N <= 0) return TN_BAD_SHAPE;
     int mm = m;
@@ -471,38 +506,90 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
     if ((long long)mm > N) mm = (int)N;
     if (mm < 1) mm = 1;
     const int grid = vec_grid(N, c.sm_count);
-    // workspace: V (mm+1 vectors), w, partials
-    size_t need = sizeof(double) * ((size_t)(mm + 2) * N + (size_t)grid * LZ_MAXK + 64);
+    // workspace: V (mm+1 vectors), w, xcur, partials
+    size_t need = sizeof(double) * ((size_t)(mm + 3) * N + (size_t)grid * LZ_MAXK + 64);
     TN_CHECK(c.lz.ensure(need));
     TN_CHECK(c.lzstate.ensure(sizeof(LzState)));
     TN_CHECK(c.pinned.ensure(sizeof(LzState)));
     double* V = c.lz.as<double>();
     double* w = V + (size_t)(mm + 1) * N;
-    double* partial = w + N;
+    double* xcur = w + N;
+    double* partial = xcur + N;
     LzState* s = c.lzstate.as<LzState>();
     LzState* hs = reinterpret_cast<LzState*>(c.pinned.p);
+
+    // one Lanczos step; cond != 0 inside the graph body
+    auto enqueue_step = [&](cudaGraphConditionalHandle cond) -> int {
+        TN_CHECK(mv(xcur, w, &s->done));
+        lz_dots_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, partial, s);
+        TN_LAUNCH_CHECK();
+        lz_update_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, partial, s, cond);
+        TN_LAUNCH_CHECK();
+        lz_next_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, s, xcur);
+        TN_LAUNCH_CHECK();
+        return TN_OK;
+    };
+
+    LzGraph* gr = nullptr;
+    if (graph_key && c.use_graphs && st != nullptr) {
+        unsigned long long key = graph_key;
+        key = hash_val(key, N);
+        key = hash_val(key, mm);
+        key = hash_val(key, grid);
+        key = hash_val(key, (const void*)V);
+        key = hash_val(key, (const void*)s);
+        key = hash_val(key, st);
+        key = hash_val(key, alloc_generation());
+        auto it = c.lzgraphs.find(key);
+        if (it == c.lzgraphs.end()) {
+            if (c.lzgraphs.size() >= 256) c.clear_graphs();
+            LzGraph g;
+            TN_CUDA_CHECK(cudaGraphCreate(&g.graph, 0));
+            cudaGraphConditionalHandle h;
+            TN_CUDA_CHECK(cudaGraphConditionalHandleCreate(&h, g.graph, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            TN_CUDA_CHECK(cudaGraphAddNode(&node, g.graph, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            const unsigned long long n0 = launch_count();
+            TN_CUDA_CHECK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            int rc = enqueue_step(h);
+            cudaGraph_t captured = nullptr;
+            cudaError_t ec = cudaStreamEndCapture(st, &captured);
+            g.kernels_per_iter = launch_count() - n0;
+            if (rc != TN_OK || ec != cudaSuccess) {
+                cudaGraphDestroy(g.graph);
+                if (rc != TN_OK) return rc;
+                TN_CUDA_CHECK(ec);
+            }
+            cudaError_t ei = cudaGraphInstantiate(&g.exec, g.graph, 0);
+            if (ei != cudaSuccess) {
+                cudaGraphDestroy(g.graph);
+                TN_CUDA_CHECK(ei);
+            }
+            it = c.lzgraphs.emplace(key, g).first;
+        }
+        gr = &it->second;
+    }
 
     int restarts = 0;
     bool converged = false;
     double prev_resid = 1e300;
     for (restarts = 0; restarts < (maxRestarts > 0 ? maxRestarts : 1); ++restarts) {
-        lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, restarts == 0);
+        lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, restarts == 0, mm);
         TN_LAUNCH_CHECK();
         lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
         TN_LAUNCH_CHECK();
-        lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, V, N, s, 1);
+        lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, V, N, s, 1, xcur);
         TN_LAUNCH_CHECK();
-        for (int j = 0; j < mm; ++j) {
-            double* vj = V + (size_t)j * N;
-            TN_CHECK(mv(vj, w, &s->done));
-            lz_dots_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, j, partial, s);
-            TN_LAUNCH_CHECK();
-            lz_update_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, j, mm, partial, s);
-            TN_LAUNCH_CHECK();
-            if (j + 1 < mm) {
-                lz_next_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, j, s);
-                TN_LAUNCH_CHECK();
-            }
+        if (gr) {
+            TN_CUDA_CHECK(cudaGraphLaunch(gr->exec, st));
+        } else {
+            for (int j = 0; j < mm; ++j) TN_CHECK(enqueue_step(0));
         }
         lz_ritz_coeffs_kernel<<<1, LZ_THREADS, 0, st>>>(s);
         TN_LAUNCH_CHECK();
@@ -510,6 +597,9 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         TN_LAUNCH_CHECK();
         TN_CUDA_CHECK(cudaMemcpyAsync(hs, s, sizeof(LzState), cudaMemcpyDeviceToHost, st));
         TN_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (gr)  // kernels the graph ran: one body per step taken
+            for (int k = 0; k < hs->nb; ++k)
+                for (unsigned long long q = 0; q < gr->kernels_per_iter; ++q) count_launch();
         if (hs->converged) { converged = true; ++restarts; break; }
         if ((long long)mm >= N) { converged = true; ++restarts; break; }  // full space spanned: exact
         if (tol_rel > 0) {
@@ -519,11 +609,11 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         }
     }
     // final normalisation of the Ritz vector
-    lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0);
+    lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0, mm);
     TN_LAUNCH_CHECK();
     lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
     TN_LAUNCH_CHECK();
-    lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, x, N, s, 0);
+    lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, x, N, s, 0, nullptr);
     TN_LAUNCH_CHECK();
     if (out) {
         out->theta = hs->theta;

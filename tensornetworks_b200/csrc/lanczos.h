@@ -14,7 +14,9 @@ struct LzState {
     int matvecs;           // Heff applications so far
     int converged;         // residual criterion met
     unsigned int counter;  // last-block reduction ticket
-    int pad;
+    int j;                 // step of the current restart (read by dots / update)
+    int jn;                // index of the vector lz_next builds (set by update)
+    int mmax;              // basis limit of the current restart
     double tol, theta, theta2, resid, xnorm;
     double tol_rel;        // additional residual target relative to |T| (split-precision operators)
     double alpha[LZ_MAXK], beta[LZ_MAXK];
@@ -29,7 +31,8 @@ struct LzResult {
 };
 
 // mv(x, y, skip): enqueue y = Heff x on the context stream; the launches must
-// do nothing when *skip != 0 (device flag).
+// do nothing when *skip != 0 (device flag).  The solver always passes the same
+// x and y buffers, so the launches can be recorded once in a CUDA graph.
 using MatvecFn = std::function<int(const double*, double*, const int*)>;
 
 // theta = x.y/x.x and |y - theta x|/|x| (device vectors; synchronises).
@@ -39,7 +42,10 @@ int rayleigh_residual(Ctx& c, long long N, const double* x, const double* y, dou
 // the norm of the tridiagonal matrix (the operator's noise floor for the
 // split-precision matvec).  With tol_rel > 0 the restarts also stop once the
 // residual no longer drops by half between restarts.
+// graph_key != 0 identifies the operator (every pointer and shape mv's launches
+// depend on): the Lanczos steps of a restart then run as one CUDA graph with a
+// device-driven WHILE loop, recorded on first use of the key and replayed.
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                  LzResult* out, double tol_rel = 0.0);
+                  LzResult* out, double tol_rel = 0.0, unsigned long long graph_key = 0);
 
 }  // namespace tnb

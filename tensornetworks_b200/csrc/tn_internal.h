@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/tn_cuda.h"
@@ -32,11 +33,27 @@ void set_error(const char* fmt, ...);
 // Every launch site calls TN_LAUNCH_CHECK once per kernel launch: it checks the
 // launch and counts it (tn_launch_count).
 void count_launch();
+unsigned long long launch_count();
 #define TN_LAUNCH_CHECK()                 \
     do {                                  \
         ::tnb::count_launch();            \
         TN_CUDA_CHECK(cudaGetLastError()); \
     } while (0)
+
+// Incremented by every device (re)allocation of a DevBuf: captured CUDA graphs
+// hold raw pointers, so a graph recorded under another generation is stale.
+unsigned long long alloc_generation();
+
+// FNV-1a over raw bytes (graph-cache keys).
+inline unsigned long long hash_bytes(unsigned long long h, const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ULL;
+    return h;
+}
+template <class T> inline unsigned long long hash_val(unsigned long long h, const T& v) {
+    return hash_bytes(h, &v, sizeof(T));
+}
+constexpr unsigned long long HASH_SEED = 1469598103934665603ULL;
 
 // Growable device buffer (bytes); contents are not preserved on growth.
 struct DevBuf {
@@ -105,6 +122,14 @@ struct WTerm {
     double c;
 };
 
+// One Lanczos iteration (matvec + dots + update + next) recorded as the body
+// of a conditional WHILE node: the device decides when the loop ends.
+struct LzGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels_per_iter = 0;
+};
+
 // Execution context (one per tn_ctx handle).
 struct Ctx {
     int device = 0;
@@ -127,6 +152,10 @@ struct Ctx {
     std::vector<double> wcache_W;
     int wcache_key[4] = {0, 0, 0, 0};
     int wcache_n = 0;
+    // device-looped Lanczos graphs by operator key (TN_NO_GRAPHS=1 disables)
+    std::unordered_map<unsigned long long, LzGraph> lzgraphs;
+    bool use_graphs = true;
+    void clear_graphs();
 };
 
 }  // namespace tnb
