@@ -188,6 +188,22 @@ unsigned long long tn_launch_count(void);
 int tn_heff_matvec(tn_ctx ctx, int precision, int d, int Dw1, int Dw2, int D1, int D2,
                    const double* W_host, const double* F, const double* G,
                    const double* x, double* y);
+/* tn_heff_matvec with precision TN_PREC_FP64, allocating no memory: the MPO
+ * term list and both contraction stage buffers live in a fixed device array
+ * of TN_HEFF_STATIC_MAX_DOUBLES doubles (8 MiB) per device.  No counterpart in
+ * the reference.  Limits: 2*d*max(Dw1,Dw2)*max(D1,D2)^2 doubles plus the term
+ * list must fit (d=2, Dw=5: D1, D2 <= 224; D = 256 is rejected with
+ * TN_BAD_SHAPE and a message in tn_last_error).  The first call on a device
+ * looks up the array's address (device current) and should precede any
+ * stream capture.  All calls on one device share the array: calls that may
+ * overlap (other threads, streams or contexts on the same device) race and
+ * must be serialised by the caller.  Nothing in the array needs to start at
+ * zero.  The call enqueues on the context stream and returns without
+ * synchronising. */
+#define TN_HEFF_STATIC_MAX_DOUBLES (1 << 20)
+int tn_heff_matvec_static(tn_ctx ctx, int d, int Dw1, int Dw2, int D1, int D2,
+                          const double* W_host, const double* F, const double* G,
+                          const double* x, double* y);
 /* Heff operator object: the device-side SparseEigenSolverClient
  * (SparseEigenSolver.H:17-24) of one site.  Creation uploads W and, for the
  * split-precision modes, splits F and G into BF16 pieces once; apply is then

@@ -88,6 +88,7 @@ SIGNATURES = {
     "tn_mps_prepare_sweeps": (_I, [_V, _V]),
     "tn_launch_count": (C.c_ulonglong, []),
     "tn_heff_matvec": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _V, _V]),
+    "tn_heff_matvec_static": (_I, [_V, _I, _I, _I, _I, _I, _V, _V, _V, _V, _V]),
     "tn_heff_diag": (_I, [_V, _I, _I, _I, _I, _I, _V, _V, _V, _V]),
     "tn_heff_create": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _PV]),
     "tn_heff_size": (C.c_longlong, [_V]),
