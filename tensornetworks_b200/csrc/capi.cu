@@ -293,6 +293,9 @@ int tn_mps_set_site(tn_mps m, int site, int D1, int D2, const double* A) {
     TN_CUDA_CHECK(cudaMemcpy(s.A[site]->p, A, sizeof(double) * (size_t)s.d * D1 * D2, cudaMemcpyHostToDevice));
     s.D1[site] = D1;
     s.D2[site] = D2;
+    // a new shape changes the adjacent bonds' dimensions (Bond::NewBondDimension)
+    if (site > 1 && s.bondK[site - 1] != D1) s.set_bond_dim(site - 1, D1);
+    if (site < s.L && s.bondK[site] != D2) s.set_bond_dim(site, D2);
     return TN_OK;
 }
 

@@ -683,23 +683,27 @@ int MPSState::sweep(bool left, double epsEigen) {
 }
 
 // MPSImp::IncreaseBondDimensions (MPSImp.C:123-147) with Bond::NewBondDimension (Bond.C:60-84).
+// Bond::NewBondDimension (Bond.C:60-84): pad s with min(s)/10 (or truncate), renormalise.
+void MPSState::set_bond_dim(int b, int nD) {
+    std::vector<double>& s = bond_s[b];
+    int oD = (int)s.size();
+    if (nD > oD) {
+        double mn = s.empty() ? 1.0 : *std::min_element(s.begin(), s.end());
+        s.resize(nD, mn / 10.0);
+    } else {
+        s.resize(nD);
+    }
+    double nrm = 0;
+    for (double v : s) nrm += v * v;
+    nrm = std::sqrt(nrm);
+    if (nrm > 0)
+        for (double& v : s) v /= nrm;
+    bondK[b] = nD;
+}
+
 int MPSState::increase_bond_dims(int D) {
     TN_CHECK(ensure_capacity(std::max(D, max_D())));
-    auto bond_new = [&](int b, int nD) {
-        std::vector<double>& s = bond_s[b];
-        int oD = (int)s.size();
-        if (nD > oD) {
-            double mn = s.empty() ? 1.0 : *std::min_element(s.begin(), s.end());
-            s.resize(nD, mn / 10.0);
-        } else {
-            s.resize(nD);
-        }
-        double nrm = 0;
-        for (double v : s) nrm += v * v;
-        nrm = std::sqrt(nrm);
-        for (double& v : s) v /= nrm;
-        bondK[b] = nD;
-    };
+    auto bond_new = [&](int b, int nD) { set_bond_dim(b, nD); };
     // Dideal = d^k saturates at D (the reference's int product overflows beyond L ~ 60)
     long long Dideal = 1;
     int ia = 1;

@@ -69,7 +69,8 @@ struct MPSState {
     int normalize_site(int ia, bool left);
     int normalize_all(bool left);
     int bond_values(const std::vector<std::pair<int, int>>& which, std::vector<std::vector<double>>& out);
-    int ensure_bond_values();           // bond_s from the latest factor of every dirty bond
+    int ensure_bond_values();
+    void set_bond_dim(int b, int nD);   // Bond::NewBondDimension           // bond_s from the latest factor of every dirty bond
     int sweep_pair_dlambda(double* dl); // Bond::GetMaxDelta over the last two half-sweeps
     int compute_left_env(int ia);
     int compute_right_env(int ia);
