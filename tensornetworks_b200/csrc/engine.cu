@@ -17,6 +17,7 @@
 //   * the eigensolver is matrix-free (Lanczos/Davidson) instead of a dense
 //     zheevx on the materialised Heff.
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <cmath>
 #include <cstring>

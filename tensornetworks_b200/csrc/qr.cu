@@ -135,21 +135,21 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(double* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// Register-resident panel (m <= 1024 rows).  Thread t owns rows t + k*256
+// Register-resident panel (m <= NT*R rows).  Thread t of NT owns rows t + k*NT
 // (R rows of B columns in registers), so each column step costs two block
 // reductions and two barriers: the norm of the sub-column, then one
 // reduce-scatter of v^T P over every other column of the panel.  The same
-// reduce-scatter yields V(:,0:jj)^T v_jj, from which warp 0 appends column jj
-// of the dlarft T factor.  Reflectors follow the dlarfg convention as above.
+// reduce-scatter yields V(:,0:jj)^T v_jj (the Gram column of the reflectors),
+// from which lane i of warp 0 builds row i of the dlarft T factor at the end.
+// Reflectors follow the dlarfg convention as above.
 //
 // Register indices must be compile-time, but unrolling all B column steps is
-// instruction-fetch bound; so the loop runs over groups of QRP_U steps and
-// the register window rotates by QRP_U columns per group.  At the start of a
-// group (first column jj0) slot i holds column jj0 + i for i < B - jj0 and
-// the finished reflector l < jj0 sits in slot B - jj0 + l.
-constexpr int QRP_THREADS = 256;
-constexpr int QRP_WARPS = QRP_THREADS / 32;
-constexpr int QRP_U = 2;
+// instruction-fetch bound; so the loop runs over groups of U steps and the
+// register window rotates by U columns per group.  At the start of a group
+// (first column jj0) slot i holds column jj0 + i for i < B - jj0 and the
+// finished reflector l < jj0 sits in slot B - jj0 + l.  (Measured: 256 x 2 x
+// 32 with U = 2 is as fast as 128 x 4 x 16, 256 x 2 x 16 and U = 1; 512
+// threads are slower.)
 
 // Reduce-scatter of B per-lane values over the warp: afterwards lane l holds
 // the warp's sum for slot (l mod B).  B is 16 or 32; f(i) yields slot i.
@@ -185,11 +185,12 @@ __device__ __forceinline__ double warp_reduce_scatter(F f) {
     return h[0];
 }
 
-template <int R, int B>
-__global__ void __launch_bounds__(QRP_THREADS) qr_panel_reg_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
-                                                                     double* __restrict__ V, int ldv,
-                                                                     double* __restrict__ T, int ldt) {
-    static_assert(B % QRP_U == 0, "panel width must be a multiple of the group size");
+template <int NT, int R, int B, int U>
+__global__ void __launch_bounds__(NT) qr_panel_reg_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                                            double* __restrict__ V, int ldv,
+                                                            double* __restrict__ T, int ldt) {
+    static_assert(B % U == 0, "panel width must be a multiple of the group size");
+    constexpr int QRP_THREADS = NT, QRP_WARPS = NT / 32;
     __shared__ double redN[QRP_WARPS];
     __shared__ double redD[QRP_WARPS][32];
     __shared__ double gsh[QRP_WARPS][32];
@@ -207,10 +208,10 @@ __global__ void __launch_bounds__(QRP_THREADS) qr_panel_reg_kernel(double* __res
             p[k][c] = (r < mp && c < b) ? W[(size_t)(j0 + c) * ldw + j0 + r] : 0.0;
     }
 #pragma unroll 1
-    for (int jj0 = 0; jj0 < b; jj0 += QRP_U) {
+    for (int jj0 = 0; jj0 < b; jj0 += U) {
         const int last_trail = B - 1 - jj0;  // slots u+1 .. last_trail are trailing columns
 #pragma unroll
-        for (int u = 0; u < QRP_U; ++u) {
+        for (int u = 0; u < U; ++u) {
             const int jj = jj0 + u;
             if (jj >= b) break;
             double part = 0;
@@ -282,20 +283,20 @@ __global__ void __launch_bounds__(QRP_THREADS) qr_panel_reg_kernel(double* __res
                 if (lane == 0) taus[jj] = t;
             }
         }
-        // rotate the window left by QRP_U columns
+        // rotate the window left by U columns
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            double keep[QRP_U];
+            double keep[U];
 #pragma unroll
-            for (int i = 0; i < QRP_U; ++i) keep[i] = p[k][i];
+            for (int i = 0; i < U; ++i) keep[i] = p[k][i];
 #pragma unroll
-            for (int i = 0; i < B - QRP_U; ++i) p[k][i] = p[k][i + QRP_U];
+            for (int i = 0; i < B - U; ++i) p[k][i] = p[k][i + U];
 #pragma unroll
-            for (int i = 0; i < QRP_U; ++i) p[k][B - QRP_U + i] = keep[i];
+            for (int i = 0; i < U; ++i) p[k][B - U + i] = keep[i];
         }
     }
     // after the groups slot i holds column (i + rb) mod B, rb = b rounded up to the group size
-    const int rb = ((b + QRP_U - 1) / QRP_U) * QRP_U;
+    const int rb = ((b + U - 1) / U) * U;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int r = tid + k * QRP_THREADS;
@@ -469,7 +470,7 @@ int panel_width(int m) {
 
 namespace {
 
-template <int R, int B>
+template <int NT, int R, int B, int U>
 int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
     cudaStream_t st = c.stream;
     const int k = std::min(m, n);
@@ -477,7 +478,7 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
     int dev = 0;
     TN_CUDA_CHECK(cudaGetDevice(&dev));
     if (attr_set[B == 32] != dev) {
-        const int bytes = (int)wy_smem_bytes(B == 32 ? 2 * QRP_THREADS : 4 * QRP_THREADS, B);
+        const int bytes = (int)wy_smem_bytes(B == 32 ? 512 : 1024, B);
         TN_CUDA_CHECK(cudaFuncSetAttribute(wy_apply_kernel<B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         TN_CUDA_CHECK(cudaFuncSetAttribute(wy_apply_kernel<B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         attr_set[B == 32] = dev;
@@ -491,7 +492,7 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
         const int mp = m - j0;
         double* Vp = Vall + (size_t)j0 * m + j0;  // ld m
         double* Tp = Tall + (size_t)j0 * B;        // ld B
-        qr_panel_reg_kernel<R, B><<<1, QRP_THREADS, 0, st>>>(W, m, m, j0, b, Vp, m, Tp, B);
+        qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, st>>>(W, m, m, j0, b, Vp, m, Tp, B);
         TN_LAUNCH_CHECK();
         const int nt = n - j0 - b;
         if (nt > 0) {
@@ -525,8 +526,8 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
 int qr_dense(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
     cudaStream_t st = c.stream;
     if (m <= 0 || n <= 0) return TN_BAD_SHAPE;
-    if (m <= 2 * QRP_THREADS) return qr_dense_reg<2, 32>(c, m, n, W, Qout, ldq, Rout, ldr);
-    if (m <= 4 * QRP_THREADS) return qr_dense_reg<4, 16>(c, m, n, W, Qout, ldq, Rout, ldr);
+    if (m <= 512) return qr_dense_reg<256, 2, 32, 2>(c, m, n, W, Qout, ldq, Rout, ldr);
+    if (m <= 1024) return qr_dense_reg<256, 4, 16, 2>(c, m, n, W, Qout, ldq, Rout, ldr);
     const int k = std::min(m, n);
     const int bmax = panel_width(m);
     if ((size_t)m * bmax * 8 > 200 * 1024 || bmax < 1) {
