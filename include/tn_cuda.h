@@ -113,7 +113,10 @@ typedef struct {
     double last_dE;         /* GetMaxDeltaE() after the last sweep pair      */
     double last_dlambda;    /* GetMaxDeltal() after the last sweep pair      */
     int    not_converged;   /* site solves that hit the iteration cap        */
-    int    fallbacks;       /* learned-preconditioner fallbacks taken        */
+    int    fallbacks;       /* learned-correction stalls (diagonal Davidson
+                               took over) plus FP64 refinements of the mixed
+                               path                                          */
+    long long learned_steps; /* Davidson corrections the learned MLP made    */
 } tn_sweep_stats;
 
 /* ---- context ------------------------------------------------------------- */
@@ -255,6 +258,41 @@ int tn_lq(tn_ctx ctx, int m, int n, const double* A, int lda, double* L, int ldl
  * D columns/rows.  Returns the kept D and the discarded sum of s^2. */
 int tn_compress(tn_ctx ctx, int Dmax, double eps, int k, double* s, int* D_out,
                 double* discarded);
+
+/* ---- learned Davidson correction (no counterpart in the reference) -------
+ * A per-element MLP (4 -> 64 -> 64 -> 1, tanh; BF16 weights for inference,
+ * FP32 master copy for training) maps (diag(Heff) - theta)/sigma, r/rms(r),
+ * u*sqrt(N) and the bond position to the normalised Davidson correction.  It
+ * is trained on pairs that FP64 diagonal-Davidson sweeps record (target: the
+ * exact correction x/(u.x) - u towards the converged eigenvector x).  Sweeps
+ * use it with tn_solver_options.eigensolver = TN_EIG_DAVIDSON and
+ * use_learned = 1; diagonal Davidson takes over whenever it stalls. */
+typedef struct tn_mlp_s* tn_mlp;
+typedef struct tn_dataset_s* tn_dataset;
+int tn_mlp_create(tn_ctx ctx, uint64_t seed, tn_mlp* out);
+int tn_mlp_destroy(tn_mlp m);
+int tn_mlp_num_params(void);
+/* FP32 master parameters (layout W1[4][64], b1[64], W2[64][64], b2[64],
+ * W3[64], b3); setting them also refreshes the BF16 copy and resets Adam. */
+int tn_mlp_get_params(tn_mlp m, float* host);
+int tn_mlp_set_params(tn_mlp m, const float* host);
+/* Y[i] = MLP(F[i, 0:4]) with the BF16 weights (device pointers). */
+int tn_mlp_forward(tn_mlp m, const float* F, long long n, float* Y);
+/* Gradient of mean((MLP(F) - T)^2) w.r.t. the FP32 parameters (host, n_params). */
+int tn_mlp_gradient(tn_mlp m, const float* F, const float* T, long long n, float* grad_host,
+                    double* loss);
+/* Adam on minibatches of a seeded permutation of the n pairs. */
+int tn_mlp_train(tn_mlp m, const float* F, const float* T, long long n, int steps, int batch,
+                 double lr, uint64_t seed, double* final_loss);
+/* Training pairs recorded by FP64 diagonal-Davidson sweeps. */
+int tn_dataset_create(tn_ctx ctx, long long capacity, tn_dataset* out);
+int tn_dataset_destroy(tn_dataset ds);
+long long tn_dataset_size(tn_dataset ds);
+/* Device pointers: features (size x 4 floats) and targets (size floats). */
+int tn_dataset_data(tn_dataset ds, const float** F, const float** T);
+/* Attach (or detach with NULL) the learned correction / the recorder. */
+int tn_mps_set_learned_correction(tn_mps psi, tn_mlp m);
+int tn_mps_set_recorder(tn_mps psi, tn_dataset ds);
 
 #ifdef __cplusplus
 }

@@ -48,7 +48,7 @@ class SweepStats(C.Structure):
                 ("total_sweeps", C.c_int), ("final_D", C.c_int), ("matvecs", C.c_longlong),
                 ("matvecs_fp64", C.c_longlong), ("heff_flop", C.c_double), ("heff_ms", C.c_double),
                 ("sweep_ms", C.c_double), ("last_dE", C.c_double), ("last_dlambda", C.c_double),
-                ("not_converged", C.c_int), ("fallbacks", C.c_int)]
+                ("not_converged", C.c_int), ("fallbacks", C.c_int), ("learned_steps", C.c_longlong)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -89,6 +89,20 @@ SIGNATURES = {
     "tn_launch_count": (C.c_ulonglong, []),
     "tn_heff_matvec": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _V, _V]),
     "tn_heff_matvec_static": (_I, [_V, _I, _I, _I, _I, _I, _V, _V, _V, _V, _V]),
+    "tn_mlp_create": (_I, [_V, _ULL, _PV]),
+    "tn_mlp_destroy": (_I, [_V]),
+    "tn_mlp_num_params": (_I, []),
+    "tn_mlp_get_params": (_I, [_V, _V]),
+    "tn_mlp_set_params": (_I, [_V, _V]),
+    "tn_mlp_forward": (_I, [_V, _V, C.c_longlong, _V]),
+    "tn_mlp_gradient": (_I, [_V, _V, _V, C.c_longlong, _V, _PD]),
+    "tn_mlp_train": (_I, [_V, _V, _V, C.c_longlong, _I, _I, _D, _ULL, _PD]),
+    "tn_dataset_create": (_I, [_V, C.c_longlong, _PV]),
+    "tn_dataset_destroy": (_I, [_V]),
+    "tn_dataset_size": (C.c_longlong, [_V]),
+    "tn_dataset_data": (_I, [_V, _PV, _PV]),
+    "tn_mps_set_learned_correction": (_I, [_V, _V]),
+    "tn_mps_set_recorder": (_I, [_V, _V]),
     "tn_heff_diag": (_I, [_V, _I, _I, _I, _I, _I, _V, _V, _V, _V]),
     "tn_heff_create": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _PV]),
     "tn_heff_size": (C.c_longlong, [_V]),

@@ -305,10 +305,121 @@ class MPS:
         self.last_stats = st.as_dict()
         return self.last_stats
 
+    def SetLearnedCorrection(self, model: Optional["LearnedCorrection"]):
+        """Attach (None: detach) the learned Davidson correction used when the
+        options select eigensolver=DAVIDSON with use_learned=1."""
+        self._mlp = model  # keep it alive while attached
+        check(self._lib.tn_mps_set_learned_correction(self.handle, model.handle if model is not None else None),
+              "tn_mps_set_learned_correction")
+
+    def SetRecorder(self, ds: Optional["TrainingSet"]):
+        """Record (feature, exact-correction) pairs in FP64 diagonal-Davidson sweeps."""
+        self._rec = ds
+        check(self._lib.tn_mps_set_recorder(self.handle, ds.handle if ds is not None else None),
+              "tn_mps_set_recorder")
+
     def __del__(self):  # pragma: no cover
         try:
             if getattr(self, "handle", None):
                 self._lib.tn_mps_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Learned Davidson correction (no reference counterpart)
+# ---------------------------------------------------------------------------
+class _DevArray:
+    """__cuda_array_interface__ view of library-owned device memory (float32)."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+class TrainingSet:
+    """Device buffer of (features[4], target) pairs filled by FP64 diagonal-Davidson sweeps."""
+
+    def __init__(self, capacity: int, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self._lib = self.ctx._lib
+        h = C.c_void_p()
+        check(self._lib.tn_dataset_create(self.ctx.handle, int(capacity), C.byref(h)), "tn_dataset_create")
+        self.handle = h
+
+    def __len__(self):
+        return int(self._lib.tn_dataset_size(self.handle))
+
+    def device_arrays(self):
+        """(features, targets) as torch CUDA tensors viewing the library's buffers."""
+        torch = _torch()
+        fp, tp = C.c_void_p(), C.c_void_p()
+        check(self._lib.tn_dataset_data(self.handle, C.byref(fp), C.byref(tp)), "tn_dataset_data")
+        n = len(self)
+        F = torch.as_tensor(_DevArray(fp.value or 0, (n, 4)), device="cuda")
+        T = torch.as_tensor(_DevArray(tp.value or 0, (n,)), device="cuda")
+        return F, T
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if getattr(self, "handle", None):
+                self._lib.tn_dataset_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class LearnedCorrection:
+    """Per-element MLP (4 -> 64 -> 64 -> 1, tanh) for the Davidson correction;
+    BF16 weights for inference, FP32 master copy trained with Adam on the GPU."""
+
+    def __init__(self, seed: int = 1, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self._lib = self.ctx._lib
+        h = C.c_void_p()
+        check(self._lib.tn_mlp_create(self.ctx.handle, int(seed), C.byref(h)), "tn_mlp_create")
+        self.handle = h
+        self.n_params = int(self._lib.tn_mlp_num_params())
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.n_params, dtype=np.float32)
+        check(self._lib.tn_mlp_get_params(self.handle, out.ctypes.data), "tn_mlp_get_params")
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.n_params
+        check(self._lib.tn_mlp_set_params(self.handle, p.ctypes.data), "tn_mlp_set_params")
+
+    def forward(self, F):
+        """F: (n, 4) float32 CUDA tensor -> (n,) outputs (BF16 weights)."""
+        torch = _torch()
+        F = F.contiguous()
+        Y = torch.empty(F.shape[0], dtype=torch.float32, device=F.device)
+        check(self._lib.tn_mlp_forward(self.handle, F.data_ptr(), int(F.shape[0]), Y.data_ptr()), "tn_mlp_forward")
+        return Y
+
+    def gradient(self, F, T):
+        """Gradient of mean((MLP(F) - T)^2) w.r.t. the FP32 parameters, and the loss."""
+        F, T = F.contiguous(), T.contiguous()
+        g = np.empty(self.n_params, dtype=np.float32)
+        loss = C.c_double()
+        check(self._lib.tn_mlp_gradient(self.handle, F.data_ptr(), T.data_ptr(), int(F.shape[0]), g.ctypes.data,
+                                        C.byref(loss)), "tn_mlp_gradient")
+        return g, loss.value
+
+    def train(self, F, T, steps: int = 2000, batch: int = 4096, lr: float = 2e-3, seed: int = 7) -> float:
+        F, T = F.contiguous(), T.contiguous()
+        loss = C.c_double()
+        check(self._lib.tn_mlp_train(self.handle, F.data_ptr(), T.data_ptr(), int(F.shape[0]), int(steps),
+                                     int(batch), float(lr), int(seed), C.byref(loss)), "tn_mlp_train")
+        return loss.value
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if getattr(self, "handle", None):
+                self._lib.tn_mlp_destroy(self.handle)
                 self.handle = None
         except Exception:
             pass

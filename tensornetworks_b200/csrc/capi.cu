@@ -534,8 +534,25 @@ int tn_eigensolve_heff(tn_ctx c, const tn_solver_options* opt, int d, int Dw1, i
     MatvecFn mv = [&](const double* xi, double* yo, const int* skip) {
         return heff_matvec_f64(s, t, nt, F, G, xi, yo, P, Q, skip, cx.stream);
     };
+    const long long N = (long long)d * D1 * D2;
+    if (opt && opt->eigensolver == TN_EIG_DAVIDSON) {
+        // diagonal Davidson (the learned correction needs an MPS site context)
+        const size_t nw = (size_t)Dw1 * Dw2 * d * d;
+        TN_CHECK(cx.misc.ensure(sizeof(double) * (nw + (size_t)N)));
+        double* Wd = cx.misc.as<double>();
+        double* dg = Wd + nw;
+        TN_CUDA_CHECK(cudaMemcpyAsync(Wd, W_host, sizeof(double) * nw, cudaMemcpyHostToDevice, cx.stream));
+        TN_CHECK(heff_diag(s, Wd, F, G, dg, cx.stream));
+        DvResult r{};
+        TN_CHECK(davidson_solve(cx, N, x, std::min(krylov, DV_MAXK), restarts * krylov, tol, mv, dg, nullptr, 0.0,
+                                &r));
+        if (theta) *theta = r.theta;
+        if (residual) *residual = r.resid;
+        if (matvecs) *matvecs = r.matvecs;
+        return r.converged ? TN_OK : TN_NOT_CONVERGED;
+    }
     LzResult r{};
-    TN_CHECK(lanczos_solve(cx, (long long)d * D1 * D2, x, krylov, restarts, tol, mv, &r));
+    TN_CHECK(lanczos_solve(cx, N, x, krylov, restarts, tol, mv, &r));
     TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
     if (theta) *theta = r.theta;
     if (residual) *residual = r.resid;
@@ -706,6 +723,102 @@ int tn_compress(tn_ctx c, int Dmax, double eps, int k, double* s, int* D_out, do
     }
     *D_out = std::max(D, 0);
     if (discarded) *discarded = integ;
+    return TN_OK;
+}
+
+
+struct tn_mlp_s {
+    tnb::MlpModel m;
+};
+struct tn_dataset_s {
+    tnb::DvRecorder r;
+};
+
+int tn_mlp_create(tn_ctx c, uint64_t seed, tn_mlp* out) {
+    if (!c || !out) return TN_BAD_ARG;
+    auto* h = new tn_mlp_s();
+    const int st = tnb::mlp_init(h->m, c->c, seed);
+    if (st != TN_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return TN_OK;
+}
+
+int tn_mlp_destroy(tn_mlp m) {
+    if (!m) return TN_BAD_ARG;
+    delete m;
+    return TN_OK;
+}
+
+int tn_mlp_num_params(void) { return tnb::MLP_NP; }
+
+int tn_mlp_get_params(tn_mlp m, float* host) {
+    if (!m || !host) return TN_BAD_ARG;
+    return tnb::mlp_get_params(m->m, host);
+}
+
+int tn_mlp_set_params(tn_mlp m, const float* host) {
+    if (!m || !host) return TN_BAD_ARG;
+    return tnb::mlp_set_params(m->m, host);
+}
+
+int tn_mlp_forward(tn_mlp m, const float* F, long long n, float* Y) {
+    if (!m || !F || !Y || n < 0) return TN_BAD_ARG;
+    TN_CHECK(tnb::mlp_forward(m->m, F, n, Y, m->m.ctx->stream));
+    TN_CUDA_CHECK(cudaStreamSynchronize(m->m.ctx->stream));
+    return TN_OK;
+}
+
+int tn_mlp_gradient(tn_mlp m, const float* F, const float* T, long long n, float* grad_host, double* loss) {
+    if (!m || !F || !T || !grad_host || n < 1) return TN_BAD_ARG;
+    return tnb::mlp_gradient(m->m, F, T, n, grad_host, loss);
+}
+
+int tn_mlp_train(tn_mlp m, const float* F, const float* T, long long n, int steps, int batch, double lr,
+                 uint64_t seed, double* final_loss) {
+    if (!m || !F || !T || n < 1 || steps < 1 || !(lr > 0)) return TN_BAD_ARG;
+    if (n > 2000000000LL) return TN_BAD_SHAPE;
+    return tnb::mlp_train(m->m, F, T, n, steps, batch, lr, seed, final_loss);
+}
+
+int tn_dataset_create(tn_ctx c, long long capacity, tn_dataset* out) {
+    if (!c || !out || capacity < 1) return TN_BAD_ARG;
+    auto* h = new tn_dataset_s();
+    const int st = tnb::recorder_init(h->r, c->c, capacity);
+    if (st != TN_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return TN_OK;
+}
+
+int tn_dataset_destroy(tn_dataset ds) {
+    if (!ds) return TN_BAD_ARG;
+    delete ds;
+    return TN_OK;
+}
+
+long long tn_dataset_size(tn_dataset ds) { return ds ? ds->r.size : -1; }
+
+int tn_dataset_data(tn_dataset ds, const float** F, const float** T) {
+    if (!ds || !F || !T) return TN_BAD_ARG;
+    *F = ds->r.feats.as<float>();
+    *T = ds->r.targets.as<float>();
+    return TN_OK;
+}
+
+int tn_mps_set_learned_correction(tn_mps psi, tn_mlp m) {
+    if (!psi) return TN_BAD_ARG;
+    psi->m.mlp = m ? &m->m : nullptr;
+    return TN_OK;
+}
+
+int tn_mps_set_recorder(tn_mps psi, tn_dataset ds) {
+    if (!psi) return TN_BAD_ARG;
+    psi->m.recorder = ds ? &ds->r : nullptr;
     return TN_OK;
 }
 

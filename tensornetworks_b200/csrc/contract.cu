@@ -154,6 +154,18 @@ int slab_sum(const double* in, int nslab, long long slab, double* out, const int
     return TN_OK;
 }
 
+__global__ void shift_vector_kernel(double* p, long long n, double v) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] += v;
+}
+
+int shift_vector(double* p, long long n, double v, cudaStream_t st) {
+    if (n <= 0) return TN_OK;
+    shift_vector_kernel<<<grid_for(n), 256, 0, st>>>(p, n, v);
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
 int fill(double* p, long long n, double v, cudaStream_t st) {
     if (n <= 0) return TN_OK;
     fill_kernel<<<grid_for(n), 256, 0, st>>>(p, n, v);

@@ -21,6 +21,8 @@ int wcombine(const double* P, double* Q, const WTermDev* terms, int nterms, long
 int copy2d(int rows, int cols, const double* src, IdxMap sr, IdxMap sc, double* dst, IdxMap dr, IdxMap dc,
            double scale, cudaStream_t st);
 int fill(double* p, long long n, double v, cudaStream_t st);
+// p[i] += v
+int shift_vector(double* p, long long n, double v, cudaStream_t st);
 int slab_sum(const double* in, int nslab, long long slab, double* out, const int* skip, cudaStream_t st);
 int slab_sum_skip(const double* in, int nslab, long long slab, double* out, const int* skip, cudaStream_t st);
 int heff_diag(const ContractShape& s, const double* Wdev, const double* F, const double* G, double* diag,

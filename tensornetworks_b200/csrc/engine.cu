@@ -607,10 +607,92 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     return TN_OK;
 }
 
+// MPSSite::Refine with the device Davidson solver: diagonal correction, or the
+// learned one (opt.use_learned with a model attached), FP64 or split-precision
+// operator; with a recorder attached (FP64, diagonal) every correction step
+// of the solve becomes training pairs.
+int MPSState::refine_site_davidson(int ia, double epsEigen) {
+    const SiteMPO& op = H->ops[ia];
+    ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+    const long long N = (long long)d * D1[ia] * D2[ia];
+    size_t scr = sizeof(double) * contract_scratch_doubles(s);
+    TN_CHECK(ctx->P.ensure(scr));
+    TN_CHECK(ctx->Q.ensure(scr));
+    TN_CHECK(yvec.ensure(sizeof(double) * (size_t)N));
+    TN_CHECK(diagbuf.ensure(sizeof(double) * (size_t)N));
+    const WTermDev* t = H->terms.as<WTermDev>() + op.offLR;
+    const double* F = Lenv[ia - 1]->as<double>();
+    const double* G = Renv[ia + 1]->as<double>();
+    double* P = ctx->P.as<double>();
+    double* Q = ctx->Q.as<double>();
+    cudaStream_t st = ctx->stream;
+    TN_CHECK(heff_diag(s, H->Wdev.as<double>() + op.offW, F, G, diagbuf.as<double>(), st));
+    const bool mixed = opt.precision != TN_PREC_FP64 && mixed_supported(s);
+    const int ns = opt.precision == TN_PREC_MIXED_HI ? 3 : 2;
+    MatvecFn mv;
+    unsigned long long key = hash_val(HASH_SEED, 0x64617669ULL);
+    key = hash_val(key, s);
+    key = hash_val(key, (const void*)t);
+    key = hash_val(key, op.nLR);
+    double tol_rel = 0.0;
+    if (mixed) {
+        const int wF = H->form == TN_FORM_REGULAR_LOWER ? 0 : op.Dw1 - 1;
+        const int wG = H->form == TN_FORM_REGULAR_LOWER ? op.Dw2 - 1 : 0;
+        TN_CHECK(mixed_prepare_site(*ctx, msite, s, t, op.nLR, F, G, wF, wG, ns));
+        // the split operator is Heff - sigma I: shift the diagonal the same way
+        const double sigma = mixed_shift_host(msite, st);
+        TN_CHECK(shift_vector(diagbuf.as<double>(), N, -sigma, st));
+        mv = [&](const double* x, double* y, const int* skip) { return heff_matvec_mixed(*ctx, msite, x, y, skip); };
+        tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-7);
+        key = hash_val(key, ns);
+        for (const DevBuf* b : {&msite.Fs, &msite.Gs, &msite.Xs, &msite.P32, &msite.Qs, &msite.shifts, &msite.err})
+            key = hash_val(key, b->p);
+    } else {
+        mv = [&](const double* x, double* y, const int* skip) {
+            return heff_matvec_f64(s, t, op.nLR, F, G, x, y, P, Q, skip, st);
+        };
+        for (const void* q : {(const void*)F, (const void*)G, (const void*)P, (const void*)Q}) key = hash_val(key, q);
+    }
+    const MlpModel* model = (opt.use_learned && mlp) ? mlp : nullptr;
+    DvRecorder* rec = (!mixed && !model) ? recorder : nullptr;
+    const double pos = L > 1 ? (double)(ia - 1) / (double)(L - 1) : 0.0;
+    const int kmax = opt.krylov > 0 ? std::min(opt.krylov, DV_MAXK) : 16;
+    const int maxit = std::max(8, (opt.max_restarts > 0 ? opt.max_restarts : 10) * kmax);
+    DvResult r{};
+    TN_CHECK(davidson_solve(*ctx, N, A[ia]->as<double>(), kmax, maxit, epsEigen, mv, diagbuf.as<double>(), model, pos,
+                            &r, rec, key, tol_rel));
+    if (mixed) TN_CHECK(mixed_check_error(msite, st));
+    matvecs += r.matvecs;
+    if (!mixed) matvecs_fp64 += r.matvecs;
+    heff_flop += heff_flops(s) * r.matvecs;
+    learned_steps += r.learned_steps;
+    if (r.stalled) ++learned_stalls;
+    double theta = r.theta;
+    if (mixed) {
+        // FP64 Rayleigh quotient of the Ritz vector
+        TN_CHECK(heff_matvec_f64(s, t, op.nLR, F, G, A[ia]->as<double>(), yvec.as<double>(), P, Q, nullptr, st));
+        double resid = 0;
+        TN_CHECK(rayleigh_residual(*ctx, N, A[ia]->as<double>(), yvec.as<double>(), &theta, &resid));
+        matvecs += 1;
+        matvecs_fp64 += 1;
+        heff_flop += heff_flops(s);
+    }
+    if (opt.verbose >= 3)
+        std::printf("site %3d D %3dx%3d davidson%s%s: %d matvecs (%d learned, stalled %d) resid %.2e theta %.12f\n", ia,
+                    D1[ia], D2[ia], mixed ? " mixed" : "", model ? " learned" : "", r.matvecs, r.learned_steps,
+                    r.stalled, r.resid, theta);
+    if (!r.converged) ++not_converged;
+    iterDE[ia] = theta - Emin[ia];
+    Emin[ia] = theta;
+    gapE[ia] = 0.0;  // the Davidson solver tracks the lowest pair only
+    return TN_OK;
+}
+
 // MPSSite::Refine (MPSSite_Variational.C:18-44) with the device eigensolver.
 int MPSState::refine_site(int ia, double epsEigen) {
     const SiteMPO& op = H->ops[ia];
     ContractShape s{d, op.Dw1, op.Dw2, D1[ia], D2[ia]};
+    if (opt.eigensolver == TN_EIG_DAVIDSON) return refine_site_davidson(ia, epsEigen);
     if (opt.precision != TN_PREC_FP64 && mixed_supported(s)) return refine_site_mixed(ia, epsEigen);
     const long long N = (long long)d * D1[ia] * D2[ia];
     size_t scr = sizeof(double) * contract_scratch_doubles(s);
@@ -759,6 +841,7 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
     matvecs = matvecs_fp64 = 0;
     heff_flop = 0;
     not_converged = fallbacks = 0;
+    learned_steps = learned_stalls = 0;
     t_refine = t_gauge = t_env = t_bond = 0;
     n_refine = n_gauge = n_env = 0;
     TN_CUDA_CHECK(cudaEventRecord(ctx->ev_a, st));
@@ -792,7 +875,8 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
         stats->last_dE = dE;
         stats->last_dlambda = dl;
         stats->not_converged = not_converged;
-        stats->fallbacks = fallbacks;
+        stats->fallbacks = fallbacks + (int)learned_stalls;
+        stats->learned_steps = learned_steps;
     }
     return TN_OK;
 }
@@ -813,6 +897,7 @@ int MPSState::find_ground_state(const tn_sched_line* lines, int nlines, const tn
     matvecs = matvecs_fp64 = 0;
     heff_flop = 0;
     not_converged = fallbacks = 0;
+    learned_steps = learned_stalls = 0;
     TN_CHECK(normalize_all(false));
     TN_CHECK(load_heff_caches());
     double E1 = 0, E2 = 0, DE2 = 0, dE = 0, dl = 0;
@@ -869,7 +954,8 @@ int MPSState::find_ground_state(const tn_sched_line* lines, int nlines, const tn
         stats->last_dE = dE;
         stats->last_dlambda = dl;
         stats->not_converged = not_converged;
-        stats->fallbacks = fallbacks;
+        stats->fallbacks = fallbacks + (int)learned_stalls;
+        stats->learned_steps = learned_steps;
     }
     return TN_OK;
 }

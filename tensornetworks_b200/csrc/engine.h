@@ -6,6 +6,8 @@
 #include "contract.h"
 #include "lanczos.h"
 #include "mixed.h"
+#include "davidson.h"
+#include "mlp.h"
 #include "qr.h"
 
 namespace tnb {
@@ -51,11 +53,14 @@ struct MPSState {
     std::vector<int> bondK;                   // current bond dimension (Bond::GetD)
     std::vector<char> bondDirty;              // bond_s lags behind the latest factor
     std::vector<double> Emin, iterDE, gapE;
-    DevBuf tmp, Wqr, Qqr, svdw, envA, envB, yvec;
+    DevBuf tmp, Wqr, Qqr, svdw, envA, envB, yvec, diagbuf;
     MixedSite msite;
     long long matvecs = 0, matvecs_fp64 = 0;
     double heff_flop = 0;
     int not_converged = 0, fallbacks = 0;
+    long long learned_steps = 0, learned_stalls = 0;  // Davidson with the learned correction
+    MlpModel* mlp = nullptr;         // learned Davidson correction (not owned)
+    DvRecorder* recorder = nullptr;  // training-pair recorder (not owned)
     tn_solver_options opt{};
     // phase timing (verbose >= 2): seconds in refine / gauge / environment / bond values
     double t_refine = 0, t_gauge = 0, t_env = 0, t_bond = 0;
@@ -77,6 +82,7 @@ struct MPSState {
     int load_heff_caches();
     int refine_site(int ia, double epsEigen);
     int refine_site_mixed(int ia, double epsEigen);
+    int refine_site_davidson(int ia, double epsEigen);
     int sweep(bool left, double epsEigen);
     int increase_bond_dims(int D);
     int expectation(const std::vector<SiteMPO>& ops, double* E);

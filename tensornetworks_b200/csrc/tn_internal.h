@@ -141,6 +141,7 @@ struct Ctx {
     DevBuf lz;             // Lanczos basis + work vectors
     DevBuf lzstate;        // Lanczos device state
     DevBuf rq;             // Rayleigh-quotient state + partials
+    DevBuf dv, dvstate;    // Davidson basis + work vectors, device state
     DevBuf qrw;            // QR workspace
     DevBuf svdw;           // SVD workspace
     DevBuf wterms;         // MPO term lists
