@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--D", type=int, default=D_FINAL)
     p.add_argument("--cpu-sites", type=int, default=4, help="bulk site updates in the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--matvec-only", action="store_true",
+                   help="only time the bulk D x D Heff application through the operator handle (profiling)")
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -491,6 +493,13 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.matvec_only:
+        import torch
+        import tensornetworks_b200 as T
+        torch.cuda.set_device(local_rank)
+        t, flop = matvec_microbench(T, T.Context(local_rank), torch, args.D, args.precision, reps=max(1, args.steps))
+        print(json.dumps({"matvec_us": round(t * 1e6, 2), "flop": flop, "tflops": round(flop / t / 1e12, 3),
+                          "D": args.D, "precision": args.precision}), flush=True)
     else:
         run_ours(args, rank, world, local_rank)
 
