@@ -259,6 +259,35 @@ int tn_lq(tn_ctx ctx, int m, int n, const double* A, int lda, double* L, int ldl
 int tn_compress(tn_ctx ctx, int Dmax, double eps, int k, double* s, int* D_out,
                 double* discarded);
 
+/* ---- iTEBD gates path -------------------------------------------------------
+ * iTEBDState (TensorNetworks/iTEBDState.H) on an infinite chain with a
+ * two-site unit cell, Vidal form.  FindiTimeGroundState
+ * (iTEBDStateImp_iTime.C:25-104) with second-order Trotter gates
+ * (iTEBDGates::InitGates, iTEBDGates.C:21-54) applied as
+ * iTEBDStateImp::Apply(MultigateType) (iTEBDStateImp_iTime.C:119-135):
+ * contraction, reshape (ReshapeForSVD), Jacobi SVD, SVCompressor truncation
+ * (eps 1e-7 before the last two gates, Dmax after), Unpack. */
+typedef struct tn_itebd_s* tn_itebd;
+/* Gammas uniform(-1,1) from mt19937_64(seed), bond values 1/sqrt(D). */
+int tn_itebd_create(tn_ctx ctx, double S, double Jxy, double Jz, double hz, int D, uint64_t seed,
+                    tn_itebd* out);
+int tn_itebd_destroy(tn_itebd st);
+/* Site s (0 or 1): Gamma (d, Dl, Dr), element (n, i, j) at n*Dl*Dr + j*Dl + i;
+ * bond b joins site b to site 1-b.  Dims of a site follow its two bonds. */
+int tn_itebd_get_site(tn_itebd st, int site, int* Dl, int* Dr, double* host);
+int tn_itebd_set_site(tn_itebd st, int site, int Dl, int Dr, const double* host);
+int tn_itebd_get_bond(tn_itebd st, int bond, int* D, double* host);
+int tn_itebd_set_bond(tn_itebd st, int bond, int D, const double* host);
+/* nsteps second-order Trotter steps at time step dt, truncation to Dmax. */
+int tn_itebd_step(tn_itebd st, double dt, int Dmax, int nsteps);
+/* Schedule of time steps dts[0..ndt): each line runs steps until the bond
+ * values move by at most eps_factor*dt or max_iter steps (steps_out[i]). */
+int tn_itebd_find_ground_state(tn_itebd st, const double* dts, int ndt, int max_iter, int Dmax,
+                               double eps_factor, int* steps_out);
+/* Energy per bond (iTEBDState::GetExpectation): transfer-matrix fixed points by
+ * power iteration (max_iters, tolerance tol on the normalised fixed point). */
+int tn_itebd_energy(tn_itebd st, int max_iters, double tol, double* E);
+
 /* ---- learned Davidson correction (no counterpart in the reference) -------
  * A per-element MLP (4 -> 64 -> 64 -> 1, tanh; BF16 weights for inference,
  * FP32 master copy for training) maps (diag(Heff) - theta)/sigma, r/rms(r),

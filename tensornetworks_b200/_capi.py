@@ -89,6 +89,15 @@ SIGNATURES = {
     "tn_launch_count": (C.c_ulonglong, []),
     "tn_heff_matvec": (_I, [_V, _I, _I, _I, _I, _I, _I, _V, _V, _V, _V, _V]),
     "tn_heff_matvec_static": (_I, [_V, _I, _I, _I, _I, _I, _V, _V, _V, _V, _V]),
+    "tn_itebd_create": (_I, [_V, _D, _D, _D, _D, _I, _ULL, _PV]),
+    "tn_itebd_destroy": (_I, [_V]),
+    "tn_itebd_get_site": (_I, [_V, _I, _PI, _PI, _V]),
+    "tn_itebd_set_site": (_I, [_V, _I, _I, _I, _V]),
+    "tn_itebd_get_bond": (_I, [_V, _I, _PI, _V]),
+    "tn_itebd_set_bond": (_I, [_V, _I, _I, _V]),
+    "tn_itebd_step": (_I, [_V, _D, _I, _I]),
+    "tn_itebd_find_ground_state": (_I, [_V, _V, _I, _I, _I, _D, _V]),
+    "tn_itebd_energy": (_I, [_V, _I, _D, _PD]),
     "tn_mlp_create": (_I, [_V, _ULL, _PV]),
     "tn_mlp_destroy": (_I, [_V]),
     "tn_mlp_num_params": (_I, []),

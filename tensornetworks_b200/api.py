@@ -328,6 +328,76 @@ class MPS:
 
 
 # ---------------------------------------------------------------------------
+# iTEBD (TensorNetworks/iTEBDState.H): infinite chain, two-site unit cell
+# ---------------------------------------------------------------------------
+class iTEBDState:
+    """iTEBDState on the GPU: Gammas and bond values of a two-site unit cell
+    (Vidal form); FindiTimeGroundState with second-order Trotter gates."""
+
+    def __init__(self, S: float, D: int, Jxy: float = 1.0, Jz: float = 1.0, hz: float = 0.0, seed: int = 1234,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self._lib = self.ctx._lib
+        self.d = int(round(2 * S + 1))
+        h = C.c_void_p()
+        check(self._lib.tn_itebd_create(self.ctx.handle, float(S), float(Jxy), float(Jz), float(hz), int(D),
+                                        int(seed), C.byref(h)), "tn_itebd_create")
+        self.handle = h
+
+    def GetSite(self, site: int) -> np.ndarray:
+        """Gamma of site 0 or 1 as (d, Dl, Dr)."""
+        Dl, Dr = C.c_int(), C.c_int()
+        check(self._lib.tn_itebd_get_site(self.handle, site, C.byref(Dl), C.byref(Dr), None), "tn_itebd_get_site")
+        buf = np.empty(self.d * Dl.value * Dr.value)
+        check(self._lib.tn_itebd_get_site(self.handle, site, C.byref(Dl), C.byref(Dr), buf.ctypes.data),
+              "tn_itebd_get_site")
+        return np.transpose(buf.reshape(self.d, Dr.value, Dl.value), (0, 2, 1)).copy()
+
+    def SetSite(self, site: int, G: np.ndarray):
+        d, Dl, Dr = G.shape
+        buf = np.ascontiguousarray(np.transpose(G, (0, 2, 1)), dtype=np.float64).ravel()
+        check(self._lib.tn_itebd_set_site(self.handle, site, Dl, Dr, buf.ctypes.data), "tn_itebd_set_site")
+
+    def GetBond(self, bond: int) -> np.ndarray:
+        D = C.c_int()
+        check(self._lib.tn_itebd_get_bond(self.handle, bond, C.byref(D), None), "tn_itebd_get_bond")
+        out = np.empty(D.value)
+        check(self._lib.tn_itebd_get_bond(self.handle, bond, C.byref(D), out.ctypes.data), "tn_itebd_get_bond")
+        return out
+
+    def SetBond(self, bond: int, s: np.ndarray):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        check(self._lib.tn_itebd_set_bond(self.handle, bond, s.size, s.ctypes.data), "tn_itebd_set_bond")
+
+    def Step(self, dt: float, Dmax: int, nsteps: int = 1):
+        check(self._lib.tn_itebd_step(self.handle, float(dt), int(Dmax), int(nsteps)), "tn_itebd_step")
+
+    def FindiTimeGroundState(self, dts, max_iter: int, Dmax: int, eps_factor: float = 5e-5) -> List[int]:
+        """One schedule line per dt (IterationScheduleLine itsdt): steps until the
+        bond values move by at most eps_factor*dt, or max_iter steps."""
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        steps = np.zeros(dts.size, dtype=np.int32)
+        check(self._lib.tn_itebd_find_ground_state(self.handle, dts.ctypes.data, dts.size, int(max_iter), int(Dmax),
+                                                   float(eps_factor), steps.ctypes.data),
+              "tn_itebd_find_ground_state")
+        return steps.tolist()
+
+    def GetExpectation(self, max_iters: int = 20000, tol: float = 1e-13) -> float:
+        """Energy per bond of the infinite chain."""
+        E = C.c_double()
+        check(self._lib.tn_itebd_energy(self.handle, int(max_iters), float(tol), C.byref(E)), "tn_itebd_energy")
+        return E.value
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if getattr(self, "handle", None):
+                self._lib.tn_itebd_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
 # Learned Davidson correction (no reference counterpart)
 # ---------------------------------------------------------------------------
 class _DevArray:

@@ -8,6 +8,7 @@
 
 #include "engine.h"
 #include "mixed.h"
+#include "itebd.h"
 
 namespace tnb {
 
@@ -820,6 +821,112 @@ int tn_mps_set_recorder(tn_mps psi, tn_dataset ds) {
     if (!psi) return TN_BAD_ARG;
     psi->m.recorder = ds ? &ds->r : nullptr;
     return TN_OK;
+}
+
+
+struct tn_itebd_s {
+    tnb::ITebdState s;
+};
+
+int tn_itebd_create(tn_ctx c, double S, double Jxy, double Jz, double hz, int D, uint64_t seed, tn_itebd* out) {
+    if (!c || !out || D < 1 || S <= 0) return TN_BAD_ARG;
+    auto* h = new tn_itebd_s();
+    const int st = h->s.init(c->c, S, Jxy, Jz, hz, D, seed);
+    if (st != TN_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return TN_OK;
+}
+
+int tn_itebd_destroy(tn_itebd st) {
+    if (!st) return TN_BAD_ARG;
+    delete st;
+    return TN_OK;
+}
+
+int tn_itebd_get_site(tn_itebd st, int site, int* Dl, int* Dr, double* host) {
+    if (!st || site < 0 || site > 1) return TN_BAD_ARG;
+    auto& s = st->s;
+    const int l = s.dim(1 - site), r = s.dim(site);
+    if (Dl) *Dl = l;
+    if (Dr) *Dr = r;
+    if (host) {
+        TN_CUDA_CHECK(cudaStreamSynchronize(s.ctx->stream));
+        TN_CUDA_CHECK(cudaMemcpy(host, s.G[site].p, sizeof(double) * (size_t)s.d * l * r, cudaMemcpyDeviceToHost));
+    }
+    return TN_OK;
+}
+
+int tn_itebd_set_site(tn_itebd st, int site, int Dl, int Dr, const double* host) {
+    if (!st || site < 0 || site > 1 || !host) return TN_BAD_ARG;
+    auto& s = st->s;
+    if (Dl != s.dim(1 - site) || Dr != s.dim(site)) {
+        tnb::set_error("tn_itebd_set_site: site %d is %d x %d (set the bond values first)", site, s.dim(1 - site),
+                       s.dim(site));
+        return TN_BAD_SHAPE;
+    }
+    TN_CHECK(s.G[site].ensure(sizeof(double) * (size_t)s.d * Dl * Dr));
+    TN_CUDA_CHECK(cudaStreamSynchronize(s.ctx->stream));
+    TN_CUDA_CHECK(cudaMemcpy(s.G[site].p, host, sizeof(double) * (size_t)s.d * Dl * Dr, cudaMemcpyHostToDevice));
+    return TN_OK;
+}
+
+int tn_itebd_get_bond(tn_itebd st, int bond, int* D, double* host) {
+    if (!st || bond < 0 || bond > 1) return TN_BAD_ARG;
+    const auto& v = st->s.lam_h[bond];
+    if (D) *D = (int)v.size();
+    if (host) std::memcpy(host, v.data(), sizeof(double) * v.size());
+    return TN_OK;
+}
+
+int tn_itebd_set_bond(tn_itebd st, int bond, int D, const double* host) {
+    if (!st || bond < 0 || bond > 1 || D < 1 || !host) return TN_BAD_ARG;
+    auto& s = st->s;
+    s.lam_h[bond].assign(host, host + D);
+    TN_CHECK(s.lam[bond].ensure(sizeof(double) * D));
+    TN_CUDA_CHECK(cudaStreamSynchronize(s.ctx->stream));
+    TN_CUDA_CHECK(cudaMemcpy(s.lam[bond].p, host, sizeof(double) * D, cudaMemcpyHostToDevice));
+    return TN_OK;
+}
+
+int tn_itebd_step(tn_itebd st, double dt, int Dmax, int nsteps) {
+    if (!st || Dmax < 1 || nsteps < 0) return TN_BAD_ARG;
+    for (int k = 0; k < nsteps; ++k) TN_CHECK(st->s.step2(dt, Dmax));
+    return TN_OK;
+}
+
+int tn_itebd_find_ground_state(tn_itebd st, const double* dts, int ndt, int max_iter, int Dmax, double eps_factor,
+                               int* steps_out) {
+    if (!st || !dts || ndt < 1 || max_iter < 1 || Dmax < 1) return TN_BAD_ARG;
+    auto& s = st->s;
+    for (int l = 0; l < ndt; ++l) {
+        const double dt = dts[l];
+        int n = 0;
+        for (n = 1; n <= max_iter; ++n) {
+            const std::vector<double> old0 = s.lam_h[0], old1 = s.lam_h[1];
+            TN_CHECK(s.step2(dt, Dmax));
+            double dl = 0;
+            for (int b = 0; b < 2; ++b) {
+                const auto& o = b == 0 ? old0 : old1;
+                const auto& x = s.lam_h[b];
+                if (o.size() != x.size()) {
+                    dl = 1.0;
+                    continue;
+                }
+                for (size_t i = 0; i < x.size(); ++i) dl = std::max(dl, std::fabs(o[i] - x[i]));
+            }
+            if (dl <= eps_factor * dt) break;
+        }
+        if (steps_out) steps_out[l] = std::min(n, max_iter);
+    }
+    return TN_OK;
+}
+
+int tn_itebd_energy(tn_itebd st, int max_iters, double tol, double* E) {
+    if (!st || !E || max_iters < 1) return TN_BAD_ARG;
+    return st->s.energy(E, max_iters, tol);
 }
 
 }  // extern "C"

@@ -1,7 +1,8 @@
 // davidson.cu -- device Davidson for the lowest eigenpair of Heff, with the
-// diagonal correction t = r / (theta - diag) or the learned per-element MLP
-// correction.  No reference counterpart (the reference diagonalises the dense
-// Heff with zheevx, MPSSite_Variational.C:18-33); it is the "Davidson
+// diagonal correction t = r / (theta - diag), optionally plus a learned
+// per-element MLP estimate of its error.  No reference counterpart (the
+// reference diagonalises the dense Heff with zheevx,
+// MPSSite_Variational.C:18-33); it is the "Davidson
 // correction equation" solver of the learned preconditioner, and plain
 // diagonal Davidson is its fallback whenever the learned correction stalls.
 //
@@ -447,12 +448,21 @@ __global__ void dv_restart_kernel(double* __restrict__ V, double* __restrict__ W
     }
 }
 
-// Correction t from the residual: diagonal r / (theta - diag) or the MLP.
+// Diagonal correction r / (theta - diag), the denominator kept away from zero.
+__device__ __forceinline__ double diag_correction(double ri, double di, double th, double eps) {
+    double den = th - di;
+    if (fabs(den) < eps) den = den < 0 ? -eps : eps;
+    return ri / den;
+}
+
+// Correction t from the residual: the diagonal one, plus (learned) the MLP's
+// estimate of its error, in units of rms(r) / sigma.
 __global__ void dv_correct_kernel(const double* __restrict__ r, const double* __restrict__ diag,
                                   const double* __restrict__ u, double* __restrict__ t, long long N,
                                   const __nv_bfloat16* __restrict__ w16, DvState* st) {
     if (st->done) return;
     const double th = st->theta;
+    const double eps = 1e-8 * fmax(1.0, fabs(th));
     const bool use_mlp = (w16 != nullptr) && st->learned && !st->stalled;
     if (use_mlp) {
         __shared__ float w[MLP_NP];
@@ -470,23 +480,20 @@ __global__ void dv_correct_kernel(const double* __restrict__ r, const double* __
             f[1] = mlp_clip((float)r[i] * rinv, MLP_FEAT_CLIP);
             f[2] = mlp_clip((float)u[i] * sqn, MLP_FEAT_CLIP);
             f[3] = pos;
-            t[i] = (double)mlp_eval(w, f) * back;
+            t[i] = diag_correction(r[i], diag[i], th, eps) + (double)mlp_eval(w, f) * back;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) st->learned_steps += 1;
         return;
     }
-    const double eps = 1e-8 * fmax(1.0, fabs(th));
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
-        double den = th - diag[i];
-        if (fabs(den) < eps) den = den < 0 ? -eps : eps;
-        t[i] = r[i] / den;
-    }
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+        t[i] = diag_correction(r[i], diag[i], th, eps);
 }
 
-// Training record of this step: features of every element and the Ritz
-// vector (targets follow once the eigenvector is known).
+// Training record of this step: features of every element, the Ritz vector,
+// and (in the target slot) the normalised diagonal correction; the targets
+// are completed once the eigenvector is known.
 __global__ void dv_record_kernel(const double* __restrict__ r, const double* __restrict__ diag,
-                                 const double* __restrict__ u, long long N, DvState* st, float* feats,
+                                 const double* __restrict__ u, long long N, DvState* st, float* feats, float* targets,
                                  long long base, long long capacity, double* ubuf, double* scales, int max_steps) {
     if (st->done) return;
     const int step = st->iters - 1;  // the step whose residual was just formed
@@ -496,7 +503,10 @@ __global__ void dv_record_kernel(const double* __restrict__ r, const double* __r
     const double th = st->theta, rs = st->rms_r, sg = st->sigma;
     const float sqn = (float)sqrt((double)N);
     const float rinv = rs > 0 ? (float)(1.0 / rs) : 0.f, sinv = (float)(1.0 / sg);
+    const double eps = 1e-8 * fmax(1.0, fabs(th));
+    const double norm = rs > 0 ? sg / rs : 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        targets[off + i] = mlp_clip((float)(diag_correction(r[i], diag[i], th, eps) * norm), 1e30f);
         float* f = feats + (off + i) * MLP_IN;
         f[0] = mlp_clip((float)(diag[i] - th) * sinv, MLP_FEAT_CLIP);
         f[1] = mlp_clip((float)r[i] * rinv, MLP_FEAT_CLIP);
@@ -535,7 +545,9 @@ __global__ void dv_dot_kernel(const double* __restrict__ a, const double* __rest
     }
 }
 
-// Targets of one recorded step: t* = x / (u.x) - u, scaled by sigma / rms_r.
+// Targets of one recorded step: the error of the diagonal correction against
+// the exact one t* = x / (u.x) - u, both scaled by sigma / rms_r (the slot
+// holds the scaled diagonal correction on entry).
 __global__ void dv_target_kernel(const double* __restrict__ x, const double* __restrict__ ub, long long N,
                                  const double* __restrict__ ux, const double* __restrict__ scales, float* targets) {
     const double dot = *ux;
@@ -543,7 +555,7 @@ __global__ void dv_target_kernel(const double* __restrict__ x, const double* __r
     const double sc = scales[0] > 0 ? scales[1] / scales[0] : 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         const double ts = x[i] * inv - ub[i];
-        targets[i] = mlp_clip((float)(ts * sc), MLP_TARGET_CLIP);
+        targets[i] = mlp_clip((float)(ts * sc - (double)targets[i]), MLP_TARGET_CLIP);
     }
 }
 
@@ -620,7 +632,8 @@ int davidson_solve(Ctx& c, long long N, double* x, int kmax, int max_iters, doub
         dv_resid_kernel<<<grid, DV_THREADS, 0, st>>>(V, W, diag, N, r, u, wu, partial, s, cond);
         TN_LAUNCH_CHECK();
         if (recording) {
-            dv_record_kernel<<<grid, DV_THREADS, 0, st>>>(r, diag, u, N, s, rec->feats.as<float>(), rec->size,
+            dv_record_kernel<<<grid, DV_THREADS, 0, st>>>(r, diag, u, N, s, rec->feats.as<float>(),
+                                                          rec->targets.as<float>(), rec->size,
                                                           rec->capacity, rec->ubuf.as<double>(),
                                                           rec->scales.as<double>(), max_iters);
             TN_LAUNCH_CHECK();

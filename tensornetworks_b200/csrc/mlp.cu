@@ -1,10 +1,11 @@
 // mlp.cu -- hand-written inference, gradient and Adam kernels of the learned
 // Davidson correction (no reference counterpart).  The network maps the
 // features of one element (f0 = (diag - theta)/sigma, f1 = r/rms(r),
-// f2 = u sqrt(N), f3 = bond position) to the normalised correction
-// y = t sigma / rms(r); it is trained by mean squared error on pairs the plain
-// FP64 Davidson solver records in its own sweeps (target: the exact
-// correction x/(u.x) - u towards the converged eigenvector x).
+// f2 = u sqrt(N), f3 = bond position) to the error of the diagonal correction
+// in units of rms(r)/sigma; it is trained by mean squared error on pairs the
+// plain FP64 Davidson solver records in its own sweeps (target: the exact
+// correction x/(u.x) - u towards the converged eigenvector x, minus the
+// diagonal correction r/(theta - diag)).
 //
 // Inference reads BF16 weights (FP32 in shared memory, FP32 accumulation);
 // training keeps an FP32 master copy: per block, every thread runs forward

@@ -1,0 +1,68 @@
+"""iTEBD gates path on the device against the CPU oracle (same initial
+Gammas and bond values, same gate sequence) and against the reference's
+bounds (TensorNetworksUnittests/iTEBDTests.C:737-759).
+
+Tolerances: bond values after a few Trotter steps 1e-10 (FP64 throughout;
+the SVD and the contraction order differ); energies 1e-9."""
+import numpy as np
+import pytest
+
+from oracle import itebd_oracle as I
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+EXACT = 0.25 - np.log(2.0)
+
+
+@pytest.fixture(scope="module")
+def T():
+    import tensornetworks_b200 as T
+    return T
+
+
+def load(T, st_or, D):
+    s = T.iTEBDState(st_or.S, D, seed=1)
+    for b in range(2):
+        s.SetBond(b, st_or.l[b])
+    for site in range(2):
+        s.SetSite(site, st_or.G[site])
+    return s
+
+
+@pytest.mark.parametrize("S,D,dt,nsteps", [(0.5, 4, 0.1, 3), (0.5, 8, 0.05, 5), (1.0, 6, 0.1, 3)])
+def test_trotter_steps_match_oracle(T, S, D, dt, nsteps):
+    ref = I.State(S, D, seed=7)
+    dev = load(T, ref, D)
+    gates = [I.gate(S, 1, 1, 0, dt / 2), I.gate(S, 1, 1, 0, dt), I.gate(S, 1, 1, 0, dt / 2)]
+    for _ in range(nsteps):
+        ref.step(gates, D)
+        dev.Step(dt, D, 1)
+        for b in range(2):
+            lb = dev.GetBond(b)
+            assert lb.size == ref.l[b].size
+            np.testing.assert_allclose(lb, ref.l[b], atol=1e-10)
+    h = O.local_h12(S, 1, 1, 0)
+    e_ref = I.expectation(ref, h)
+    assert abs(dev.GetExpectation() - e_ref) < 1e-9
+    # Gammas agree up to the sign of each singular vector
+    for site in range(2):
+        g, gr = dev.GetSite(site), ref.G[site]
+        assert g.shape == gr.shape
+        np.testing.assert_allclose(np.abs(g), np.abs(gr), rtol=1e-7, atol=1e-8)
+
+
+def test_ground_state_d8_within_reference_bounds(T):
+    st = T.iTEBDState(0.5, 8, seed=11)
+    steps = st.FindiTimeGroundState([0.5, 0.2, 0.1, 0.01, 0.001], 1000, 8)
+    E = st.GetExpectation()
+    print("iTEBD D=8", E, steps)
+    assert EXACT < E < -0.442846
+    assert st.GetBond(0).size == 8 and st.GetBond(1).size == 8
+
+
+def test_ground_state_d32_improves(T):
+    st = T.iTEBDState(0.5, 32, seed=12)
+    st.FindiTimeGroundState([0.5, 0.2, 0.1, 0.01], 300, 32)
+    E = st.GetExpectation()
+    print("iTEBD D=32", E)
+    assert EXACT < E < -0.4430
