@@ -367,8 +367,11 @@ def run_ours(args, rank, world, local_rank):
         peak = peaks["bf16_tflops"] / nprod
         peak_src = f"{peak_kind} bf16 burst / {nprod} (BF16 split products per FP32-accurate flop)"
     achieved = F_mv / t_mv / 1e12
+    # DRAM bytes per application from the ncu capture of the same command
+    # (profiles/heff_matvec_D256.md); measured at D = 256 only
+    traffic = {("mixed", 256): 11.6e6, ("fp64", 256): 21.1e6}.get((args.precision, args.D))
     roofline = {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "kernel": "heff_matvec (3-stage chain)",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": "heff_matvec (3-stage chain)",
                 "per_launch_us": round(t_mv * 1e6, 2), "flop_per_launch": F_mv, "peak_source": peak_src}
 
     out = None
