@@ -67,6 +67,16 @@ def parse():
     return p.parse_args()
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest replica's time: every rank contributes its own device time."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def unit_of(args):
     return f"s per sweep pair (L={args.L}, D={args.D})"
 
@@ -301,11 +311,7 @@ def run_ours(args, rank, world, local_rank):
         launches = lib.tn_launch_count() - launches0
         if clocks:
             clocks.stop()
-        t_step = sum(step_ms) / len(step_ms) / 1e3
-        if dist:
-            tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_step = float(tt.item())
+        t_step = max_over_ranks(sum(step_ms) / len(step_ms) / 1e3, dist, "cuda")
         E_step = psi.GetExpectation(H)
         # finish the schedule (the D line to convergence) from the grown snapshot
         for i, a in enumerate(grown, start=1):
