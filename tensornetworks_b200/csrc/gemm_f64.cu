@@ -4,8 +4,9 @@
 // effective-Hamiltonian matvec and of the environment updates
 // (MPSSite::GetHeff / IterateLeft_F / IterateRightF in the reference,
 // MPSSite_Contractions.C:155-400), and for small gauge products.
-// Tile 64x64x16, 256 threads, 4x4 outputs per thread, register-staged
-// double buffering of the next k-tile.
+// Plain strided operands take the FP64 tensor-core (DMMA) kernel below;
+// split-index operands the SIMT kernel: tile 64x64x16, 256 threads, 4x4
+// outputs per thread, register-staged double buffering of the next k-tile.
 #include "tn_internal.h"
 
 namespace tnb {
@@ -107,6 +108,115 @@ __global__ void __launch_bounds__(NT) gemm_f64_kernel(GemmArgs g) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core path: mma.sync m8n8k4 (DMMA), for operands whose index maps
+// are plain strides over the ranges used (no split indices).  CTA tile 64x64,
+// 4 warps each owning a 32x32 quarter (4x4 MMA tiles, 32 accumulators per
+// thread), k-tiles of 16 staged in shared memory with the next tile
+// prefetched into registers.  The shared row stride 68 (= 4 mod 16 doubles)
+// makes the fragment loads of a half-warp hit 16 distinct bank pairs.
+constexpr int TBM = 64, TBN = 64, TBK = 16, TNT = 128, TLD = TBM + 4;
+
+struct LinGemm {
+    int M, N, K, nb1;
+    long long sAm, sAk, sBk, sBn, sCm, sCn;
+    long long sA0, sA1, sB0, sB1, sC0, sC1;
+    const double *A, *B;
+    double* C;
+    double alpha, beta;
+    const int* skip;
+};
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+template <bool A_MCONTIG, bool B_KCONTIG>
+__global__ void __launch_bounds__(TNT) gemm_f64_dmma_kernel(LinGemm g) {
+    if (g.skip && *g.skip) return;
+    __shared__ double As[TBK][TLD];
+    __shared__ double Bs[TBK][TLD];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
+    const int b = blockIdx.z;
+    const int b0 = b / g.nb1, b1 = b - b0 * g.nb1;
+    const double* Ab = g.A + b0 * g.sA0 + b1 * g.sA1;
+    const double* Bb = g.B + b0 * g.sB0 + b1 * g.sB1;
+    // tile slots: 8 per thread for A (TBK x TBM) and 8 for B (TBK x TBN)
+    double ra[8], rb[8];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int e = t + TNT * r;
+            int am, ak, bk, bn;
+            if (A_MCONTIG) { am = e % TBM; ak = e / TBM; } else { ak = e % TBK; am = e / TBK; }
+            if (B_KCONTIG) { bk = e % TBK; bn = e / TBK; } else { bn = e % TBN; bk = e / TBN; }
+            const int gm = m0 + am, gk = k0 + ak, hk = k0 + bk, gn = n0 + bn;
+            ra[r] = (gm < g.M && gk < g.K) ? __ldg(Ab + gm * g.sAm + gk * g.sAk) : 0.0;
+            rb[r] = (gn < g.N && hk < g.K) ? __ldg(Bb + hk * g.sBk + gn * g.sBn) : 0.0;
+        }
+    };
+    auto store = [&]() {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int e = t + TNT * r;
+            int am, ak, bk, bn;
+            if (A_MCONTIG) { am = e % TBM; ak = e / TBM; } else { ak = e % TBK; am = e / TBK; }
+            if (B_KCONTIG) { bk = e % TBK; bn = e / TBK; } else { bn = e % TBN; bk = e / TBN; }
+            As[ak][am] = ra[r];
+            Bs[bk][bn] = rb[r];
+        }
+    };
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    load(0);
+    for (int k0 = 0; k0 < g.K; k0 += TBK) {
+        store();
+        __syncthreads();
+        if (k0 + TBK < g.K) load(k0 + TBK);
+#pragma unroll
+        for (int ks = 0; ks < TBK; ks += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = As[ks + tig][wm + i * 8 + gid];  // A(row gid, col tig)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bf[j] = Bs[ks + tig][wn + j * 8 + gid];  // B(row tig, col gid)
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j], af[i], bf[j]);
+        }
+        __syncthreads();
+    }
+    double* Cb = g.C + b0 * g.sC0 + b1 * g.sC1;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + wm + i * 8 + gid;
+        if (gm >= g.M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int gn = n0 + wn + j * 8 + tig * 2 + q;
+                if (gn >= g.N) continue;
+                double* c = Cb + gm * g.sCm + gn * g.sCn;
+                double v = g.alpha * acc[i][j][q];
+                if (g.beta != 0.0) v += g.beta * *c;
+                *c = v;
+            }
+    }
+}
+
+// An index map that is a plain stride over [0, n).
+inline bool plain(const IdxMap& m, int n) { return m.div >= n; }
+
 }  // namespace
 
 int gemm_f64(const GemmArgs& g, cudaStream_t st) {
@@ -124,6 +234,21 @@ int gemm_f64(const GemmArgs& g, cudaStream_t st) {
     }
     bool amc = (g.A.mn.s == 1);
     bool bkc = (g.B.k.s == 1);
+    if (plain(g.A.mn, g.M) && plain(g.A.k, g.K) && plain(g.B.k, g.K) && plain(g.B.mn, g.N) && plain(g.C.m, g.M) &&
+        plain(g.C.n, g.N)) {
+        LinGemm l;
+        l.M = g.M; l.N = g.N; l.K = g.K; l.nb1 = g.nb1;
+        l.sAm = g.A.mn.s; l.sAk = g.A.k.s; l.sBk = g.B.k.s; l.sBn = g.B.mn.s; l.sCm = g.C.m.s; l.sCn = g.C.n.s;
+        l.sA0 = g.A.sb0; l.sA1 = g.A.sb1; l.sB0 = g.B.sb0; l.sB1 = g.B.sb1; l.sC0 = g.C.sb0; l.sC1 = g.C.sb1;
+        l.A = g.A.ptr; l.B = g.B.ptr; l.C = g.C.ptr; l.alpha = g.alpha; l.beta = g.beta; l.skip = g.skip;
+        dim3 tg((g.N + TBN - 1) / TBN, (g.M + TBM - 1) / TBM, g.nb0 * g.nb1);
+        if (amc && bkc) gemm_f64_dmma_kernel<true, true><<<tg, TNT, 0, st>>>(l);
+        else if (amc && !bkc) gemm_f64_dmma_kernel<true, false><<<tg, TNT, 0, st>>>(l);
+        else if (!amc && bkc) gemm_f64_dmma_kernel<false, true><<<tg, TNT, 0, st>>>(l);
+        else gemm_f64_dmma_kernel<false, false><<<tg, TNT, 0, st>>>(l);
+        TN_LAUNCH_CHECK();
+        return TN_OK;
+    }
     if (amc && bkc) gemm_f64_kernel<true, true><<<grid, NT, 0, st>>>(g);
     else if (amc && !bkc) gemm_f64_kernel<true, false><<<grid, NT, 0, st>>>(g);
     else if (!amc && bkc) gemm_f64_kernel<false, true><<<grid, NT, 0, st>>>(g);
