@@ -153,6 +153,8 @@ int tn_ctx_create(int device, tn_ctx* out) {
     if (const char* ng = std::getenv("TN_NO_GRAPHS")) c->c.use_graphs = !(ng[0] == '1');
     TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.own_stream, cudaStreamNonBlocking));
     c->c.stream = c->c.own_stream;
+    TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.aux, cudaStreamNonBlocking));
+    for (auto& e : c->c.ev_x) TN_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     TN_CUDA_CHECK(cudaEventCreate(&c->c.ev_a));
     TN_CUDA_CHECK(cudaEventCreate(&c->c.ev_b));
     *out = c;
@@ -164,6 +166,10 @@ int tn_ctx_destroy(tn_ctx c) {
     cudaSetDevice(c->c.device);
     cudaStreamSynchronize(c->c.stream);
     c->c.clear_graphs();
+    if (c->c.aux) cudaStreamSynchronize(c->c.aux);
+    for (auto& e : c->c.ev_x)
+        if (e) cudaEventDestroy(e);
+    if (c->c.aux) cudaStreamDestroy(c->c.aux);
     if (c->c.ev_a) cudaEventDestroy(c->c.ev_a);
     if (c->c.ev_b) cudaEventDestroy(c->c.ev_b);
     if (c->c.own_stream) cudaStreamDestroy(c->c.own_stream);

@@ -453,9 +453,24 @@ __global__ void extract_r_kernel(const double* W, int ldw, int k, int n, double*
     }
 }
 
+__global__ void copy_cols_kernel(const double* __restrict__ src, int lds, double* __restrict__ dst, int ldd, int m,
+                                 int k) {
+    const long long total = (long long)m * k;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % m), j = (int)(e / m);
+        dst[(size_t)j * ldd + i] = src[(size_t)j * lds + i];
+    }
+}
+
 inline int g1d(long long n) {
     long long b = (n + 255) / 256;
     return (int)std::max<long long>(1, std::min<long long>(b, 148 * 8));
+}
+
+int copy2d_f64(int m, int k, const double* src, int lds, double* dst, int ldd, cudaStream_t st) {
+    copy_cols_kernel<<<g1d((long long)m * k), 256, 0, st>>>(src, lds, dst, ldd, m, k);
+    TN_LAUNCH_CHECK();
+    return TN_OK;
 }
 
 int panel_width(int m) {
@@ -469,6 +484,94 @@ int panel_width(int m) {
 }  // namespace
 
 namespace {
+
+// Several panels: look-ahead on two streams.  The main stream runs panel k,
+// then applies its block reflector to panel k+1's columns only ("narrow"),
+// then panel k+1; the side stream applies it to the columns beyond
+// ("wide") and accumulates Q forward, Q <- Q (I - V_k T_k V_k^T) on the full
+// m x m Q (three FP64 GEMMs), while the main stream factors later panels.
+// The narrow update of panel k+1 waits for the wide update of panel k, which
+// brought panel k+2's columns up to date.  Q's first k columns and R are read
+// out once the side stream has finished.
+template <int NT, int R, int B, int U>
+int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr, double* Vall,
+                 double* Tall) {
+    cudaStream_t s0 = c.stream, s1 = c.aux;
+    cudaEvent_t ev_p = c.ev_x[0], ev_w = c.ev_x[1], ev_q = c.ev_x[2];
+    const int k = std::min(m, n);
+    double *Qf = nullptr, *Z = nullptr, *Z2 = nullptr;
+    if (Qout) {
+        TN_CHECK(c.qaccum.ensure(sizeof(double) * ((size_t)m * m + 2 * (size_t)m * B)));
+        Qf = c.qaccum.as<double>();
+        Z = Qf + (size_t)m * m;
+        Z2 = Z + (size_t)m * B;
+    }
+    // the side stream starts after everything already queued on the main stream
+    TN_CUDA_CHECK(cudaEventRecord(ev_p, s0));
+    TN_CUDA_CHECK(cudaStreamWaitEvent(s1, ev_p, 0));
+    if (Qout) {
+        set_identity_kernel<<<g1d((long long)m * m), 256, 0, s1>>>(Qf, m, m, m);
+        TN_LAUNCH_CHECK();
+    }
+    bool have_wide = false;
+    for (int j0 = 0; j0 < k; j0 += B) {
+        const int b = std::min(B, k - j0);
+        const int mp = m - j0;
+        double* Vp = Vall + (size_t)j0 * m + j0;  // ld m
+        double* Tp = Tall + (size_t)j0 * B;        // ld B
+        qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, s0>>>(W, m, m, j0, b, Vp, m, Tp, B);
+        TN_LAUNCH_CHECK();
+        TN_CUDA_CHECK(cudaEventRecord(ev_p, s0));
+        // narrow: the next panel's columns (after the previous wide update reached them)
+        const int c1 = j0 + b;
+        const int nb_next = std::max(0, std::min(B, k - c1));
+        if (nb_next > 0) {
+            if (have_wide) TN_CUDA_CHECK(cudaStreamWaitEvent(s0, ev_w, 0));
+            wy_apply_kernel<B, true><<<(nb_next + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(mp, B), s0>>>(
+                Vp, m, Tp, B, b, W + (size_t)c1 * m + j0, m, mp, nb_next);
+            TN_LAUNCH_CHECK();
+        }
+        // wide: every column beyond the next panel, on the side stream
+        TN_CUDA_CHECK(cudaStreamWaitEvent(s1, ev_p, 0));
+        const int c2 = c1 + nb_next;
+        if (n - c2 > 0) {
+            wy_apply_kernel<B, true><<<(n - c2 + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(mp, B), s1>>>(
+                Vp, m, Tp, B, b, W + (size_t)c2 * m + j0, m, mp, n - c2);
+            TN_LAUNCH_CHECK();
+        }
+        TN_CUDA_CHECK(cudaEventRecord(ev_w, s1));
+        have_wide = true;
+        if (Qout) {
+            // Q[:, j0:] <- Q[:, j0:] - (Q[:, j0:] V) T V^T
+            GemmArgs g;
+            g.M = m; g.N = b; g.K = mp;
+            g.A.ptr = Qf + (size_t)j0 * m; g.A.mn = idx(1); g.A.k = idx(m);
+            g.B.ptr = Vp; g.B.k = idx(1); g.B.mn = idx(m);
+            g.C.ptr = Z; g.C.m = idx(1); g.C.n = idx(m);
+            TN_CHECK(gemm_f64(g, s1));
+            GemmArgs h;
+            h.M = m; h.N = b; h.K = b;
+            h.A.ptr = Z; h.A.mn = idx(1); h.A.k = idx(m);
+            h.B.ptr = Tp; h.B.k = idx(1); h.B.mn = idx(B);
+            h.C.ptr = Z2; h.C.m = idx(1); h.C.n = idx(m);
+            TN_CHECK(gemm_f64(h, s1));
+            GemmArgs u;
+            u.M = m; u.N = mp; u.K = b; u.alpha = -1.0; u.beta = 1.0;
+            u.A.ptr = Z2; u.A.mn = idx(1); u.A.k = idx(m);
+            u.B.ptr = Vp; u.B.k = idx(m); u.B.mn = idx(1);
+            u.C.ptr = Qf + (size_t)j0 * m; u.C.m = idx(1); u.C.n = idx(m);
+            TN_CHECK(gemm_f64(u, s1));
+        }
+    }
+    TN_CUDA_CHECK(cudaEventRecord(ev_q, s1));
+    TN_CUDA_CHECK(cudaStreamWaitEvent(s0, ev_q, 0));
+    if (Rout) {
+        extract_r_kernel<<<g1d((long long)k * n), 256, 0, s0>>>(W, m, k, n, Rout, ldr);
+        TN_LAUNCH_CHECK();
+    }
+    if (Qout) TN_CHECK(copy2d_f64(m, k, Qf, m, Qout, ldq, s0));
+    return TN_OK;
+}
 
 template <int NT, int R, int B, int U>
 int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
@@ -487,6 +590,7 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
     TN_CHECK(c.qrw.ensure(need));
     double* Vall = c.qrw.as<double>();
     double* Tall = Vall + (size_t)m * k;
+    if (k > B && c.aux) return qr_lookahead<NT, R, B, U>(c, m, n, W, Qout, ldq, Rout, ldr, Vall, Tall);
     for (int j0 = 0; j0 < k; j0 += B) {
         const int b = std::min(B, k - j0);
         const int mp = m - j0;

@@ -136,6 +136,9 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    // side stream for work that overlaps the main stream's critical path (QR look-ahead)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_x[3] = {nullptr, nullptr, nullptr};
     // scratch
     DevBuf P, Q;           // contraction intermediates
     DevBuf lz;             // Lanczos basis + work vectors
@@ -143,6 +146,7 @@ struct Ctx {
     DevBuf rq;             // Rayleigh-quotient state + partials
     DevBuf dv, dvstate;    // Davidson basis + work vectors, device state
     DevBuf qrw;            // QR workspace
+    DevBuf qaccum;         // QR: forward-accumulated Q and its two m x b temporaries
     DevBuf svdw;           // SVD workspace
     DevBuf wterms;         // MPO term lists
     DevBuf misc;
