@@ -334,6 +334,229 @@ __global__ void __launch_bounds__(NT) qr_panel_reg_kernel(double* __restrict__ W
     }
 }
 
+// Asynchronous 8-byte global -> shared copies (all in flight until the wait).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Column-group panel (B = 32 columns, mp <= 32 + 8 RR rows, 256 threads).
+// Lane l of warp w has row group rg = l & 3 and column group cg = l >> 2: it
+// holds columns 4cg .. 4cg+3 on one top row, 4w + rg (the top 32 rows hold
+// the diagonal), and on RR/4 bulk rows, 32 + RR w + (RR/4) rg + 0 .. RR/4-1,
+// all in registers.  Step j needs v_j^T p_c for every column c.  Each warp's
+// share of column j sits in its four lanes of column group j/4; every lane
+// takes its rows of it from the lane of its row group by shuffles, keeps them
+// in registers for both the dot and the update, and forms four column sums;
+// two shuffle levels leave lane l with the warp's sum for column l, and one
+// block barrier per step adds the eight warps' sums.  The reflector's scaling is deferred: the sums use
+// the unscaled column u_j (zeroed at rows <= j), so
+//     v_j^T p_c = p_c[j] + scal_j sum_{r>j} u_j[r] p_c[r],
+// and the same sum for c = j is the squared norm dlarfg needs, so no separate
+// norm reduction is made.  A finished column keeps u until the end, where it
+// is scaled and its diagonal set to beta; its Gram entry v_c^T v_j is scal_c
+// times the sum above.  Row j of every column (read by all warps) and the
+// partial sums are double-buffered by step parity in shared memory, which is
+// what lets one barrier per step suffice.  The panel moves between global and
+// shared memory with coalesced copies.  Reflectors follow dlarfg as above.
+template <int RR>
+__global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                                           double* __restrict__ V, int ldv,
+                                                           double* __restrict__ T, int ldt) {
+    constexpr int B = 32, NW = 8, RB = RR / 4, RL = RB + 1;
+    static_assert(RR % 4 == 0 && RL % 2 == 0, "bulk rows per lane must be odd");
+    extern __shared__ double stage[];               // the panel, column-major, ld mp + 1
+    __shared__ double part[2][NW][B];               // per-warp column sums
+    __shared__ double rowj[2][B];                   // row j of every column
+    __shared__ double Gs[B][B + 1];                 // Gs[l][jj] = v_l^T v_jj, l < jj
+    __shared__ double taus[B], scals[B], betas[B];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int rg = lane & 3, cg = lane >> 2;
+    const int mp = m - j0;
+    const int ls = mp + 1;
+    constexpr int RT = (32 + 8 * RR + 255) / 256;  // rows of a column per thread in the copies
+#pragma unroll 4
+    for (int c = 0; c < b; ++c) {
+#pragma unroll
+        for (int h = 0; h < RT; ++h) {
+            const int r = tid + 256 * h;
+            if (r < mp) cp_async8(stage + (size_t)c * ls + r, W + (size_t)(j0 + c) * ldw + j0 + r);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    auto row_of = [&](int ri) { return ri == 0 ? 4 * w + rg : 32 + RR * w + RB * rg + (ri - 1); };
+    double p[4][RL];
+#pragma unroll
+    for (int ci = 0; ci < 4; ++ci) {
+        const int c = 4 * cg + ci;
+#pragma unroll
+        for (int ri = 0; ri < RL; ++ri) {
+            const int r = row_of(ri);
+            p[ci][ri] = (r < mp && c < b) ? stage[(size_t)c * ls + r] : 0.0;
+        }
+    }
+    // u <- this lane's rows of column slot `col` of lane `src`
+    auto fetch = [&](double(&u)[RL], const double(&col)[RL], int src) {
+#pragma unroll
+        for (int ri = 0; ri < RL; ++ri) u[ri] = __shfl_sync(0xffffffffu, col[ri], src);
+    };
+    auto tree8 = [](const double* x, int stride) {
+        return ((x[0] + x[stride]) + (x[2 * stride] + x[3 * stride])) +
+               ((x[4 * stride] + x[5 * stride]) + (x[6 * stride] + x[7 * stride]));
+    };
+#pragma unroll 1
+    for (int j = 0; j < b; ++j) {
+        const int par = j & 1;
+        const int jh = j >> 2, jl = j & 3;  // column j: group jh, slot jl; row j: warp jh, row group jl
+        if (w == jh && rg == jl) {
+#pragma unroll
+            for (int ci = 0; ci < 4; ++ci) rowj[par][4 * cg + ci] = p[ci][0];
+        }
+        double u[RL];
+        const int src = 4 * jh + rg;
+        if (jl == 0) fetch(u, p[0], src);
+        else if (jl == 1) fetch(u, p[1], src);
+        else if (jl == 2) fetch(u, p[2], src);
+        else fetch(u, p[3], src);
+        if (4 * w + rg <= j) u[0] = 0.0;  // top row at or above the diagonal
+        double acc[4][2];
+#pragma unroll
+        for (int ci = 0; ci < 4; ++ci) {
+            acc[ci][0] = 0.0;
+            acc[ci][1] = 0.0;
+#pragma unroll
+            for (int ri = 0; ri < RL; ++ri) acc[ci][ri & 1] = fma(u[ri], p[ci][ri], acc[ci][ri & 1]);
+        }
+        // reduce-scatter over the row groups: lane l ends with column 4cg + rg = l
+        const bool hi = rg & 2, lo = rg & 1;
+        double k0 = hi ? acc[2][0] + acc[2][1] : acc[0][0] + acc[0][1];
+        double k1 = hi ? acc[3][0] + acc[3][1] : acc[1][0] + acc[1][1];
+        const double s0 = hi ? acc[0][0] + acc[0][1] : acc[2][0] + acc[2][1];
+        const double s1 = hi ? acc[1][0] + acc[1][1] : acc[3][0] + acc[3][1];
+        k0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+        k1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+        const double keep = lo ? k1 : k0, send = lo ? k0 : k1;
+        part[par][w][lane] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+        __syncthreads();
+        static_assert(NW == 8, "eight warps");
+        const double S = tree8(&part[par][0][lane], B), xn2 = tree8(&part[par][0][j], B);
+        const double alpha = rowj[par][j];
+        double tau = 0, beta = alpha, scal = 1;
+        if (xn2 > 0.0) {
+            const double nrm = sqrt(alpha * alpha + xn2);
+            beta = alpha >= 0 ? -nrm : nrm;
+            const double amb = alpha - beta;
+            const double rinv = 1.0 / (beta * amb);  // tau = -amb / beta, scal = 1 / amb
+            tau = -amb * amb * rinv;
+            scal = beta * rinv;
+        }
+        const double g = fma(scal, S, rowj[par][lane]);  // v_j^T p_lane
+        if (tau != 0.0) {
+            double tg[4];
+#pragma unroll
+            for (int ci = 0; ci < 4; ++ci) {
+                const double gc = __shfl_sync(0xffffffffu, g, (lane & ~3) | ci);
+                tg[ci] = (4 * cg + ci > j) ? tau * gc : 0.0;
+            }
+#pragma unroll
+            for (int ci = 0; ci < 4; ++ci) {
+                const double cu = tg[ci] * scal;
+#pragma unroll
+                for (int ri = 0; ri < RL; ++ri) p[ci][ri] = fma(-cu, u[ri], p[ci][ri]);
+            }
+            if (w == jh && rg == jl) {
+#pragma unroll
+                for (int ci = 0; ci < 4; ++ci) p[ci][0] -= tg[ci];
+            }
+        }
+        if (w == 0) {
+            if (lane < j) Gs[lane][j] = scals[lane] * g;
+            if (lane == j) {
+                taus[j] = tau;
+                scals[j] = scal;
+                betas[j] = beta;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ci = 0; ci < 4; ++ci) {
+        const int c = 4 * cg + ci;
+        if (c < b) {
+            const double sc = scals[c], be = betas[c];
+#pragma unroll
+            for (int ri = 0; ri < RL; ++ri) {
+                const int r = row_of(ri);
+                if (r < mp) stage[(size_t)c * ls + r] = r < c ? p[ci][ri] : (r == c ? be : sc * p[ci][ri]);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int c = 0; c < b; ++c) {
+#pragma unroll
+        for (int h = 0; h < RT; ++h) {
+            const int r = tid + 256 * h;
+            if (r < mp) {
+                const double val = stage[(size_t)c * ls + r];
+                W[(size_t)(j0 + c) * ldw + j0 + r] = val;
+                V[(size_t)c * ldv + r] = r < c ? 0.0 : (r == c ? 1.0 : val);
+            }
+        }
+    }
+    // dlarft (forward, columnwise), lane i of warp 0 builds row i of T
+    if (w == 0) {
+        const int i = lane;
+        double trow[B];
+#pragma unroll
+        for (int jj = 0; jj < B; ++jj) {
+            double a0 = 0, a1 = 0;
+#pragma unroll
+            for (int l = 0; l < jj; ++l) {
+                const double term = (l >= i) ? trow[l] * Gs[l][jj] : 0.0;
+                if (l & 1) a1 += term; else a0 += term;
+            }
+            const double tj = jj < b ? taus[jj] : 0.0;
+            trow[jj] = (jj < i) ? 0.0 : (jj == i ? tj : -tj * (a0 + a1));
+        }
+#pragma unroll
+        for (int jj = 0; jj < B; ++jj)
+            if (i < b && jj < b) T[(size_t)jj * ldt + i] = trow[jj];
+    }
+}
+
+// Panel launch: the column-per-lane kernel for 32-wide panels, the row-per-thread
+// register kernel otherwise.
+template <int NT, int R, int B, int U>
+void launch_panel(cudaStream_t st, double* W, int ldw, int m, int j0, int b, double* V, int ldv, double* T, int ldt) {
+    const int mp = m - j0;
+    if (B == 32 && mp <= 32 + 8 * 60) {
+        static thread_local int attr_dev = -1;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const size_t maxb = sizeof(double) * (size_t)(32 + 8 * 60 + 1) * 32;
+        if (attr_dev != dev) {
+            cudaFuncSetAttribute(qr_panel_col_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
+            cudaFuncSetAttribute(qr_panel_col_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
+            cudaFuncSetAttribute(qr_panel_col_kernel<28>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
+            cudaFuncSetAttribute(qr_panel_col_kernel<60>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
+            attr_dev = dev;
+        }
+        const size_t sm = sizeof(double) * (size_t)(mp + 1) * b;
+        if (mp <= 64) qr_panel_col_kernel<4><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
+        else if (mp <= 128) qr_panel_col_kernel<12><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
+        else if (mp <= 256) qr_panel_col_kernel<28><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
+        else qr_panel_col_kernel<60><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
+    } else {
+        qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
+    }
+}
+
 // C (mp x nc, ld ldc) <- (I - V T' V^T) C with T' = T^T (TRANS: applying Q^T,
 // the trailing update) or T (forming Q).  V is mp x b (ld ldv, unit lower
 // trapezoidal, explicit), T is b x b upper triangular (ld ldt), b <= B.
@@ -348,18 +571,13 @@ constexpr int WY_THREADS = 256;
 
 inline size_t wy_smem_bytes(int mp, int B) { return sizeof(double) * (size_t)(mp + 1) * (B + WY_COLS); }
 
-__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-}
 
 template <int B, bool TRANS>
 __global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __restrict__ V, int ldv,
                                                               const double* __restrict__ T, int ldt, int b,
-                                                              double* __restrict__ C, int ldc, int mp, int nc) {
+                                                              double* __restrict__ C, int ldc, int mp, int nc,
+                                                              double* __restrict__ C2 = nullptr, int ldc2 = 0,
+                                                              int nc2 = 0) {
     constexpr int NPART = WY_THREADS / (B * WY_COLS);  // row partitions of the Z reduction
     extern __shared__ double wsm[];
     const int ld = mp + 1;
@@ -368,7 +586,16 @@ __global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __re
     __shared__ double Zp[NPART][B][WY_COLS];
     __shared__ double Z2[B][WY_COLS];
     const int tid = threadIdx.x;
-    const int c0 = blockIdx.x * WY_COLS;
+    // blocks past the first target's columns work on the second target (same V, T)
+    int blk = blockIdx.x;
+    const int nblk1 = (nc + WY_COLS - 1) / WY_COLS;
+    if (blk >= nblk1) {
+        blk -= nblk1;
+        C = C2;
+        ldc = ldc2;
+        nc = nc2;
+    }
+    const int c0 = blk * WY_COLS;
     const int ncol = min(WY_COLS, nc - c0);
     for (int e = tid; e < mp * B; e += WY_THREADS) {
         const int r = e % mp, col = e / mp;
@@ -453,24 +680,25 @@ __global__ void extract_r_kernel(const double* W, int ldw, int k, int n, double*
     }
 }
 
-__global__ void copy_cols_kernel(const double* __restrict__ src, int lds, double* __restrict__ dst, int ldd, int m,
-                                 int k) {
-    const long long total = (long long)m * k;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(e % m), j = (int)(e / m);
-        dst[(size_t)j * ldd + i] = src[(size_t)j * lds + i];
+// dst (cols x rows, ld ldd) = src (rows x cols, ld lds)^T, through 32 x 32 shared tiles
+__global__ void transpose_kernel(const double* __restrict__ src, int lds, double* __restrict__ dst, int ldd, int rows,
+                                 int cols) {
+    __shared__ double tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = r0 + threadIdx.x, c = c0 + y;
+        if (r < rows && c < cols) tile[y][threadIdx.x] = src[(size_t)c * lds + r];
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int c = c0 + threadIdx.x, r = r0 + y;
+        if (r < rows && c < cols) dst[(size_t)r * ldd + c] = tile[threadIdx.x][y];
     }
 }
 
 inline int g1d(long long n) {
     long long b = (n + 255) / 256;
     return (int)std::max<long long>(1, std::min<long long>(b, 148 * 8));
-}
-
-int copy2d_f64(int m, int k, const double* src, int lds, double* dst, int ldd, cudaStream_t st) {
-    copy_cols_kernel<<<g1d((long long)m * k), 256, 0, st>>>(src, lds, dst, ldd, m, k);
-    TN_LAUNCH_CHECK();
-    return TN_OK;
 }
 
 int panel_width(int m) {
@@ -487,30 +715,29 @@ namespace {
 
 // Several panels: look-ahead on two streams.  The main stream runs panel k,
 // then applies its block reflector to panel k+1's columns only ("narrow"),
-// then panel k+1; the side stream applies it to the columns beyond
-// ("wide") and accumulates Q forward, Q <- Q (I - V_k T_k V_k^T) on the full
-// m x m Q (three FP64 GEMMs), while the main stream factors later panels.
-// The narrow update of panel k+1 waits for the wide update of panel k, which
-// brought panel k+2's columns up to date.  Q's first k columns and R are read
-// out once the side stream has finished.
+// then panel k+1; the side stream, meanwhile, applies it to the columns
+// beyond ("wide") and accumulates Q forward, Q <- Q (I - V_k T_k V_k^T), kept
+// transposed (Qt = Q^T, m x m) so that the same kernel serves both targets in
+// one launch: Qt[j0:, :] <- (I - V T^T V^T) Qt[j0:, :].  The narrow update of
+// panel k+1 waits for the wide update of panel k, which brought panel k+2's
+// columns up to date.  R and Q's first k columns (Qt's first k rows,
+// transposed) are read out once the side stream has finished.
 template <int NT, int R, int B, int U>
 int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr, double* Vall,
                  double* Tall) {
     cudaStream_t s0 = c.stream, s1 = c.aux;
     cudaEvent_t ev_p = c.ev_x[0], ev_w = c.ev_x[1], ev_q = c.ev_x[2];
     const int k = std::min(m, n);
-    double *Qf = nullptr, *Z = nullptr, *Z2 = nullptr;
+    double* Qt = nullptr;
     if (Qout) {
-        TN_CHECK(c.qaccum.ensure(sizeof(double) * ((size_t)m * m + 2 * (size_t)m * B)));
-        Qf = c.qaccum.as<double>();
-        Z = Qf + (size_t)m * m;
-        Z2 = Z + (size_t)m * B;
+        TN_CHECK(c.qaccum.ensure(sizeof(double) * (size_t)m * m));
+        Qt = c.qaccum.as<double>();
     }
     // the side stream starts after everything already queued on the main stream
     TN_CUDA_CHECK(cudaEventRecord(ev_p, s0));
     TN_CUDA_CHECK(cudaStreamWaitEvent(s1, ev_p, 0));
     if (Qout) {
-        set_identity_kernel<<<g1d((long long)m * m), 256, 0, s1>>>(Qf, m, m, m);
+        set_identity_kernel<<<g1d((long long)m * m), 256, 0, s1>>>(Qt, m, m, m);
         TN_LAUNCH_CHECK();
     }
     bool have_wide = false;
@@ -519,7 +746,7 @@ int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
         const int mp = m - j0;
         double* Vp = Vall + (size_t)j0 * m + j0;  // ld m
         double* Tp = Tall + (size_t)j0 * B;        // ld B
-        qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, s0>>>(W, m, m, j0, b, Vp, m, Tp, B);
+        launch_panel<NT, R, B, U>(s0, W, m, m, j0, b, Vp, m, Tp, B);
         TN_LAUNCH_CHECK();
         TN_CUDA_CHECK(cudaEventRecord(ev_p, s0));
         // narrow: the next panel's columns (after the previous wide update reached them)
@@ -531,37 +758,18 @@ int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
                 Vp, m, Tp, B, b, W + (size_t)c1 * m + j0, m, mp, nb_next);
             TN_LAUNCH_CHECK();
         }
-        // wide: every column beyond the next panel, on the side stream
+        // wide: every column beyond the next panel, and Qt's rows j0.., on the side stream
         TN_CUDA_CHECK(cudaStreamWaitEvent(s1, ev_p, 0));
         const int c2 = c1 + nb_next;
-        if (n - c2 > 0) {
-            wy_apply_kernel<B, true><<<(n - c2 + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(mp, B), s1>>>(
-                Vp, m, Tp, B, b, W + (size_t)c2 * m + j0, m, mp, n - c2);
+        const int nw = std::max(0, n - c2), nq = Qout ? m : 0;
+        const int blocks = (nw + WY_COLS - 1) / WY_COLS + (nq + WY_COLS - 1) / WY_COLS;
+        if (blocks > 0) {
+            wy_apply_kernel<B, true><<<blocks, WY_THREADS, wy_smem_bytes(mp, B), s1>>>(
+                Vp, m, Tp, B, b, W + (size_t)c2 * m + j0, m, mp, nw, Qt ? Qt + j0 : nullptr, m, nq);
             TN_LAUNCH_CHECK();
         }
         TN_CUDA_CHECK(cudaEventRecord(ev_w, s1));
         have_wide = true;
-        if (Qout) {
-            // Q[:, j0:] <- Q[:, j0:] - (Q[:, j0:] V) T V^T
-            GemmArgs g;
-            g.M = m; g.N = b; g.K = mp;
-            g.A.ptr = Qf + (size_t)j0 * m; g.A.mn = idx(1); g.A.k = idx(m);
-            g.B.ptr = Vp; g.B.k = idx(1); g.B.mn = idx(m);
-            g.C.ptr = Z; g.C.m = idx(1); g.C.n = idx(m);
-            TN_CHECK(gemm_f64(g, s1));
-            GemmArgs h;
-            h.M = m; h.N = b; h.K = b;
-            h.A.ptr = Z; h.A.mn = idx(1); h.A.k = idx(m);
-            h.B.ptr = Tp; h.B.k = idx(1); h.B.mn = idx(B);
-            h.C.ptr = Z2; h.C.m = idx(1); h.C.n = idx(m);
-            TN_CHECK(gemm_f64(h, s1));
-            GemmArgs u;
-            u.M = m; u.N = mp; u.K = b; u.alpha = -1.0; u.beta = 1.0;
-            u.A.ptr = Z2; u.A.mn = idx(1); u.A.k = idx(m);
-            u.B.ptr = Vp; u.B.k = idx(m); u.B.mn = idx(1);
-            u.C.ptr = Qf + (size_t)j0 * m; u.C.m = idx(1); u.C.n = idx(m);
-            TN_CHECK(gemm_f64(u, s1));
-        }
     }
     TN_CUDA_CHECK(cudaEventRecord(ev_q, s1));
     TN_CUDA_CHECK(cudaStreamWaitEvent(s0, ev_q, 0));
@@ -569,7 +777,11 @@ int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
         extract_r_kernel<<<g1d((long long)k * n), 256, 0, s0>>>(W, m, k, n, Rout, ldr);
         TN_LAUNCH_CHECK();
     }
-    if (Qout) TN_CHECK(copy2d_f64(m, k, Qf, m, Qout, ldq, s0));
+    if (Qout) {
+        dim3 grid((m + 31) / 32, (k + 31) / 32);
+        transpose_kernel<<<grid, dim3(32, 8), 0, s0>>>(Qt, m, Qout, ldq, k, m);
+        TN_LAUNCH_CHECK();
+    }
     return TN_OK;
 }
 
@@ -596,7 +808,7 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
         const int mp = m - j0;
         double* Vp = Vall + (size_t)j0 * m + j0;  // ld m
         double* Tp = Tall + (size_t)j0 * B;        // ld B
-        qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, st>>>(W, m, m, j0, b, Vp, m, Tp, B);
+        launch_panel<NT, R, B, U>(st, W, m, m, j0, b, Vp, m, Tp, B);
         TN_LAUNCH_CHECK();
         const int nt = n - j0 - b;
         if (nt > 0) {

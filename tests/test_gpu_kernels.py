@@ -135,6 +135,27 @@ def test_qr_lq(T, ctx, oracle, m, n):
     assert np.allclose(np.tril(Lm), Lm)
 
 
+@pytest.mark.parametrize("m,n", [(512, 256), (300, 200), (256, 96)])
+def test_qr_rank_deficient_panels(T, ctx, oracle, m, n):
+    """Several panels (with a ragged last one) on a matrix whose columns repeat."""
+    rng = np.random.default_rng(m + n)
+    A = rng.uniform(-1, 1, size=(m, n))
+    A[:, 1::3] = A[:, 0::3][:, :A[:, 1::3].shape[1]] * 0.5
+    k = min(m, n)
+    # exact dependence: past a zero pivot R is set by rounding, so check the invariants
+    Q, R = T.CudaQRSolver(ctx).SolveThinQR(A)
+    assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-13
+    assert np.abs(Q @ R - A).max() < 1e-12
+    assert np.allclose(np.triu(R), R)
+    assert np.abs(np.diag(R)[1::3]).max() < 1e-12
+    # near dependence: the factors are determined, so they match the oracle's
+    A[:, 1::3] += 1e-3 * rng.uniform(-1, 1, size=A[:, 1::3].shape)
+    Q, R = T.CudaQRSolver(ctx).SolveThinQR(A)
+    Qo, Ro = oracle.qr(A)
+    np.testing.assert_allclose(R, Ro, atol=1e-10)
+    assert np.abs(Q @ R - A).max() < 1e-12
+
+
 def test_qr_zero_columns_complete(T, ctx):
     rng = np.random.default_rng(1)
     A = np.zeros((40, 16))
