@@ -12,6 +12,8 @@
 
 #include "qr.h"
 
+#include <cooperative_groups.h>
+
 namespace tnb {
 
 namespace {
@@ -349,11 +351,12 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // holds columns 4cg .. 4cg+3 on one top row, 4w + rg (the top 32 rows hold
 // the diagonal), and on RR/4 bulk rows, 32 + RR w + (RR/4) rg + 0 .. RR/4-1,
 // all in registers.  Step j needs v_j^T p_c for every column c.  Each warp's
-// share of column j sits in its four lanes of column group j/4; every lane
-// takes its rows of it from the lane of its row group by shuffles, keeps them
-// in registers for both the dot and the update, and forms four column sums;
-// two shuffle levels leave lane l with the warp's sum for column l, and one
-// block barrier per step adds the eight warps' sums.  The reflector's scaling is deferred: the sums use
+// share of column j sits in its four lanes of column group j/4, which copy it
+// to the warp's slice of shared memory as soon as step j-1 has updated it;
+// every lane reads its rows of it (broadcast), keeps them in registers for
+// both the dot and the update, and forms four column sums; two shuffle levels
+// leave lane l with the warp's sum for column l, and one block barrier per
+// step adds the eight warps' sums.  The reflector's scaling is deferred: the sums use
 // the unscaled column u_j (zeroed at rows <= j), so
 //     v_j^T p_c = p_c[j] + scal_j sum_{r>j} u_j[r] p_c[r],
 // and the same sum for c = j is the squared norm dlarfg needs, so no separate
@@ -371,6 +374,7 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
     static_assert(RR % 4 == 0 && RL % 2 == 0, "bulk rows per lane must be odd");
     extern __shared__ double stage[];               // the panel, column-major, ld mp + 1
     __shared__ double part[2][NW][B];               // per-warp column sums
+    __shared__ double2 vb[2][NW][RL / 2][4];        // each warp's rows of u_j, row pairs by row group
     __shared__ double rowj[2][B];                   // row j of every column
     __shared__ double Gs[B][B + 1];                 // Gs[l][jj] = v_l^T v_jj, l < jj
     __shared__ double taus[B], scals[B], betas[B];
@@ -400,11 +404,23 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
             p[ci][ri] = (r < mp && c < b) ? stage[(size_t)c * ls + r] : 0.0;
         }
     }
-    // u <- this lane's rows of column slot `col` of lane `src`
-    auto fetch = [&](double(&u)[RL], const double(&col)[RL], int src) {
+    // this lane's rows of column slot `col` -> the warp's slice for step jn (zero at rows <= jn)
+    auto publish = [&](const double(&col)[RL], int jn) {
 #pragma unroll
-        for (int ri = 0; ri < RL; ++ri) u[ri] = __shfl_sync(0xffffffffu, col[ri], src);
+        for (int ri = 0; ri < RL; ri += 2) {
+            double x0 = col[ri];
+            if (ri == 0 && 4 * w + rg <= jn) x0 = 0.0;  // top row at or above the diagonal
+            vb[jn & 1][w][ri / 2][rg] = make_double2(x0, col[ri + 1]);
+        }
     };
+    auto publish_slot = [&](int jn) {
+        const int sl = jn & 3;
+        if (sl == 0) publish(p[0], jn);
+        else if (sl == 1) publish(p[1], jn);
+        else if (sl == 2) publish(p[2], jn);
+        else publish(p[3], jn);
+    };
+    if (cg == 0) publish_slot(0);
     auto tree8 = [](const double* x, int stride) {
         return ((x[0] + x[stride]) + (x[2 * stride] + x[3 * stride])) +
                ((x[4 * stride] + x[5 * stride]) + (x[6 * stride] + x[7 * stride]));
@@ -417,13 +433,14 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
 #pragma unroll
             for (int ci = 0; ci < 4; ++ci) rowj[par][4 * cg + ci] = p[ci][0];
         }
+        __syncwarp();
         double u[RL];
-        const int src = 4 * jh + rg;
-        if (jl == 0) fetch(u, p[0], src);
-        else if (jl == 1) fetch(u, p[1], src);
-        else if (jl == 2) fetch(u, p[2], src);
-        else fetch(u, p[3], src);
-        if (4 * w + rg <= j) u[0] = 0.0;  // top row at or above the diagonal
+#pragma unroll
+        for (int ri = 0; ri < RL; ri += 2) {
+            const double2 u2 = vb[par][w][ri / 2][rg];
+            u[ri] = u2.x;
+            u[ri + 1] = u2.y;
+        }
         double acc[4][2];
 #pragma unroll
         for (int ci = 0; ci < 4; ++ci) {
@@ -474,6 +491,7 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
                 for (int ci = 0; ci < 4; ++ci) p[ci][0] -= tg[ci];
             }
         }
+        if (j + 1 < b && cg == ((j + 1) >> 2)) publish_slot(j + 1);
         if (w == 0) {
             if (lane < j) Gs[lane][j] = scals[lane] * g;
             if (lane == j) {
@@ -505,7 +523,7 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
             if (r < mp) {
                 const double val = stage[(size_t)c * ls + r];
                 W[(size_t)(j0 + c) * ldw + j0 + r] = val;
-                V[(size_t)c * ldv + r] = r < c ? 0.0 : (r == c ? 1.0 : val);
+                if (V) V[(size_t)c * ldv + r] = r < c ? 0.0 : (r == c ? 1.0 : val);
             }
         }
     }
@@ -559,7 +577,8 @@ void launch_panel(cudaStream_t st, double* W, int ldw, int m, int j0, int b, dou
 
 // C (mp x nc, ld ldc) <- (I - V T' V^T) C with T' = T^T (TRANS: applying Q^T,
 // the trailing update) or T (forming Q).  V is mp x b (ld ldv, unit lower
-// trapezoidal, explicit), T is b x b upper triangular (ld ldt), b <= B.
+// trapezoidal; only the entries below the diagonal are read, so V may be the
+// factored panel itself), T is b x b upper triangular (ld ldt), b <= B.
 // One CTA per 8 columns of C.  The whole of V and the CTA's columns of C are
 // staged in shared memory by asynchronous copies (all in flight at once; the
 // kernel is latency bound otherwise), then Z = V^T C, Z2 = T' Z, C -= V Z2.
@@ -599,8 +618,8 @@ __global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __re
     const int ncol = min(WY_COLS, nc - c0);
     for (int e = tid; e < mp * B; e += WY_THREADS) {
         const int r = e % mp, col = e / mp;
-        if (col < b) cp_async8(Vs + (size_t)col * ld + r, V + (size_t)col * ldv + r);
-        else Vs[(size_t)col * ld + r] = 0.0;
+        if (col < b && r > col) cp_async8(Vs + (size_t)col * ld + r, V + (size_t)col * ldv + r);
+        else Vs[(size_t)col * ld + r] = (col < b && r == col) ? 1.0 : 0.0;
     }
     for (int e = tid; e < mp * WY_COLS; e += WY_THREADS) {
         const int r = e % mp, col = e / mp;
@@ -662,6 +681,97 @@ __global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __re
         for (int q = 0; q < WY_COLS; ++q)
             if (q < ncol) C[(size_t)(c0 + q) * ldc + r] = acc[q];
     }
+}
+
+// Narrow trailing update, C (mp x nc) <- (I - V T^T V^T) C, for a few columns
+// on the critical path.  The rows are split over a cluster of four CTAs (each
+// stages only its quarter of V and C); each CTA forms its partial Z = V^T C
+// (B x 8), the cluster adds the four partials through distributed shared
+// memory, and each CTA applies Z2 = T^T Z to its own rows.
+constexpr int WYN_RANKS = 4;
+template <int B>
+__global__ void __cluster_dims__(1, WYN_RANKS, 1) __launch_bounds__(256)
+    wy_narrow_kernel(const double* __restrict__ V, int ldv, const double* __restrict__ T, int ldt, int b,
+                     double* __restrict__ C, int ldc, int mp, int nc) {
+    constexpr int NC = WY_COLS;
+    static_assert(B * NC == 256, "one thread per entry of Z");
+    extern __shared__ double wsm[];
+    __shared__ double Zp[B][NC];  // this CTA's partial V^T C
+    __shared__ double Zs[B][NC];
+    __shared__ double Z2[B][NC];
+    namespace cgx = cooperative_groups;
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int tid = threadIdx.x;
+    const int rb = (mp + WYN_RANKS - 1) / WYN_RANKS;
+    const int r0 = rank * rb, nr = max(0, min(rb, mp - r0));
+    const int ld = rb + 1;
+    double* Vs = wsm;
+    double* Cs = Vs + (size_t)ld * B;
+    const int c0 = blockIdx.x * NC, ncol = min(NC, nc - c0);
+    for (int e = tid; e < nr * B; e += 256) {
+        const int r = e % nr, col = e / nr;
+        if (col < b && r0 + r > col) cp_async8(Vs + (size_t)col * ld + r, V + (size_t)col * ldv + r0 + r);
+        else Vs[(size_t)col * ld + r] = (col < b && r0 + r == col) ? 1.0 : 0.0;
+    }
+    for (int e = tid; e < nr * NC; e += 256) {
+        const int r = e % nr, col = e / nr;
+        if (col < ncol) cp_async8(Cs + (size_t)col * ld + r, C + (size_t)(c0 + col) * ldc + r0 + r);
+        else Cs[(size_t)col * ld + r] = 0.0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    {
+        const int l = tid % B, q = tid / B;
+        const double* vcol = Vs + (size_t)l * ld;
+        const double* ccol = Cs + (size_t)q * ld;
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        int r = 0;
+        for (; r + 3 < nr; r += 4) {
+            a0 = fma(vcol[r], ccol[r], a0);
+            a1 = fma(vcol[r + 1], ccol[r + 1], a1);
+            a2 = fma(vcol[r + 2], ccol[r + 2], a2);
+            a3 = fma(vcol[r + 3], ccol[r + 3], a3);
+        }
+        for (; r < nr; ++r) a0 = fma(vcol[r], ccol[r], a0);
+        Zp[l][q] = (a0 + a1) + (a2 + a3);
+    }
+    cluster.sync();
+    {
+        const int l = tid % B, q = tid / B;
+        double z = 0;
+#pragma unroll
+        for (int k = 0; k < WYN_RANKS; ++k) z += cluster.map_shared_rank(&Zp[0][0], k)[l * NC + q];
+        Zs[l][q] = z;
+    }
+    cluster.sync();  // every rank has read the partials; they may go away now
+    {
+        const int bb = tid % B, q = tid / B;
+        double s = 0;
+        if (bb < b)
+            for (int l = 0; l <= bb; ++l) s = fma(T[(size_t)bb * ldt + l], Zs[l][q], s);
+        Z2[bb][q] = s;
+    }
+    __syncthreads();
+    for (int r = tid; r < nr; r += 256) {
+        double acc[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) acc[q] = Cs[(size_t)q * ld + r];
+#pragma unroll 4
+        for (int l = 0; l < B; ++l) {
+            const double vl = Vs[(size_t)l * ld + r];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) acc[q] = fma(-vl, Z2[l][q], acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (q < ncol) C[(size_t)(c0 + q) * ldc + r0 + r] = acc[q];
+    }
+}
+
+inline size_t wyn_smem_bytes(int mp, int B) {
+    const int rb = (mp + WYN_RANKS - 1) / WYN_RANKS;
+    return sizeof(double) * (size_t)(rb + 1) * (B + WY_COLS);
 }
 
 __global__ void set_identity_kernel(double* Q, int m, int k, int ldq) {
@@ -744,9 +854,10 @@ int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
     for (int j0 = 0; j0 < k; j0 += B) {
         const int b = std::min(B, k - j0);
         const int mp = m - j0;
-        double* Vp = Vall + (size_t)j0 * m + j0;  // ld m
-        double* Tp = Tall + (size_t)j0 * B;        // ld B
-        launch_panel<NT, R, B, U>(s0, W, m, m, j0, b, Vp, m, Tp, B);
+        // the 32-wide panel kernel leaves the reflectors only in W (below the diagonal)
+        double* Vp = B == 32 ? W + (size_t)j0 * m + j0 : Vall + (size_t)j0 * m + j0;  // ld m
+        double* Tp = Tall + (size_t)j0 * B;                                           // ld B
+        launch_panel<NT, R, B, U>(s0, W, m, m, j0, b, B == 32 ? nullptr : Vp, m, Tp, B);
         TN_LAUNCH_CHECK();
         TN_CUDA_CHECK(cudaEventRecord(ev_p, s0));
         // narrow: the next panel's columns (after the previous wide update reached them)
@@ -754,8 +865,14 @@ int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
         const int nb_next = std::max(0, std::min(B, k - c1));
         if (nb_next > 0) {
             if (have_wide) TN_CUDA_CHECK(cudaStreamWaitEvent(s0, ev_w, 0));
-            wy_apply_kernel<B, true><<<(nb_next + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(mp, B), s0>>>(
-                Vp, m, Tp, B, b, W + (size_t)c1 * m + j0, m, mp, nb_next);
+            if (B == 32) {
+                dim3 grid((nb_next + WY_COLS - 1) / WY_COLS, WYN_RANKS);
+                wy_narrow_kernel<32><<<grid, 256, wyn_smem_bytes(mp, 32), s0>>>(Vp, m, Tp, B, b,
+                                                                                W + (size_t)c1 * m + j0, m, mp, nb_next);
+            } else {
+                wy_apply_kernel<B, true><<<(nb_next + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(mp, B), s0>>>(
+                    Vp, m, Tp, B, b, W + (size_t)c1 * m + j0, m, mp, nb_next);
+            }
             TN_LAUNCH_CHECK();
         }
         // wide: every column beyond the next panel, and Qt's rows j0.., on the side stream
@@ -796,6 +913,9 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
         const int bytes = (int)wy_smem_bytes(B == 32 ? 512 : 1024, B);
         TN_CUDA_CHECK(cudaFuncSetAttribute(wy_apply_kernel<B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         TN_CUDA_CHECK(cudaFuncSetAttribute(wy_apply_kernel<B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        if (B == 32)
+            TN_CUDA_CHECK(cudaFuncSetAttribute(wy_narrow_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)wyn_smem_bytes(512, 32)));
         attr_set[B == 32] = dev;
     }
     size_t need = sizeof(double) * ((size_t)m * k + (size_t)B * k + 16);
