@@ -155,6 +155,8 @@ int tn_ctx_create(int device, tn_ctx* out) {
     c->c.stream = c->c.own_stream;
     TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.aux, cudaStreamNonBlocking));
     for (auto& e : c->c.ev_x) TN_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.aux2, cudaStreamNonBlocking));
+    for (auto& e : c->c.ev_y) TN_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     TN_CUDA_CHECK(cudaEventCreate(&c->c.ev_a));
     TN_CUDA_CHECK(cudaEventCreate(&c->c.ev_b));
     *out = c;
@@ -167,9 +169,13 @@ int tn_ctx_destroy(tn_ctx c) {
     cudaStreamSynchronize(c->c.stream);
     c->c.clear_graphs();
     if (c->c.aux) cudaStreamSynchronize(c->c.aux);
+    if (c->c.aux2) cudaStreamSynchronize(c->c.aux2);
     for (auto& e : c->c.ev_x)
         if (e) cudaEventDestroy(e);
+    for (auto& e : c->c.ev_y)
+        if (e) cudaEventDestroy(e);
     if (c->c.aux) cudaStreamDestroy(c->c.aux);
+    if (c->c.aux2) cudaStreamDestroy(c->c.aux2);
     if (c->c.ev_a) cudaEventDestroy(c->c.ev_a);
     if (c->c.ev_b) cudaEventDestroy(c->c.ev_b);
     if (c->c.own_stream) cudaStreamDestroy(c->c.own_stream);

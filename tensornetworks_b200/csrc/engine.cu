@@ -315,6 +315,7 @@ int MPSState::gauge_qr(int m, int n, double* W, double* Q, double* R, int ldr) {
 int MPSState::normalize_site(int ia, bool left) {
     cudaStream_t st = ctx->stream;
     // HandleEdges
+    if ((!left && ia == 1) || (left && ia == L)) rq_order();
     if (!left && ia == 1) {
         if (L > 1) {
             int newD2 = std::max(bondK[1], d);
@@ -342,6 +343,7 @@ int MPSState::normalize_site(int ia, bool left) {
         TN_CHECK(copy2d(m, n, Aia, idx2(1, a1, blk), idx(a1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
         TN_CHECK(gauge_qr(m, n, Wqr.as<double>(), Qqr.as<double>(), Rb->as<double>(), k));
         // site := Q with D2 = k
+        rq_order();
         TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(1, a1, (long long)a1 * k), idx(a1), 1.0, st));
         D2[ia] = k;
         // right neighbour: M_n <- R M_n
@@ -369,6 +371,7 @@ int MPSState::normalize_site(int ia, bool left) {
         TN_CHECK(copy2d(m, n, Aia, idx2(a1, a2, blk), idx(1), Wqr.as<double>(), idx(1), idx(m), 1.0, st));
         TN_CHECK(gauge_qr(m, n, Wqr.as<double>(), Qqr.as<double>(), Rb->as<double>(), k));
         // site := Q^T with D1 = k: element (n_, i1', i2) = Q(n_*D2+i2, i1')
+        rq_order();
         TN_CHECK(copy2d(m, k, Qqr.as<double>(), idx(1), idx(m), Aia, idx2(k, a2, (long long)k * a2), idx(1), 1.0, st));
         D1[ia] = k;
         // left neighbour: M_n <- M_n L, L = R^T (n x k)
@@ -572,9 +575,18 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
         key = hash_val(key, b->p);
     LzResult rm{};
     TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel, key));
-    TN_CHECK(mixed_check_error(msite, st));
     matvecs += rm.matvecs;
     heff_flop += heff_flops(s) * rm.matvecs;
+    if (opt.refine_tol <= 0 && opt.verbose < 3 && ctx->aux2) {
+        // nothing here waits for the FP64 check: it runs beside the gauge move
+        TN_CHECK(rq_launch(ia, s, t, op.nLR, F, G, N, rm.theta2 - rm.theta));
+        matvecs += 1;
+        matvecs_fp64 += 1;
+        heff_flop += heff_flops(s);
+        if (!rm.converged) ++not_converged;
+        return TN_OK;
+    }
+    TN_CHECK(mixed_check_error(msite, st));
     // FP64 Rayleigh quotient and residual of the Ritz vector
     TN_CHECK(heff_matvec_f64(s, t, op.nLR, F, G, A[ia]->as<double>(), yvec.as<double>(), P, Q, nullptr, st));
     double theta = 0, resid = 0;
@@ -604,6 +616,64 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     iterDE[ia] = theta - Emin[ia];
     Emin[ia] = theta;
     gapE[ia] = theta2 - theta;
+    return TN_OK;
+}
+
+// The FP64 Rayleigh quotient and residual of site ia's eigenvector, on the
+// second side stream once the Lanczos solve has finished; the result (and the
+// split operator's error flag) is read by rq_collect().
+int MPSState::rq_launch(int ia, const ContractShape& s, const WTermDev* t, int nLR, const double* F, const double* G,
+                        long long N, double dtheta) {
+    cudaStream_t st = ctx->stream, sx = ctx->aux2;
+    TN_CHECK(rqhost.ensure(sizeof(double) * 4 * (size_t)(L + 2)));
+    if ((int)rq_pending.size() != L + 2) {
+        rq_pending.assign(L + 2, 0);
+        rq_dtheta.assign(L + 2, 0.0);
+    }
+    const size_t scr = sizeof(double) * contract_scratch_doubles(s);
+    TN_CHECK(rqP.ensure(scr));
+    TN_CHECK(rqQ.ensure(scr));
+    TN_CHECK(yvec.ensure(sizeof(double) * (size_t)N));
+    TN_CHECK(rqbuf.ensure(rayleigh_scratch_bytes(N, ctx->sm_count)));
+    double* slot = reinterpret_cast<double*>(rqhost.p) + 4 * (size_t)ia;
+    TN_CUDA_CHECK(cudaMemcpyAsync(slot + 3, msite.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TN_CUDA_CHECK(cudaEventRecord(ctx->ev_y[0], st));
+    TN_CUDA_CHECK(cudaStreamWaitEvent(sx, ctx->ev_y[0], 0));
+    const double* x = A[ia]->as<double>();
+    TN_CHECK(heff_matvec_f64(s, t, nLR, F, G, x, yvec.as<double>(), rqP.as<double>(), rqQ.as<double>(), nullptr, sx));
+    TN_CHECK(rayleigh_residual_async(sx, ctx->sm_count, N, x, yvec.as<double>(), rqbuf.p, slot));
+    TN_CUDA_CHECK(cudaEventRecord(ctx->ev_y[1], sx));
+    rq_pending[ia] = 1;
+    rq_dtheta[ia] = dtheta;
+    rq_inflight = true;
+    return TN_OK;
+}
+
+void MPSState::rq_order() {
+    if (rq_inflight) cudaStreamWaitEvent(ctx->stream, ctx->ev_y[1], 0);
+}
+
+int MPSState::rq_collect() {
+    if (!rq_inflight) return TN_OK;
+    TN_CUDA_CHECK(cudaEventSynchronize(ctx->ev_y[1]));
+    rq_inflight = false;
+    int bad = 0;
+    for (int ia = 1; ia <= L; ++ia) {
+        if (!rq_pending[ia]) continue;
+        rq_pending[ia] = 0;
+        const double* slot = reinterpret_cast<double*>(rqhost.p) + 4 * (size_t)ia;
+        int err = 0;
+        std::memcpy(&err, slot + 3, sizeof(int));
+        bad |= err;
+        const double theta = slot[0];
+        iterDE[ia] = theta - Emin[ia];
+        Emin[ia] = theta;
+        gapE[ia] = rq_dtheta[ia];
+    }
+    if (bad) {
+        set_error("tcgen05 GEMM: a bounded mbarrier wait expired");
+        return TN_CUDA_ERROR;
+    }
     return TN_OK;
 }
 
@@ -762,7 +832,7 @@ int MPSState::sweep(bool left, double epsEigen) {
                             1e6 * secs(t2, t3), launch_count() - n2);
         }
     }
-    return TN_OK;
+    return rq_collect();
 }
 
 // MPSImp::IncreaseBondDimensions (MPSImp.C:123-147) with Bond::NewBondDimension (Bond.C:60-84).

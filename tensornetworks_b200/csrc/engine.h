@@ -54,6 +54,14 @@ struct MPSState {
     std::vector<char> bondDirty;              // bond_s lags behind the latest factor
     std::vector<double> Emin, iterDE, gapE;
     DevBuf tmp, Wqr, Qqr, svdw, envA, envB, yvec, diagbuf;
+    // FP64 check of the split-precision eigenvector on the context's second side
+    // stream (refine_tol = 0): contraction scratch, reduction state, and per site
+    // (theta, -, resid, error flag) in pinned memory, applied by rq_collect().
+    DevBuf rqP, rqQ, rqbuf;
+    HostBuf rqhost;
+    std::vector<char> rq_pending;
+    std::vector<double> rq_dtheta;
+    bool rq_inflight = false;
     MixedSite msite;
     long long matvecs = 0, matvecs_fp64 = 0;
     double heff_flop = 0;
@@ -93,6 +101,10 @@ struct MPSState {
     int site_resize(int ia, int nD1, int nD2);
     int gauge_qr(int m, int n, double* W, double* Q, double* R, int ldr);
     int rescale_site(int ia);
+    int rq_launch(int ia, const ContractShape& s, const WTermDev* t, int nLR, const double* F, const double* G,
+                  long long N, double dtheta);
+    void rq_order();   // the context stream waits for the in-flight check (before A[ia] changes)
+    int rq_collect();  // wait for the checks and apply them to Emin / iterDE / gapE
 };
 
 }  // namespace tnb

@@ -12,6 +12,7 @@
 #include "tridiag.cuh"
 
 #include <cmath>
+#include <cstddef>
 
 namespace tnb {
 
@@ -545,6 +546,27 @@ int rayleigh_residual(Ctx& c, long long N, const double* x, const double* y, dou
     TN_CUDA_CHECK(cudaStreamSynchronize(st));
     *theta = hs->theta;
     *resid = hs->resid;
+    return TN_OK;
+}
+
+size_t rayleigh_scratch_bytes(long long N, int sm_count) {
+    return sizeof(LzState) + sizeof(double) * (2 * (size_t)vec_grid(N, sm_count) + 8);
+}
+
+int rayleigh_residual_async(cudaStream_t st, int sm_count, long long N, const double* x, const double* y, void* dev,
+                            double* host_out) {
+    const int grid = vec_grid(N, sm_count);
+    LzState* s = reinterpret_cast<LzState*>(dev);
+    double* partial = reinterpret_cast<double*>(reinterpret_cast<char*>(dev) + sizeof(LzState));
+    TN_CUDA_CHECK(cudaMemsetAsync(&s->counter, 0, sizeof(unsigned int), st));
+    rq_dots_kernel<<<grid, LZ_THREADS, 0, st>>>(x, y, N, partial, s);
+    TN_LAUNCH_CHECK();
+    rq_resid_kernel<<<grid, LZ_THREADS, 0, st>>>(x, y, N, partial, s);
+    TN_LAUNCH_CHECK();
+    static_assert(offsetof(LzState, theta2) == offsetof(LzState, theta) + sizeof(double) &&
+                      offsetof(LzState, resid) == offsetof(LzState, theta) + 2 * sizeof(double),
+                  "theta, theta2, resid are adjacent");
+    TN_CUDA_CHECK(cudaMemcpyAsync(host_out, &s->theta, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     return TN_OK;
 }
 

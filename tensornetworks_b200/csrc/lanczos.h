@@ -37,6 +37,12 @@ using MatvecFn = std::function<int(const double*, double*, const int*)>;
 
 // theta = x.y/x.x and |y - theta x|/|x| (device vectors; synchronises).
 int rayleigh_residual(Ctx& c, long long N, const double* x, const double* y, double* theta, double* resid);
+// The same on stream st without waiting: dev (rayleigh_scratch_bytes) holds the
+// reduction state; (theta, -, resid) land in host_out[0..2] (pinned) when the
+// stream gets there.
+size_t rayleigh_scratch_bytes(long long N, int sm_count);
+int rayleigh_residual_async(cudaStream_t st, int sm_count, long long N, const double* x, const double* y, void* dev,
+                            double* host_out);
 
 // tol: absolute residual target; tol_rel (>= 0): residual target relative to
 // the norm of the tridiagonal matrix (the operator's noise floor for the

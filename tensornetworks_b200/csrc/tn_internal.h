@@ -139,6 +139,9 @@ struct Ctx {
     // side stream for work that overlaps the main stream's critical path (QR look-ahead)
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_x[3] = {nullptr, nullptr, nullptr};
+    // second side stream: the FP64 check of a site's eigenvector, overlapping the gauge move
+    cudaStream_t aux2 = nullptr;
+    cudaEvent_t ev_y[2] = {nullptr, nullptr};
     // scratch
     DevBuf P, Q;           // contraction intermediates
     DevBuf lz;             // Lanczos basis + work vectors
