@@ -7,15 +7,31 @@
 namespace tnb {
 namespace {
 
-// Number of eigenvalues of the symmetric tridiagonal (a, b) below x.
-__device__ int sturm_count(int n, const double* a, const double* b, double x, double pivmin) {
-    int cnt = 0;
-    double q = a[0] - x;
-    if (q < 0) ++cnt;
+// Number of eigenvalues of the symmetric tridiagonal (a, b) below x: the sign
+// changes of p_0 = 1, p_k = (a_{k-1} - x) p_{k-1} - b_{k-2}^2 p_{k-2}, the
+// leading principal minors of T - x.  The three-term recurrence needs no
+// division (the ratio form q_k = p_k / p_{k-1} spends an FP64 division, a long
+// serial latency, on every step); the pair is rescaled to stay in range.  A
+// zero minor takes its predecessor's sign, as the ratio form's +pivmin does.
+__device__ int sturm_count(int n, const double* a, const double* b, double x) {
+    double pm = 1.0, p = a[0] - x;
+    bool neg = p < 0;
+    int cnt = neg;
     for (int i = 1; i < n; ++i) {
-        if (fabs(q) < pivmin) q = (q < 0 ? -pivmin : pivmin);
-        q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
-        if (q < 0) ++cnt;
+        const double pn = fma(a[i] - x, p, -(b[i - 1] * b[i - 1]) * pm);
+        pm = p;
+        p = pn;
+        const bool ng = p < 0 ? true : (p > 0 ? false : neg);
+        cnt += (ng != neg);
+        neg = ng;
+        const double mx = fmax(fabs(p), fabs(pm));
+        if (mx > 1e150) {
+            p *= 1e-150;
+            pm *= 1e-150;
+        } else if (mx < 1e-150 && mx > 0) {
+            p *= 1e150;
+            pm *= 1e150;
+        }
     }
     return cnt;
 }
@@ -31,13 +47,12 @@ __device__ double block_eig_k(int n, const double* a, const double* b, int k) {
         hi = fmax(hi, a[i] + r);
     }
     double scale = fmax(fabs(lo), fabs(hi));
-    double pivmin = 2.2e-16 * fmax(scale, 1e-300);
     lo -= 1e-14 * scale + 1e-300;
     hi += 1e-14 * scale + 1e-300;
     const int T = blockDim.x;
     for (int round = 0; round < 12; ++round) {
         double x = lo + (hi - lo) * (double)(threadIdx.x + 1) / (double)(T + 1);
-        int ok = sturm_count(n, a, b, x, pivmin) <= k;
+        int ok = sturm_count(n, a, b, x) <= k;
         int cnt = __syncthreads_count(ok);
         if (threadIdx.x == 0) {
             double nlo = cnt > 0 ? lo + (hi - lo) * (double)cnt / (double)(T + 1) : lo;
