@@ -38,6 +38,12 @@ void Ctx::clear_graphs() {
     lzgraphs.clear();
 }
 
+int Ctx::prof_events() {
+    for (auto& e : pev)
+        if (!e) TN_CUDA_CHECK(cudaEventCreate(&e));
+    return TN_OK;
+}
+
 int DevBuf::ensure(size_t nbytes) {
     if (nbytes <= bytes && p) return TN_OK;
     release();
@@ -173,6 +179,8 @@ int tn_ctx_destroy(tn_ctx c) {
     for (auto& e : c->c.ev_x)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->c.ev_y)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->c.pev)
         if (e) cudaEventDestroy(e);
     if (c->c.aux) cudaStreamDestroy(c->c.aux);
     if (c->c.aux2) cudaStreamDestroy(c->c.aux2);

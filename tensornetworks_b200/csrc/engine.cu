@@ -556,7 +556,12 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     // channels carrying the completed block energy (lower form: left 0, right Dw-1)
     const int wF = H->form == TN_FORM_REGULAR_LOWER ? 0 : op.Dw1 - 1;
     const int wG = H->form == TN_FORM_REGULAR_LOWER ? op.Dw2 - 1 : 0;
+    if (ctx->prof) {
+        TN_CHECK(ctx->prof_events());
+        TN_CUDA_CHECK(cudaEventRecord(ctx->pev[0], st));
+    }
     TN_CHECK(mixed_prepare_site(*ctx, msite, s, t, op.nLR, F, G, wF, wG, ns));
+    if (ctx->prof) TN_CUDA_CHECK(cudaEventRecord(ctx->pev[1], st));
     MatvecFn mvm = [&](const double* x, double* y, const int* skip) {
         return heff_matvec_mixed(*ctx, msite, x, y, skip);
     };
@@ -575,6 +580,11 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
         key = hash_val(key, b->p);
     LzResult rm{};
     TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel, key));
+    if (ctx->prof) {  // the solve ended with a host wait, so the events have completed
+        float a = 0;
+        cudaEventElapsedTime(&a, ctx->pev[0], ctx->pev[1]);
+        ctx->prof_ms[0] += a;
+    }
     matvecs += rm.matvecs;
     heff_flop += heff_flops(s) * rm.matvecs;
     if (opt.refine_tol <= 0 && opt.verbose < 3 && ctx->aux2) {
@@ -914,6 +924,9 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
     learned_steps = learned_stalls = 0;
     t_refine = t_gauge = t_env = t_bond = 0;
     n_refine = n_gauge = n_env = 0;
+    ctx->prof = opt.verbose >= 4;
+    for (double& v : ctx->prof_ms) v = 0;
+    ctx->prof_steps = ctx->prof_restarts = 0;
     TN_CUDA_CHECK(cudaEventRecord(ctx->ev_a, st));
     double dE = 0, dl = 0;
     for (int in = 0; in < nsweeps; ++in) {
@@ -931,6 +944,13 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
         std::printf("phase seconds: refine %.4f gauge %.4f env %.4f bond-values %.4f (matvecs %lld, fp64 %lld); "
                     "launches refine %llu gauge %llu env %llu\n",
                     t_refine, t_gauge, t_env, t_bond, matvecs, matvecs_fp64, n_refine, n_gauge, n_env);
+    if (ctx->prof) {
+        std::printf("refine device ms: split operator %.2f | restart set-up %.2f | Krylov steps %.2f | Ritz %.2f "
+                    "(%lld restarts, %lld steps)\n",
+                    ctx->prof_ms[0], ctx->prof_ms[1], ctx->prof_ms[2], ctx->prof_ms[3], ctx->prof_restarts,
+                    ctx->prof_steps);
+        ctx->prof = false;
+    }
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         double e = 0;

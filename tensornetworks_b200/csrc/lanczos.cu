@@ -10,6 +10,7 @@
 // reductions and a deterministic last-block final reduction.
 #include "lanczos.h"
 #include "tridiag.cuh"
+#include "pdl.cuh"
 
 #include <cmath>
 #include <cstddef>
@@ -45,6 +46,22 @@ __device__ void block_sum_chunk(double (&v)[KCHUNK], double* out, double* sh /* 
         }
     }
     __syncthreads();
+}
+
+// out[k] = sum over the nb blocks' partials partial[b * stride + k], k < nk, by
+// the whole block (every thread must call it): each thread adds its share of
+// the blocks in a fixed order, then a block reduction, so the result does not
+// depend on timing.  out is shared memory with room for nk rounded up to KCHUNK.
+__device__ void reduce_partials(const double* partial, int nb, int stride, int nk, double* out, double* sh) {
+    for (int k0 = 0; k0 < nk; k0 += KCHUNK) {
+        double v[KCHUNK] = {0};
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+#pragma unroll
+            for (int q = 0; q < KCHUNK; ++q)
+                if (k0 + q < nk) v[q] += __ldcg(partial + (long long)b * stride + k0 + q);
+        }
+        block_sum_chunk(v, out + k0, sh);
+    }
 }
 
 // ---- kernels ---------------------------------------------------------------
@@ -87,11 +104,12 @@ __global__ void lz_norm_kernel(const double* __restrict__ x, long long N, double
         last = (prev == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        double s = 0;
-        for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + b);
-        st->xnorm = sqrt(s);
-        st->counter = 0;
+    if (last) {
+        reduce_partials(partial, gridDim.x, 1, 1, res, sh);
+        if (threadIdx.x == 0) {
+            st->xnorm = sqrt(res[0]);
+            st->counter = 0;
+        }
     }
 }
 
@@ -116,6 +134,7 @@ __global__ void lz_scale_kernel(const double* x, double* v0, long long N, const 
 // h_k = V_k . w for k = 0..j  (partials per block, last block reduces).
 __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __restrict__ w, long long N,
                                double* partial, LzState* st) {
+    pdl_wait();
     if (st->done) return;
     __shared__ double sh[KCHUNK * 32];
     __shared__ double res[KCHUNK];
@@ -143,11 +162,9 @@ __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __res
     }
     __syncthreads();
     if (last) {
-        for (int k = threadIdx.x; k < nk; k += blockDim.x) {
-            double s = 0;
-            for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + (long long)b * LZ_MAXK + k);
-            st->h[k] = s;
-        }
+        __shared__ double hsum[LZ_MAXK + KCHUNK];
+        reduce_partials(partial, gridDim.x, LZ_MAXK, nk, hsum, sh);
+        for (int k = threadIdx.x; k < nk; k += blockDim.x) st->h[k] = hsum[k];
         if (threadIdx.x == 0) st->counter = 0;
     }
 }
@@ -159,6 +176,7 @@ __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __res
 // the basis limit is reached, so the loop always terminates.
 __global__ void lz_update_kernel(const double* __restrict__ V, double* __restrict__ w, long long N,
                                  double* partial, LzState* st, cudaGraphConditionalHandle cond) {
+    pdl_wait();
     if (st->done) {
         if (cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
         return;
@@ -202,13 +220,8 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
     }
     __syncthreads();
     if (!last) return;
-    __shared__ double h2s[LZ_MAXK + 1];
-    for (int k = threadIdx.x; k <= nk; k += blockDim.x) {
-        double s = 0;
-        for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + (long long)b * LZ_MAXK + k);
-        h2s[k] = s;
-    }
-    __syncthreads();
+    __shared__ double h2s[LZ_MAXK + KCHUNK];
+    reduce_partials(partial, gridDim.x, LZ_MAXK, nk + 1, h2s, sh);
     if (threadIdx.x == 0) {
         double ss = 0;
         for (int k = 0; k < nk; ++k) { st->h2[k] = h2s[k]; ss += h2s[k] * h2s[k]; }
@@ -252,6 +265,7 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
 // block advances the step index (the other blocks read only jn).
 __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N, LzState* st,
                                double* __restrict__ xcur) {
+    pdl_wait();
     if (st->done) return;
     __shared__ double hs[LZ_MAXK];
     __shared__ double inv;
@@ -347,15 +361,14 @@ __global__ void rq_dots_kernel(const double* __restrict__ x, const double* __res
         last = (prev == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        double xy = 0, xx = 0;
-        for (int b = 0; b < (int)gridDim.x; ++b) {
-            xy += __ldcg(partial + 2 * b);
-            xx += __ldcg(partial + 2 * b + 1);
+    if (last) {
+        reduce_partials(partial, gridDim.x, 2, 2, res, sh);
+        if (threadIdx.x == 0) {
+            const double xy = res[0], xx = res[1];
+            st->theta = xx > 0 ? xy / xx : 0.0;
+            st->xnorm = sqrt(xx);
+            st->counter = 0;
         }
-        st->theta = xx > 0 ? xy / xx : 0.0;
-        st->xnorm = sqrt(xx);
-        st->counter = 0;
     }
 }
 
@@ -378,11 +391,12 @@ __global__ void rq_resid_kernel(const double* __restrict__ x, const double* __re
         last = (prev == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        double s = 0;
-        for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(partial + b);
-        st->resid = st->xnorm > 0 ? sqrt(s) / st->xnorm : 0.0;
-        st->counter = 0;
+    if (last) {
+        reduce_partials(partial, gridDim.x, 1, 1, res, sh);
+        if (threadIdx.x == 0) {
+            st->resid = st->xnorm > 0 ? sqrt(res[0]) / st->xnorm : 0.0;
+            st->counter = 0;
+        }
     }
 }
 
@@ -420,12 +434,9 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
     // one Lanczos step; cond != 0 inside the graph body
     auto enqueue_step = [&](cudaGraphConditionalHandle cond) -> int {
         TN_CHECK(mv(xcur, w, &s->done));
-        lz_dots_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, partial, s);
-        TN_LAUNCH_CHECK();
-        lz_update_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, partial, s, cond);
-        TN_LAUNCH_CHECK();
-        lz_next_kernel<<<grid, LZ_THREADS, 0, st>>>(V, w, N, s, xcur);
-        TN_LAUNCH_CHECK();
+        TN_CHECK(launch_pdl(lz_dots_kernel, grid, LZ_THREADS, 0, st, (const double*)V, (const double*)w, N, partial, s));
+        TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, st, (const double*)V, w, N, partial, s, cond));
+        TN_CHECK(launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, st, V, (const double*)w, N, s, xcur));
         return TN_OK;
     };
 
@@ -478,24 +489,40 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
     int restarts = 0;
     bool converged = false;
     double prev_resid = 1e300;
+    if (c.prof) TN_CHECK(c.prof_events());
     for (restarts = 0; restarts < (maxRestarts > 0 ? maxRestarts : 1); ++restarts) {
+        if (c.prof) TN_CUDA_CHECK(cudaEventRecord(c.pev[2], st));
         lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, restarts == 0, mm);
         TN_LAUNCH_CHECK();
         lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
         TN_LAUNCH_CHECK();
         lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, V, N, s, 1, xcur);
         TN_LAUNCH_CHECK();
+        if (c.prof) TN_CUDA_CHECK(cudaEventRecord(c.pev[3], st));
         if (gr) {
             TN_CUDA_CHECK(cudaGraphLaunch(gr->exec, st));
         } else {
             for (int j = 0; j < mm; ++j) TN_CHECK(enqueue_step(0));
         }
+        if (c.prof) TN_CUDA_CHECK(cudaEventRecord(c.pev[4], st));
         lz_ritz_coeffs_kernel<<<1, LZ_THREADS, 0, st>>>(s);
         TN_LAUNCH_CHECK();
         lz_ritz_vector_kernel<<<grid, LZ_THREADS, 0, st>>>(V, x, N, s);
         TN_LAUNCH_CHECK();
+        if (c.prof) TN_CUDA_CHECK(cudaEventRecord(c.pev[5], st));
         TN_CUDA_CHECK(cudaMemcpyAsync(hs, s, sizeof(LzState), cudaMemcpyDeviceToHost, st));
         TN_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (c.prof) {
+            float a = 0, b = 0, d = 0;
+            cudaEventElapsedTime(&a, c.pev[2], c.pev[3]);
+            cudaEventElapsedTime(&b, c.pev[3], c.pev[4]);
+            cudaEventElapsedTime(&d, c.pev[4], c.pev[5]);
+            c.prof_ms[1] += a;
+            c.prof_ms[2] += b;
+            c.prof_ms[3] += d;
+            c.prof_steps += hs->nb;
+            c.prof_restarts += 1;
+        }
         if (gr)  // kernels the graph ran: one body per step taken
             for (int k = 0; k < hs->nb; ++k)
                 for (unsigned long long q = 0; q < gr->kernels_per_iter; ++q) count_launch();

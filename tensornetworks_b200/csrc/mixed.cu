@@ -18,6 +18,7 @@
 #include <algorithm>
 
 #include "mixed.h"
+#include "pdl.cuh"
 
 namespace tnb {
 
@@ -75,6 +76,7 @@ __global__ void split_env_left_kernel(const double* __restrict__ F, int Dw, int 
 
 __global__ void split_vec_kernel(const double* __restrict__ x, long long n, uint16_t* __restrict__ out, int ns,
                                  long long pstride, const int* skip) {
+    pdl_wait();
     if (skip && *skip) return;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         split_bf16((float)x[e], ns, out, pstride, e);
@@ -84,6 +86,7 @@ __global__ void split_vec_kernel(const double* __restrict__ x, long long n, uint
 __global__ void wcombine_split_kernel(const float* __restrict__ P, uint16_t* __restrict__ qout, int ns,
                                       long long pstride, const WTermDev* __restrict__ terms, int nterms,
                                       int D1, int D2, int Dwout, const int* skip) {
+    pdl_wait();
     if (skip && *skip) return;
     const long long blk = (long long)D1 * D2;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < blk;
@@ -108,6 +111,7 @@ __global__ void wcombine_split_kernel(const float* __restrict__ P, uint16_t* __r
 // y[m][e] = sum_w2 Yp[(m*Dw2 + w2)][e]   (FP32 partials -> FP64 site layout)
 __global__ void reduce_w2_kernel(const float* __restrict__ Yp, int d, int Dw2, long long blk, double* __restrict__ y,
                                  const int* skip) {
+    pdl_wait();
     if (skip && *skip) return;
     const long long total = (long long)d * blk;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
@@ -197,19 +201,19 @@ int heff_matvec_mixed(Ctx& c, MixedSite& ms, const double* x, double* y, const i
     const ContractShape& s = ms.shape;
     const long long blk = (long long)s.D1 * s.D2;
     const long long nX = (long long)s.d * blk;
-    split_vec_kernel<<<g1d(nX), 256, 0, st>>>(x, nX, ms.Xs.as<uint16_t>(), ms.nsplit, (long long)ms.nX, skip);
-    TN_LAUNCH_CHECK();
+    TN_CHECK(launch_pdl(split_vec_kernel, g1d(nX), 256, 0, st, x, nX, ms.Xs.as<uint16_t>(), ms.nsplit,
+                        (long long)ms.nX, skip));
     TcGemmPlan p1 = ms.plan1;
     p1.args.skip = skip;
     TN_CHECK(tc_gemm_run(p1, st));
-    wcombine_split_kernel<<<g1d(blk), 256, 0, st>>>(ms.P32.as<float>(), ms.Qs.as<uint16_t>(), ms.nsplit,
-                                                     (long long)ms.nQ, ms.termsLR, ms.nLR, s.D1, s.D2, s.Dw2, skip);
-    TN_LAUNCH_CHECK();
+    TN_CHECK(launch_pdl(wcombine_split_kernel, g1d(blk), 256, 0, st, (const float*)ms.P32.as<float>(),
+                        ms.Qs.as<uint16_t>(), ms.nsplit, (long long)ms.nQ, (const WTermDev*)ms.termsLR, ms.nLR, s.D1,
+                        s.D2, s.Dw2, skip));
     TcGemmPlan p3 = ms.plan3;
     p3.args.skip = skip;
     TN_CHECK(tc_gemm_run(p3, st));
-    reduce_w2_kernel<<<g1d(nX), 256, 0, st>>>(ms.P32.as<float>(), s.d, s.Dw2, blk, y, skip);
-    TN_LAUNCH_CHECK();
+    TN_CHECK(launch_pdl(reduce_w2_kernel, g1d(nX), 256, 0, st, (const float*)ms.P32.as<float>(), s.d, s.Dw2, blk, y,
+                        skip));
     return TN_OK;
 }
 

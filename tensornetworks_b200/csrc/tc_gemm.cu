@@ -17,6 +17,7 @@
 #include <cstdint>
 
 #include "tc_gemm.h"
+#include "pdl.cuh"
 
 namespace tnb {
 
@@ -129,6 +130,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     __shared__ uint32_t tmem_base_sh;
     __shared__ int s_fail;
 
+    pdl_wait();
     if (p.skip && *p.skip) return;
 
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -329,9 +331,7 @@ static int launch_tc(const TcGemmPlan& pl, cudaStream_t st) {
     dim3 grid((p.N + BN - 1) / BN, (p.M + BM - 1) / BM, p.batch);
     const int smem = SmemLayout<BN, NS>::TOTAL;
     TN_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_bf16x3_kernel<BN, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    tc_gemm_bf16x3_kernel<BN, NS><<<grid, THREADS, smem, st>>>(pl.maps, p);
-    TN_LAUNCH_CHECK();
-    return TN_OK;
+    return launch_pdl(tc_gemm_bf16x3_kernel<BN, NS>, grid, dim3(THREADS), (size_t)smem, st, pl.maps, p);
 }
 
 int tc_gemm_run(const TcGemmPlan& pl, cudaStream_t st) {

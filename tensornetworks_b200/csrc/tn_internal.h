@@ -142,6 +142,14 @@ struct Ctx {
     // second side stream: the FP64 check of a site's eigenvector, overlapping the gauge move
     cudaStream_t aux2 = nullptr;
     cudaEvent_t ev_y[2] = {nullptr, nullptr};
+    // refine sub-phase timing (solver verbose >= 4): device milliseconds in
+    // [0] split-operator preparation, [1] restart set-up, [2] Krylov steps,
+    // [3] Ritz vector; events pev, created on first use
+    bool prof = false;
+    cudaEvent_t pev[6] = {};
+    double prof_ms[4] = {};
+    long long prof_steps = 0, prof_restarts = 0;
+    int prof_events();
     // scratch
     DevBuf P, Q;           // contraction intermediates
     DevBuf lz;             // Lanczos basis + work vectors
