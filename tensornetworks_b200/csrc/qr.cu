@@ -383,6 +383,7 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
     const int mp = m - j0;
     const int ls = mp + 1;
     constexpr int RT = (32 + 8 * RR + 255) / 256;  // rows of a column per thread in the copies
+    for (int e = tid; e < B * (B + 1); e += 256) (&Gs[0][0])[e] = 0.0;  // entries past b stay zero
 #pragma unroll 4
     for (int c = 0; c < b; ++c) {
 #pragma unroll
@@ -527,24 +528,55 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
             }
         }
     }
-    // dlarft (forward, columnwise), lane i of warp 0 builds row i of T
-    if (w == 0) {
-        const int i = lane;
-        double trow[B];
+    // T (dlarft, forward, columnwise) blockwise.  For reflectors split into two
+    // groups, I - V T V^T = (I - V1 T11 V1^T)(I - V2 T22 V2^T) gives
+    // T = [T11, -T11 (V1^T V2) T22; 0, T22]: the four 8 x 8 diagonal blocks by
+    // the recurrence T(i, jj) = -tau_jj sum_{l=i}^{jj-1} T(i, l) G(l, jj) (one
+    // warp each, lane i builds row i), then the off-diagonal blocks at widths 8
+    // and 16 as small products over the whole block.  Columns past b have
+    // tau = 0 and zero Gram entries, so they come out zero.
+    __shared__ double Tsm[B][B + 1];  // Tsm[i][jj] = T(i, jj)
+    __shared__ double Xs[B][B + 1];
+    for (int e = tid; e < B * (B + 1); e += 256) (&Tsm[0][0])[e] = 0.0;
+    __syncthreads();
+    if (w < 4 && lane < 8) {
+        const int q0 = 8 * w, i = lane;
+        double trow[8];
 #pragma unroll
-        for (int jj = 0; jj < B; ++jj) {
-            double a0 = 0, a1 = 0;
+        for (int jj = 0; jj < 8; ++jj) {
+            double a = 0;
 #pragma unroll
-            for (int l = 0; l < jj; ++l) {
-                const double term = (l >= i) ? trow[l] * Gs[l][jj] : 0.0;
-                if (l & 1) a1 += term; else a0 += term;
-            }
-            const double tj = jj < b ? taus[jj] : 0.0;
-            trow[jj] = (jj < i) ? 0.0 : (jj == i ? tj : -tj * (a0 + a1));
+            for (int l = 0; l < jj; ++l)
+                if (l >= i) a = fma(trow[l], Gs[q0 + l][q0 + jj], a);
+            const double tj = q0 + jj < b ? taus[q0 + jj] : 0.0;
+            trow[jj] = (jj < i) ? 0.0 : (jj == i ? tj : -tj * a);
         }
 #pragma unroll
-        for (int jj = 0; jj < B; ++jj)
-            if (i < b && jj < b) T[(size_t)jj * ldt + i] = trow[jj];
+        for (int jj = 0; jj < 8; ++jj) Tsm[q0 + i][q0 + jj] = trow[jj];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 8; h < B; h *= 2) {
+        // pairs of h x h blocks at r0 = 0, 2h, ...: X = G12 T22, then T12 = -T11 X
+        const int npair = B / (2 * h);
+        for (int e = tid; e < npair * h * h; e += 256) {
+            const int pr = e / (h * h), a = (e / h) % h, c = e % h, r0 = 2 * h * pr;
+            double x = 0;
+            for (int k = 0; k <= c; ++k) x = fma(Gs[r0 + a][r0 + h + k], Tsm[r0 + h + k][r0 + h + c], x);
+            Xs[r0 + a][r0 + h + c] = x;
+        }
+        __syncthreads();
+        for (int e = tid; e < npair * h * h; e += 256) {
+            const int pr = e / (h * h), a = (e / h) % h, c = e % h, r0 = 2 * h * pr;
+            double t = 0;
+            for (int k = a; k < h; ++k) t = fma(Tsm[r0 + a][r0 + k], Xs[r0 + k][r0 + h + c], t);
+            Tsm[r0 + a][r0 + h + c] = -t;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < b * b; e += 256) {
+        const int i = e % b, jj = e / b;
+        T[(size_t)jj * ldt + i] = Tsm[i][jj];
     }
 }
 
@@ -604,6 +636,7 @@ __global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __re
     double* Cs = Vs + (size_t)ld * B;  // WY_COLS columns of length ld
     __shared__ double Zp[NPART][B][WY_COLS];
     __shared__ double Z2[B][WY_COLS];
+    __shared__ double Ts[B][B + 1];  // Ts[c][r] = T(r, c)
     const int tid = threadIdx.x;
     // blocks past the first target's columns work on the second target (same V, T)
     int blk = blockIdx.x;
@@ -625,6 +658,11 @@ __global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __re
         const int r = e % mp, col = e / mp;
         if (col < ncol) cp_async8(Cs + (size_t)col * ld + r, C + (size_t)(c0 + col) * ldc + r);
         else Cs[(size_t)col * ld + r] = 0.0;
+    }
+    for (int e = tid; e < B * B; e += WY_THREADS) {
+        const int r = e % B, col = e / B;
+        if (r < b && col < b) cp_async8(&Ts[col][r], T + (size_t)col * ldt + r);
+        else Ts[col][r] = 0.0;
     }
     cp_async_wait_all();
     __syncthreads();
@@ -653,14 +691,14 @@ __global__ void __launch_bounds__(WY_THREADS) wy_apply_kernel(const double* __re
                     double z = 0;
 #pragma unroll
                     for (int pp = 0; pp < NPART; ++pp) z += Zp[pp][l][cc];
-                    s = fma(T[(size_t)bb * ldt + l], z, s);
+                    s = fma(Ts[bb][l], z, s);
                 }
             } else {
                 for (int l = bb; l < b; ++l) {
                     double z = 0;
 #pragma unroll
                     for (int pp = 0; pp < NPART; ++pp) z += Zp[pp][l][cc];
-                    s = fma(T[(size_t)l * ldt + bb], z, s);
+                    s = fma(Ts[l][bb], z, s);
                 }
             }
         }
@@ -699,6 +737,7 @@ __global__ void __cluster_dims__(1, WYN_RANKS, 1) __launch_bounds__(256)
     __shared__ double Zp[B][NC];  // this CTA's partial V^T C
     __shared__ double Zs[B][NC];
     __shared__ double Z2[B][NC];
+    __shared__ double Ts[B][B + 1];  // Ts[c][r] = T(r, c)
     namespace cgx = cooperative_groups;
     cgx::cluster_group cluster = cgx::this_cluster();
     const int rank = (int)cluster.block_rank();
@@ -718,6 +757,11 @@ __global__ void __cluster_dims__(1, WYN_RANKS, 1) __launch_bounds__(256)
         const int r = e % nr, col = e / nr;
         if (col < ncol) cp_async8(Cs + (size_t)col * ld + r, C + (size_t)(c0 + col) * ldc + r0 + r);
         else Cs[(size_t)col * ld + r] = 0.0;
+    }
+    for (int e = tid; e < B * B; e += 256) {
+        const int r = e % B, col = e / B;
+        if (r < b && col < b) cp_async8(&Ts[col][r], T + (size_t)col * ldt + r);
+        else Ts[col][r] = 0.0;
     }
     cp_async_wait_all();
     __syncthreads();
@@ -749,7 +793,7 @@ __global__ void __cluster_dims__(1, WYN_RANKS, 1) __launch_bounds__(256)
         const int bb = tid % B, q = tid / B;
         double s = 0;
         if (bb < b)
-            for (int l = 0; l <= bb; ++l) s = fma(T[(size_t)bb * ldt + l], Zs[l][q], s);
+            for (int l = 0; l <= bb; ++l) s = fma(Ts[bb][l], Zs[l][q], s);
         Z2[bb][q] = s;
     }
     __syncthreads();
