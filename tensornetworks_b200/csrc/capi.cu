@@ -157,6 +157,7 @@ int tn_ctx_create(int device, tn_ctx* out) {
     c->c.device = device;
     c->c.sm_count = prop.multiProcessorCount;
     if (const char* ng = std::getenv("TN_NO_GRAPHS")) c->c.use_graphs = !(ng[0] == '1');
+    if (const char* np = std::getenv("TN_NO_PERSISTENT_QR")) c->c.use_persistent_qr = !(np[0] == '1');
     TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.own_stream, cudaStreamNonBlocking));
     c->c.stream = c->c.own_stream;
     TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.aux, cudaStreamNonBlocking));
@@ -689,7 +690,7 @@ int tn_qr(tn_ctx c, int m, int n, const double* A, int lda, double* Q, int ldq, 
     TN_CHECK(copy2d(m, n, A, idx(1), idx(lda), W.as<double>(), idx(1), idx(m), 1.0, cx.stream));
     TN_CHECK(qr_dense(cx, m, n, W.as<double>(), Q, ldq, R, ldr));
     TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
-    return TN_OK;
+    return check_device_error(cx);
 }
 
 int tn_lq(tn_ctx c, int m, int n, const double* A, int lda, double* L, int ldl, double* Q, int ldq) {
@@ -707,7 +708,7 @@ int tn_lq(tn_ctx c, int m, int n, const double* A, int lda, double* L, int ldl, 
     TN_CHECK(copy2d(k, m, Rt.as<double>(), idx(1), idx(k), L, idx(ldl), idx(1), 1.0, cx.stream));
     TN_CHECK(copy2d(n, k, Qt.as<double>(), idx(1), idx(n), Q, idx(ldq), idx(1), 1.0, cx.stream));
     TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
-    return TN_OK;
+    return check_device_error(cx);
 }
 
 // SVCompressorImp<T>::Compress (SVCompressorImp.C:19-73) on a device s vector.

@@ -842,7 +842,8 @@ int MPSState::sweep(bool left, double epsEigen) {
                             1e6 * secs(t2, t3), launch_count() - n2);
         }
     }
-    return rq_collect();
+    TN_CHECK(rq_collect());
+    return check_device_error(*ctx);
 }
 
 // MPSImp::IncreaseBondDimensions (MPSImp.C:123-147) with Bond::NewBondDimension (Bond.C:60-84).

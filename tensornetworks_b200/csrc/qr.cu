@@ -366,24 +366,42 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // partial sums are double-buffered by step parity in shared memory, which is
 // what lets one barrier per step suffice.  The panel moves between global and
 // shared memory with coalesced copies.  Reflectors follow dlarfg as above.
+// Shared memory of the column-group panel (one instance per kernel, whichever
+// row capacity RR the panel uses).
+struct PanelSmem {
+    double part[2][8][32];     // per-warp column sums
+    double2 vb[2][8][8][4];    // each warp's rows of u_j, row pairs by row group (RL / 2 <= 8)
+    double rowj[2][32];        // row j of every column
+    double Gs[32][33];         // Gs[l][jj] = v_l^T v_jj, l < jj
+    double taus[32], scals[32], betas[32];
+    double Tsm[32][33];        // T(i, jj)
+    double Xs[32][33];         // products of the blocked T build
+};
+
 template <int RR>
-__global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
-                                                           double* __restrict__ V, int ldv,
-                                                           double* __restrict__ T, int ldt) {
+__device__ __forceinline__ void panel_col(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                          double* __restrict__ V, int ldv, double* __restrict__ T, int ldt,
+                                          double* stage, PanelSmem& sm) {
     constexpr int B = 32, NW = 8, RB = RR / 4, RL = RB + 1;
-    static_assert(RR % 4 == 0 && RL % 2 == 0, "bulk rows per lane must be odd");
-    extern __shared__ double stage[];               // the panel, column-major, ld mp + 1
-    __shared__ double part[2][NW][B];               // per-warp column sums
-    __shared__ double2 vb[2][NW][RL / 2][4];        // each warp's rows of u_j, row pairs by row group
-    __shared__ double rowj[2][B];                   // row j of every column
-    __shared__ double Gs[B][B + 1];                 // Gs[l][jj] = v_l^T v_jj, l < jj
-    __shared__ double taus[B], scals[B], betas[B];
+    static_assert(RR % 4 == 0 && RL % 2 == 0 && RL / 2 <= 8, "bulk rows per lane must be odd, at most 15");
+    auto& part = sm.part;
+    auto& vb = sm.vb;
+    auto& rowj = sm.rowj;
+    auto& Gs = sm.Gs;
+    auto& taus = sm.taus;
+    auto& scals = sm.scals;
+    auto& betas = sm.betas;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int rg = lane & 3, cg = lane >> 2;
     const int mp = m - j0;
     const int ls = mp + 1;
     constexpr int RT = (32 + 8 * RR + 255) / 256;  // rows of a column per thread in the copies
     for (int e = tid; e < B * (B + 1); e += 256) (&Gs[0][0])[e] = 0.0;  // entries past b stay zero
+    // Asynchronous copies through L1 (all in flight at once).  In the persistent QR
+    // other CTAs write these columns during the same launch; this SM's L1 can
+    // hold no stale line of them, since it only ever cached panels already
+    // factored plus the first <= 15 rows of the column after a panel, and rows
+    // above the diagonal of a later panel are never staged.
 #pragma unroll 4
     for (int c = 0; c < b; ++c) {
 #pragma unroll
@@ -535,8 +553,8 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
     // warp each, lane i builds row i), then the off-diagonal blocks at widths 8
     // and 16 as small products over the whole block.  Columns past b have
     // tau = 0 and zero Gram entries, so they come out zero.
-    __shared__ double Tsm[B][B + 1];  // Tsm[i][jj] = T(i, jj)
-    __shared__ double Xs[B][B + 1];
+    auto& Tsm = sm.Tsm;  // Tsm[i][jj] = T(i, jj)
+    auto& Xs = sm.Xs;
     for (int e = tid; e < B * (B + 1); e += 256) (&Tsm[0][0])[e] = 0.0;
     __syncthreads();
     if (w < 4 && lane < 8) {
@@ -578,6 +596,15 @@ __global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ 
         const int i = e % b, jj = e / b;
         T[(size_t)jj * ldt + i] = Tsm[i][jj];
     }
+}
+
+template <int RR>
+__global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                                           double* __restrict__ V, int ldv,
+                                                           double* __restrict__ T, int ldt) {
+    extern __shared__ double stage[];  // the panel, column-major, ld mp + 1
+    __shared__ PanelSmem sm;
+    panel_col<RR>(W, ldw, m, j0, b, V, ldv, T, ldt, stage, sm);
 }
 
 // Panel launch: the column-per-lane kernel for 32-wide panels, the row-per-thread
@@ -818,6 +845,250 @@ inline size_t wyn_smem_bytes(int mp, int B) {
     return sizeof(double) * (size_t)(rb + 1) * (B + WY_COLS);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent blocked QR (m <= 512, 32-wide panels): one cooperative launch.
+// CTA 0 factors the panels in order; every other CTA takes trailing-update
+// tasks -- one 2-column block of W or 8-column block of Qt (= Q^T,
+// accumulated as in the look-ahead path) under one block reflector -- from a
+// global counter, in the
+// order reflector by reflector and, within a reflector, W's blocks from the left
+// (so the next panel's columns come first), then Qt's.  Progress is tracked in
+// global memory: refready = panels factored, applied[block] = reflectors
+// applied to that block.  A task for reflector kk waits for refready > kk and
+// applied == kk; panel kk waits for applied >= kk on its own blocks.  The
+// other tasks of reflector kk also wait until its tasks on panel kk+1's
+// columns (the critical ones) have finished, so that those stage their data
+// without competition (word [3] counts finished critical tasks).  Tasks
+// only wait on earlier tasks and on panels, and every CTA is resident
+// (cooperative launch), so the waits end; each is bounded all the same
+// (spin_limit polls): on expiry it raises the error word, and every wait gives
+// up once the error word is set.  Data written by other CTAs within the launch
+// is read with L2 loads (ld.global.cg), never through L1.
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// true once *flag >= target; false if the error word is set or the poll limit runs out
+__device__ bool wait_geq(const int* flag, int target, const int* err, long long limit) {
+    for (long long it = 0; it < limit; ++it) {
+        if (ld_acquire(flag) >= target) return true;
+        if (ld_acquire(err)) return false;
+        if (it > 32) __nanosleep(128);
+    }
+    return false;
+}
+
+struct WySmem {
+    double Zp[256];     // partial V^T C, [part][l][q]
+    double Z2[32][8];
+    double Ts[32][33];  // Ts[c][r] = T(r, c)
+};
+
+// C (mp x ncol, ncol <= NC, ld ldc) <- (I - V T^T V^T) C for one 32-wide block
+// reflector (V unit lower trapezoidal, read below the diagonal only; T upper),
+// staged in shared memory.  V is a factored panel, final before any task reads
+// it, so it comes by asynchronous copies through L1 (all in flight at once);
+// C and T, rewritten by other CTAs during the launch, come by L2 loads
+// (ld.global.cg), which never allocate in L1.  The 32 x NC dots of Z = V^T C
+// are split over 256 / (32 NC) row partitions.  All 256 threads call it.
+template <int NC>
+__device__ void wy_task(const double* __restrict__ V, int ldv, const double* __restrict__ T, int ldt, int b,
+                        double* __restrict__ C, int ldc, int mp, int ncol, double* dyn, WySmem& ws) {
+    constexpr int B = 32, RT = 2, NPART = 256 / (B * NC);  // mp <= 512 rows: two per thread
+    static_assert(NPART * B * NC == 256, "one thread per (partition, l, q)");
+    const int ld = mp + 1, tid = threadIdx.x;
+    double* Vs = dyn;
+    double* Cs = Vs + (size_t)ld * B;
+#pragma unroll 8
+    for (int col = 0; col < B; ++col) {
+#pragma unroll
+        for (int h = 0; h < RT; ++h) {
+            const int r = tid + 256 * h;
+            if (r < mp) {
+                if (col < b && r > col) cp_async8(Vs + (size_t)col * ld + r, V + (size_t)col * ldv + r);
+                else Vs[(size_t)col * ld + r] = (col < b && r == col) ? 1.0 : 0.0;
+            }
+        }
+    }
+#pragma unroll
+    for (int col = 0; col < NC; ++col) {
+#pragma unroll
+        for (int h = 0; h < RT; ++h) {
+            const int r = tid + 256 * h;
+            if (r < mp) Cs[(size_t)col * ld + r] = col < ncol ? __ldcg(C + (size_t)col * ldc + r) : 0.0;
+        }
+    }
+    for (int e = tid; e < B * B; e += 256) {
+        const int r = e & (B - 1), col = e / B;
+        ws.Ts[col][r] = (r < b && col < b) ? __ldcg(T + (size_t)col * ldt + r) : 0.0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    {
+        const int l = tid % B, q = (tid / B) % NC, part = tid / (B * NC);
+        const double* vcol = Vs + (size_t)l * ld;
+        const double* ccol = Cs + (size_t)q * ld;
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        int r = part;
+        for (; r + 3 * NPART < mp; r += 4 * NPART) {
+            a0 = fma(vcol[r], ccol[r], a0);
+            a1 = fma(vcol[r + NPART], ccol[r + NPART], a1);
+            a2 = fma(vcol[r + 2 * NPART], ccol[r + 2 * NPART], a2);
+            a3 = fma(vcol[r + 3 * NPART], ccol[r + 3 * NPART], a3);
+        }
+        for (; r < mp; r += NPART) a0 = fma(vcol[r], ccol[r], a0);
+        ws.Zp[(part * B + l) * NC + q] = (a0 + a1) + (a2 + a3);
+    }
+    __syncthreads();
+    if (tid < B * NC) {
+        const int bb = tid % B, q = tid / B;
+        double s = 0;
+        if (bb < b)
+            for (int l = 0; l <= bb; ++l) {
+                double z = 0;
+#pragma unroll
+                for (int pp = 0; pp < NPART; ++pp) z += ws.Zp[(pp * B + l) * NC + q];
+                s = fma(ws.Ts[bb][l], z, s);
+            }
+        ws.Z2[bb][q] = s;
+    }
+    __syncthreads();
+    for (int r = tid; r < mp; r += 256) {
+        double acc[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) acc[q] = Cs[(size_t)q * ld + r];
+#pragma unroll 4
+        for (int l = 0; l < B; ++l) {
+            const double vl = Vs[(size_t)l * ld + r];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) acc[q] = fma(-vl, ws.Z2[l][q], acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (q < ncol) C[(size_t)q * ldc + r] = acc[q];
+    }
+    __syncthreads();
+}
+
+inline size_t qrp_smem_bytes(int m) { return sizeof(double) * (size_t)(m + 1) * 40 + sizeof(WySmem); }
+
+// sync words: [0] refready, [1] task counter, [2] error, [3] finished tasks on
+// the column blocks of the panel after their reflector's, [4 ..] applied counts of
+// W's 2-column blocks, then of Qt's 8-column blocks (zeroed before the launch);
+// *derr is a sticky error word of the context.
+constexpr int QRP_MAXM = 512;
+constexpr int QRP_WB = 2;  // columns of W per task (the next panel's 32 columns make 16 tasks)
+constexpr int QRP_QB = 8;  // columns of Qt per task
+constexpr int QRP_UNAVAILABLE = -1;  // the persistent QR cannot be launched: take the look-ahead path
+__global__ void __launch_bounds__(256, 1)
+    qr_persistent_kernel(double* __restrict__ W, int m, int n, int k, double* __restrict__ Tall,
+                         double* __restrict__ Qt, int* __restrict__ sync, int* __restrict__ derr,
+                         long long spin_limit) {
+    extern __shared__ double dyn[];  // panel stage or the workers' V and C blocks, then their WySmem
+    __shared__ PanelSmem ps;
+    __shared__ int task_sh, ok_sh;
+    WySmem& ws = *reinterpret_cast<WySmem*>(dyn + (size_t)(m + 1) * 40);
+    const int K = (k + 31) / 32;
+    int* refready = sync;
+    int* next_task = sync + 1;
+    int* err = sync + 2;
+    int* crit_done = sync + 3;
+    int* applied_w = sync + 4;
+    int* applied_q = applied_w + (n + QRP_WB - 1) / QRP_WB;
+    // tasks of reflector kk on panel kk+1's column blocks (before kk: crit_before)
+    auto crit_tasks = [&](int kk) {
+        const int start = 32 * (kk + 1);
+        if (start >= k) return 0;
+        const int end = min(start + 32, k);  // panel kk+1's columns
+        return (end - 1) / QRP_WB - start / QRP_WB + 1;
+    };
+    if (blockIdx.x == 0) {
+        for (int kk = 0; kk < K; ++kk) {
+            const int j0 = 32 * kk, b = min(32, k - j0), mp = m - j0;
+            if (kk > 0) {
+                if (threadIdx.x == 0) ok_sh = 1;
+                __syncthreads();
+                if (threadIdx.x < 32 / QRP_WB) {
+                    const int cb = j0 / QRP_WB + (int)threadIdx.x;
+                    if (QRP_WB * cb < j0 + b && !wait_geq(applied_w + cb, kk, err, spin_limit)) {
+                        atomicExch(err, 1);
+                        atomicExch(derr, 1);
+                        ok_sh = 0;
+                    }
+                }
+                __syncthreads();
+                if (!ok_sh) return;  // the same decision in every thread
+                __threadfence();
+            }
+            double* Tk = Tall + (size_t)j0 * 32;
+            if (mp <= 64) panel_col<4>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
+            else if (mp <= 128) panel_col<12>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
+            else if (mp <= 256) panel_col<28>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
+            else panel_col<60>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                st_release(refready, kk + 1);
+            }
+        }
+        return;
+    }
+    const int nqb = Qt ? (m + QRP_QB - 1) / QRP_QB : 0;
+    for (;;) {
+        if (threadIdx.x == 0) task_sh = atomicAdd(next_task, 1);
+        __syncthreads();
+        int t = task_sh;
+        int kk = 0, kind = -1, blk = 0;
+        for (; kk < K; ++kk) {
+            const int start = min(32 * (kk + 1), k);  // first column after panel kk
+            const int nwb = n > start ? (n - 1) / QRP_WB - start / QRP_WB + 1 : 0;
+            if (t < nwb) { kind = 0; blk = start / QRP_WB + t; break; }
+            t -= nwb;
+            if (t < nqb) { kind = 1; blk = t; break; }
+            t -= nqb;
+        }
+        if (kind < 0) return;
+        const int j0 = 32 * kk, b = min(32, k - j0), mp = m - j0;
+        int* flag = kind == 0 ? applied_w + blk : applied_q + blk;
+        const int ncrit = crit_tasks(kk);
+        const bool critical = kind == 0 && QRP_WB * blk < min(j0 + b + 32, k);
+        int crit_target = 0;  // critical tasks of reflectors 0 .. kk
+        if (!critical && ncrit > 0)
+            for (int q = 0; q <= kk; ++q) crit_target += crit_tasks(q);
+        if (threadIdx.x == 0) {
+            bool ok = wait_geq(refready, kk + 1, err, spin_limit) && wait_geq(flag, kk, err, spin_limit);
+            if (ok && crit_target > 0) ok = wait_geq(crit_done, crit_target, err, spin_limit);
+            if (!ok) {
+                atomicExch(err, 1);
+                atomicExch(derr, 1);
+            }
+            ok_sh = ok;
+        }
+        __syncthreads();
+        if (!ok_sh) return;
+        __threadfence();
+        const double* V = W + (size_t)j0 * m + j0;
+        const double* Tk = Tall + (size_t)j0 * 32;
+        if (kind == 0) {
+            const int cs = max(QRP_WB * blk, j0 + b), ce = min(QRP_WB * blk + QRP_WB, n);
+            wy_task<QRP_WB>(V, m, Tk, 32, b, W + (size_t)cs * m + j0, m, mp, ce - cs, dyn, ws);
+        } else {
+            const int cs = QRP_QB * blk, ce = min(cs + QRP_QB, m);
+            wy_task<QRP_QB>(V, m, Tk, 32, b, Qt + (size_t)cs * m + j0, m, mp, ce - cs, dyn, ws);
+        }
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release(flag, kk + 1);
+            if (critical) atomicAdd(crit_done, 1);
+        }
+    }
+}
+
 __global__ void set_identity_kernel(double* Q, int m, int k, int ldq) {
     long long total = (long long)m * k;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
@@ -946,6 +1217,61 @@ int qr_lookahead(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
     return TN_OK;
 }
 
+// Host side of the persistent QR (32-wide panels, m <= 512, k > 32).  Returns
+// QRP_UNAVAILABLE (nothing enqueued) when the cooperative launch is impossible.
+int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr, double* Tall) {
+    cudaStream_t st = c.stream;
+    const int k = std::min(m, n);
+    static thread_local int attr_dev = -1, max_per_sm = 0;
+    int dev = 0;
+    TN_CUDA_CHECK(cudaGetDevice(&dev));
+    const size_t smem = qrp_smem_bytes(QRP_MAXM);
+    if (attr_dev != dev) {
+        TN_CUDA_CHECK(cudaFuncSetAttribute(qr_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        TN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_per_sm, qr_persistent_kernel, 256, smem));
+        attr_dev = dev;
+    }
+    const int nwb = (n + QRP_WB - 1) / QRP_WB, nqb = Qout ? (m + QRP_QB - 1) / QRP_QB : 0;
+    const int tasks = std::max(1, (n - 32 + QRP_WB - 1) / QRP_WB) + nqb;  // most tasks of one reflector
+    const int G = std::min(max_per_sm * c.sm_count, 1 + tasks);
+    if (G < 2) return QRP_UNAVAILABLE;
+    const size_t words = 4 + (size_t)nwb + (size_t)nqb;
+    TN_CHECK(c.qrsync.ensure(sizeof(int) * words));
+    if (!c.derr.p) {
+        TN_CHECK(c.derr.ensure(sizeof(int)));
+        TN_CUDA_CHECK(cudaMemset(c.derr.p, 0, sizeof(int)));
+    }
+    double* Qt = nullptr;
+    if (Qout) {
+        TN_CHECK(c.qaccum.ensure(sizeof(double) * (size_t)m * m));
+        Qt = c.qaccum.as<double>();
+        set_identity_kernel<<<g1d((long long)m * m), 256, 0, st>>>(Qt, m, m, m);
+        TN_LAUNCH_CHECK();
+    }
+    TN_CUDA_CHECK(cudaMemsetAsync(c.qrsync.p, 0, sizeof(int) * words, st));
+    int* sync = c.qrsync.as<int>();
+    int* derr = c.derr.as<int>();
+    long long spin_limit = 1LL << 21;
+    void* args[] = {&W, &m, &n, (void*)&k, &Tall, &Qt, &sync, &derr, &spin_limit};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr_persistent_kernel, dim3(G), dim3(256), args, smem, st);
+    if (e == cudaErrorCooperativeLaunchTooLarge) {
+        cudaGetLastError();
+        return QRP_UNAVAILABLE;
+    }
+    TN_CUDA_CHECK(e);
+    count_launch();
+    if (Rout) {
+        extract_r_kernel<<<g1d((long long)k * n), 256, 0, st>>>(W, m, k, n, Rout, ldr);
+        TN_LAUNCH_CHECK();
+    }
+    if (Qout) {
+        dim3 grid((m + 31) / 32, (k + 31) / 32);
+        transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(Qt, m, Qout, ldq, k, m);
+        TN_LAUNCH_CHECK();
+    }
+    return TN_OK;
+}
+
 template <int NT, int R, int B, int U>
 int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
     cudaStream_t st = c.stream;
@@ -966,6 +1292,10 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
     TN_CHECK(c.qrw.ensure(need));
     double* Vall = c.qrw.as<double>();
     double* Tall = Vall + (size_t)m * k;
+    if (B == 32 && k > B && m <= QRP_MAXM && c.use_persistent_qr) {
+        const int rc = qr_persistent(c, m, n, W, Qout, ldq, Rout, ldr, Tall);
+        if (rc != QRP_UNAVAILABLE) return rc;
+    }
     if (k > B && c.aux) return qr_lookahead<NT, R, B, U>(c, m, n, W, Qout, ldq, Rout, ldr, Vall, Tall);
     for (int j0 = 0; j0 < k; j0 += B) {
         const int b = std::min(B, k - j0);
@@ -1002,6 +1332,16 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
 }
 
 }  // namespace
+
+int check_device_error(Ctx& c) {
+    if (!c.derr.p) return TN_OK;
+    int h = 0;
+    TN_CUDA_CHECK(cudaMemcpy(&h, c.derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!h) return TN_OK;
+    TN_CUDA_CHECK(cudaMemset(c.derr.p, 0, sizeof(int)));
+    set_error("a bounded wait between the CTAs of the persistent QR expired");
+    return TN_CUDA_ERROR;
+}
 
 int qr_dense(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
     cudaStream_t st = c.stream;

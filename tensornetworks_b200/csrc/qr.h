@@ -8,6 +8,10 @@ namespace tnb {
 // Writes Q (m x k, ld ldq) and R (k x n, ld ldr) when the pointers are non-null.
 int qr_dense(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr);
 
+// Reads (and clears) the context's sticky device error word, raised when a
+// bounded wait between CTAs expired; waits for the device.
+int check_device_error(Ctx& c);
+
 // One job of the batched one-sided Jacobi SVD (one CTA per job).  W is the
 // tall (m >= n) working copy, overwritten.  With vectors: U (m x n, ldu),
 // Vt (n x n, ldvt) and a scratch V (n x n, ld n).  s (n) is always written.

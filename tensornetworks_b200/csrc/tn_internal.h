@@ -157,13 +157,16 @@ struct Ctx {
     DevBuf rq;             // Rayleigh-quotient state + partials
     DevBuf dv, dvstate;    // Davidson basis + work vectors, device state
     DevBuf qrw;            // QR workspace
-    DevBuf qaccum;         // QR: forward-accumulated Q and its two m x b temporaries
+    DevBuf qaccum;         // QR: forward-accumulated Q (transposed)
+    DevBuf qrsync;         // QR: progress words of the persistent kernel
+    DevBuf derr;           // sticky error word of kernels with bounded waits (zero until one expires)
     DevBuf svdw;           // SVD workspace
     DevBuf wterms;         // MPO term lists
     DevBuf misc;
     DevBuf apiw[3];        // staging copies of the dense-solver entry points
     HostBuf pinned;
     int sm_count = 148;
+    bool use_persistent_qr = true;  // TN_NO_PERSISTENT_QR=1: the two-stream look-ahead QR instead
     // cache of the last MPO term list uploaded through the C ABI
     std::vector<double> wcache_W;
     int wcache_key[4] = {0, 0, 0, 0};
