@@ -1251,7 +1251,7 @@ int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double
     TN_CUDA_CHECK(cudaMemsetAsync(c.qrsync.p, 0, sizeof(int) * words, st));
     int* sync = c.qrsync.as<int>();
     int* derr = c.derr.as<int>();
-    long long spin_limit = 1LL << 21;
+    long long spin_limit = c.qr_spin_limit;
     void* args[] = {&W, &m, &n, (void*)&k, &Tall, &Qt, &sync, &derr, &spin_limit};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr_persistent_kernel, dim3(G), dim3(256), args, smem, st);
     if (e == cudaErrorCooperativeLaunchTooLarge) {

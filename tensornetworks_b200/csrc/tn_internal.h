@@ -167,6 +167,7 @@ struct Ctx {
     HostBuf pinned;
     int sm_count = 148;
     bool use_persistent_qr = true;  // TN_NO_PERSISTENT_QR=1: the two-stream look-ahead QR instead
+    long long qr_spin_limit = 1LL << 21;  // polls per wait in the persistent QR (TN_QR_SPIN_LIMIT)
     // cache of the last MPO term list uploaded through the C ABI
     std::vector<double> wcache_W;
     int wcache_key[4] = {0, 0, 0, 0};
