@@ -155,7 +155,19 @@ int Hamiltonian::build() {
     }
     std::vector<WTermDev> all;
     std::vector<double> allW;
+    std::vector<const SiteMPO*> done;
     auto add = [&](SiteMPO& op) {
+        // sites with the same W share one copy of its term lists, so that the
+        // device graphs recorded for one of them (keyed by the term pointer)
+        // serve every site of the same shape
+        for (const SiteMPO* q : done)
+            if (q->Dw1 == op.Dw1 && q->Dw2 == op.Dw2 && q->W == op.W) {
+                op.offLR = q->offLR; op.nLR = q->nLR;
+                op.offRL = q->offRL; op.nRL = q->nRL;
+                op.offW = q->offW;
+                return;
+            }
+        done.push_back(&op);
         auto lr = build_terms(op.W.data(), d, op.Dw1, op.Dw2, true);
         auto rl = build_terms(op.W.data(), d, op.Dw1, op.Dw2, false);
         op.offLR = all.size(); op.nLR = (int)lr.size();
@@ -578,6 +590,25 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     key = hash_val(key, op.nLR);
     for (const DevBuf* b : {&msite.Fs, &msite.Gs, &msite.Xs, &msite.P32, &msite.Qs, &msite.shifts, &msite.err})
         key = hash_val(key, b->p);
+    const bool deferred = opt.refine_tol <= 0 && opt.verbose < 3 && ctx->aux2;
+    if (deferred) {
+        // nothing here waits for the host: restarts decided on the device, the
+        // FP64 check beside the gauge move, both read back once per half-sweep
+        TN_CHECK(rq_slots());
+        LzSummary* slot = reinterpret_cast<LzSummary*>(reinterpret_cast<double*>(rqhost.p) + RQ_SLOT * (size_t)ia + 4);
+        const int rc = lanczos_solve_async(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, tol_rel,
+                                           key, slot);
+        if (rc == TN_OK) {
+            rq_lz[ia] = 1;
+            rq_flop[ia] = heff_flops(s);
+            TN_CHECK(rq_launch(ia, s, t, op.nLR, F, G, N, 0.0));
+            matvecs += 1;
+            matvecs_fp64 += 1;
+            heff_flop += heff_flops(s);
+            return TN_OK;
+        }
+        if (rc != LZ_ASYNC_UNAVAILABLE) return rc;
+    }
     LzResult rm{};
     TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel, key));
     if (ctx->prof) {  // the solve ended with a host wait, so the events have completed
@@ -587,8 +618,7 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     }
     matvecs += rm.matvecs;
     heff_flop += heff_flops(s) * rm.matvecs;
-    if (opt.refine_tol <= 0 && opt.verbose < 3 && ctx->aux2) {
-        // nothing here waits for the FP64 check: it runs beside the gauge move
+    if (deferred) {
         TN_CHECK(rq_launch(ia, s, t, op.nLR, F, G, N, rm.theta2 - rm.theta));
         matvecs += 1;
         matvecs_fp64 += 1;
@@ -632,20 +662,27 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
 // The FP64 Rayleigh quotient and residual of site ia's eigenvector, on the
 // second side stream once the Lanczos solve has finished; the result (and the
 // split operator's error flag) is read by rq_collect().
+int MPSState::rq_slots() {
+    TN_CHECK(rqhost.ensure(sizeof(double) * RQ_SLOT * (size_t)(L + 2)));
+    if ((int)rq_pending.size() != L + 2) {
+        rq_pending.assign(L + 2, 0);
+        rq_lz.assign(L + 2, 0);
+        rq_dtheta.assign(L + 2, 0.0);
+        rq_flop.assign(L + 2, 0.0);
+    }
+    return TN_OK;
+}
+
 int MPSState::rq_launch(int ia, const ContractShape& s, const WTermDev* t, int nLR, const double* F, const double* G,
                         long long N, double dtheta) {
     cudaStream_t st = ctx->stream, sx = ctx->aux2;
-    TN_CHECK(rqhost.ensure(sizeof(double) * 4 * (size_t)(L + 2)));
-    if ((int)rq_pending.size() != L + 2) {
-        rq_pending.assign(L + 2, 0);
-        rq_dtheta.assign(L + 2, 0.0);
-    }
+    TN_CHECK(rq_slots());
     const size_t scr = sizeof(double) * contract_scratch_doubles(s);
     TN_CHECK(rqP.ensure(scr));
     TN_CHECK(rqQ.ensure(scr));
     TN_CHECK(yvec.ensure(sizeof(double) * (size_t)N));
     TN_CHECK(rqbuf.ensure(rayleigh_scratch_bytes(N, ctx->sm_count)));
-    double* slot = reinterpret_cast<double*>(rqhost.p) + 4 * (size_t)ia;
+    double* slot = reinterpret_cast<double*>(rqhost.p) + RQ_SLOT * (size_t)ia;
     TN_CUDA_CHECK(cudaMemcpyAsync(slot + 3, msite.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     TN_CUDA_CHECK(cudaEventRecord(ctx->ev_y[0], st));
     TN_CUDA_CHECK(cudaStreamWaitEvent(sx, ctx->ev_y[0], 0));
@@ -667,11 +704,11 @@ int MPSState::rq_collect() {
     if (!rq_inflight) return TN_OK;
     TN_CUDA_CHECK(cudaEventSynchronize(ctx->ev_y[1]));
     rq_inflight = false;
-    int bad = 0;
+    int bad = 0, nan = 0;
     for (int ia = 1; ia <= L; ++ia) {
         if (!rq_pending[ia]) continue;
         rq_pending[ia] = 0;
-        const double* slot = reinterpret_cast<double*>(rqhost.p) + 4 * (size_t)ia;
+        const double* slot = reinterpret_cast<double*>(rqhost.p) + RQ_SLOT * (size_t)ia;
         int err = 0;
         std::memcpy(&err, slot + 3, sizeof(int));
         bad |= err;
@@ -679,6 +716,21 @@ int MPSState::rq_collect() {
         iterDE[ia] = theta - Emin[ia];
         Emin[ia] = theta;
         gapE[ia] = rq_dtheta[ia];
+        if (rq_lz[ia]) {  // the device-driven Lanczos solve of this site
+            rq_lz[ia] = 0;
+            LzSummary sm;
+            std::memcpy(&sm, slot + 4, sizeof(sm));
+            matvecs += sm.matvecs;
+            heff_flop += rq_flop[ia] * sm.matvecs;
+            if (!sm.converged) ++not_converged;
+            gapE[ia] = sm.theta2 - sm.theta;
+            for (long long q = 0; q < sm.launches; ++q) count_launch();
+            if (!std::isfinite(sm.theta)) nan = 1;
+        }
+    }
+    if (nan) {
+        set_error("lanczos: non-finite Ritz value");
+        return TN_NAN_DETECTED;
     }
     if (bad) {
         set_error("tcgen05 GEMM: a bounded mbarrier wait expired");

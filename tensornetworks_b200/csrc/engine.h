@@ -57,10 +57,13 @@ struct MPSState {
     // FP64 check of the split-precision eigenvector on the context's second side
     // stream (refine_tol = 0): contraction scratch, reduction state, and per site
     // (theta, -, resid, error flag) in pinned memory, applied by rq_collect().
+    // With the device-driven Lanczos solve (lanczos_solve_async) its summary
+    // goes to the same slot (doubles 4 ..) and is applied there too.
+    static constexpr int RQ_SLOT = 12;  // doubles per site
     DevBuf rqP, rqQ, rqbuf;
     HostBuf rqhost;
-    std::vector<char> rq_pending;
-    std::vector<double> rq_dtheta;
+    std::vector<char> rq_pending, rq_lz;
+    std::vector<double> rq_dtheta, rq_flop;
     bool rq_inflight = false;
     MixedSite msite;
     long long matvecs = 0, matvecs_fp64 = 0;
@@ -101,6 +104,7 @@ struct MPSState {
     int site_resize(int ia, int nD1, int nD2);
     int gauge_qr(int m, int n, double* W, double* Q, double* R, int ldr);
     int rescale_site(int ia);
+    int rq_slots();
     int rq_launch(int ia, const ContractShape& s, const WTermDev* t, int nLR, const double* F, const double* G,
                   long long N, double dtheta);
     void rq_order();   // the context stream waits for the in-flight check (before A[ia] changes)

@@ -14,6 +14,7 @@
 
 #include <cmath>
 #include <cstddef>
+#include <vector>
 
 namespace tnb {
 
@@ -66,7 +67,10 @@ __device__ void reduce_partials(const double* partial, int nb, int stride, int n
 
 // ---- kernels ---------------------------------------------------------------
 
-__global__ void lz_reset_kernel(LzState* st, double tol, double tol_rel, int first, int mmax) {
+// A restart's reset (first: the whole solve's); with a step-loop handle it
+// also re-arms that WHILE loop, whose value persists between restarts.
+__global__ void lz_reset_kernel(LzState* st, double tol, double tol_rel, int first, int mmax,
+                                cudaGraphConditionalHandle steps_loop = 0) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         st->done = 0;
         st->nb = 0;
@@ -82,8 +86,47 @@ __global__ void lz_reset_kernel(LzState* st, double tol, double tol_rel, int fir
             st->theta = 0;
             st->theta2 = 0;
             st->resid = 1e300;
+            st->restarts = 0;
+            st->steps = 0;
+            st->prev_resid = 1e300;
         }
+        if (steps_loop) cudaGraphSetConditional(steps_loop, 1u);
     }
+}
+
+// After a restart's Ritz vector: whether another restart runs (the host
+// loop's rule: stop when converged, when the basis spans the whole space,
+// after maxRestarts, or -- split-precision operators -- when the residual no
+// longer halves between restarts).
+__global__ void lz_decide_kernel(LzState* st, cudaGraphConditionalHandle restarts_loop, int maxRestarts,
+                                 long long N, int mm) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int r = st->restarts;  // index of the restart just finished
+    st->restarts = r + 1;
+    st->steps += st->nb;
+    bool stop = false;
+    if (st->converged) stop = true;
+    else if ((long long)mm >= N) { st->converged = 1; stop = true; }
+    else if (st->tol_rel > 0) {
+        if (r > 0 && st->resid > 0.5 * st->prev_resid) stop = true;
+        else st->prev_resid = st->resid;
+    }
+    if (r + 1 >= maxRestarts) stop = true;
+    cudaGraphSetConditional(restarts_loop, stop ? 0u : 1u);
+}
+
+__global__ void lz_summary_kernel(const LzState* st, LzSummary* out, int kernels_per_step) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    out->theta = st->theta;
+    out->theta2 = st->theta2;
+    out->resid = st->resid;
+    out->matvecs = st->matvecs;
+    out->restarts = st->restarts;
+    out->converged = st->converged;
+    out->steps = st->steps;
+    // first reset, per restart (reset, norm, scale, Ritz coefficients and vector,
+    // decision), this kernel, final reset, norm and scale
+    out->launches = 1 + 6LL * st->restarts + (long long)kernels_per_step * st->steps + 4;
 }
 
 // ||x||^2 -> st->xnorm (last block).
@@ -553,6 +596,152 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         set_error("lanczos: non-finite Ritz value");
         return TN_NAN_DETECTED;
     }
+    return TN_OK;
+}
+
+// Records the enqueue calls of `fn` on stream st into graph g after the nodes
+// deps; returns the capture's final frontier in `front` (when non-null).
+template <class F>
+int capture_into(cudaStream_t st, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, F&& fn,
+                 std::vector<cudaGraphNode_t>* front) {
+    TN_CUDA_CHECK(cudaStreamBeginCaptureToGraph(st, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                                cudaStreamCaptureModeRelaxed));
+    int rc = fn();
+    if (rc == TN_OK && front) {
+        cudaStreamCaptureStatus status;
+        const cudaGraphNode_t* d = nullptr;
+        size_t nd = 0;
+        if (cudaStreamGetCaptureInfo(st, &status, nullptr, nullptr, &d, &nd) != cudaSuccess) rc = TN_CUDA_ERROR;
+        else front->assign(d, d + nd);
+    }
+    cudaGraph_t out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &out);
+    if (rc != TN_OK) return rc;
+    TN_CUDA_CHECK(e);
+    return TN_OK;
+}
+
+// Adds a WHILE conditional node (handle created on `owner`, default 1) after
+// deps; returns the node and its body graph.
+int add_while(cudaGraph_t owner, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
+              cudaGraphConditionalHandle* h, cudaGraphNode_t* node, cudaGraph_t* body) {
+    TN_CUDA_CHECK(cudaGraphConditionalHandleCreate(h, owner, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = *h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    TN_CUDA_CHECK(cudaGraphAddNode(node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &cp));
+    *body = cp.conditional.phGraph_out[0];
+    return TN_OK;
+}
+
+int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
+                        double tol_rel, unsigned long long graph_key, LzSummary* host_out) {
+    cudaStream_t st = c.stream;
+    if (!graph_key || !c.use_graphs || st == nullptr || c.prof || N <= 0) return LZ_ASYNC_UNAVAILABLE;
+    int mm = std::min(m, LZ_MAXK - 1);
+    if ((long long)mm > N) mm = (int)N;
+    if (mm < 1) mm = 1;
+    const int maxR = maxRestarts > 0 ? maxRestarts : 1;
+    const int grid = vec_grid(N, c.sm_count);
+    // workspace: V (mm+1 vectors), w, xcur, the solve's copy of x, partials
+    size_t need = sizeof(double) * ((size_t)(mm + 4) * N + (size_t)grid * LZ_MAXK + 64);
+    TN_CHECK(c.lz.ensure(need));
+    TN_CHECK(c.lzstate.ensure(sizeof(LzState)));
+    TN_CHECK(c.lzsum.ensure(sizeof(LzSummary)));
+    double* V = c.lz.as<double>();
+    double* w = V + (size_t)(mm + 1) * N;
+    double* xcur = w + N;
+    double* xw = xcur + N;
+    double* partial = xw + N;
+    LzState* s = c.lzstate.as<LzState>();
+    LzSummary* sum = c.lzsum.as<LzSummary>();
+    unsigned long long key = hash_val(graph_key, 0x6e65737465644c5aULL);
+    for (unsigned long long v : {(unsigned long long)N, (unsigned long long)mm, (unsigned long long)maxR,
+                                 (unsigned long long)grid, alloc_generation()})
+        key = hash_val(key, v);
+    key = hash_val(key, tol);
+    key = hash_val(key, tol_rel);
+    key = hash_val(key, (const void*)V);
+    key = hash_val(key, (const void*)s);
+    key = hash_val(key, st);
+    auto it = c.lzgraphs.find(key);
+    if (it == c.lzgraphs.end()) {
+        if (c.lzgraphs.size() >= 1024) c.clear_graphs();
+        LzGraph g;
+        TN_CUDA_CHECK(cudaGraphCreate(&g.graph, 0));
+        // whatever fails while the graph is built, the caller falls back to the host-driven loop
+        auto fail = [&](int) {
+            cudaGraphDestroy(g.graph);
+            cudaGetLastError();
+            return LZ_ASYNC_UNAVAILABLE;
+        };
+        std::vector<cudaGraphNode_t> front;
+        // the whole solve's reset
+        int rc = capture_into(st, g.graph, {}, [&]() -> int {
+            lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 1, mm);
+            return cudaGetLastError() == cudaSuccess ? TN_OK : TN_CUDA_ERROR;
+        }, &front);
+        if (rc != TN_OK) return fail(rc);
+        cudaGraphConditionalHandle h_out, h_in;
+        cudaGraphNode_t n_out, n_in;
+        cudaGraph_t b_out, b_in;
+        if (add_while(g.graph, g.graph, front, &h_out, &n_out, &b_out) != TN_OK) return fail(TN_OK);
+        // a restart: reset (re-arming the steps loop), v0 = x / |x|, the steps, the Ritz vector, the decision
+        if (cudaGraphConditionalHandleCreate(&h_in, g.graph, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+            return fail(TN_OK);
+        rc = capture_into(st, b_out, {}, [&]() -> int {
+            lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0, mm, h_in);
+            lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, N, partial, s);
+            lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, V, N, s, 1, xcur);
+            return cudaGetLastError() == cudaSuccess ? TN_OK : TN_CUDA_ERROR;
+        }, &front);
+        if (rc != TN_OK) return fail(rc);
+        {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h_in;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            if (cudaGraphAddNode(&n_in, b_out, front.data(), front.size(), &cp) != cudaSuccess) return fail(TN_OK);
+            b_in = cp.conditional.phGraph_out[0];
+        }
+        const unsigned long long n0 = launch_count();
+        rc = capture_into(st, b_in, {}, [&]() -> int {
+            TN_CHECK(mv(xcur, w, &s->done));
+            TN_CHECK(launch_pdl(lz_dots_kernel, grid, LZ_THREADS, 0, st, (const double*)V, (const double*)w, N,
+                                partial, s));
+            TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, st, (const double*)V, w, N, partial, s, h_in));
+            TN_CHECK(launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, st, V, (const double*)w, N, s, xcur));
+            return TN_OK;
+        }, nullptr);
+        const unsigned long long kpi = launch_count() - n0;
+        if (rc != TN_OK) return fail(rc);
+        rc = capture_into(st, b_out, {n_in}, [&]() -> int {
+            lz_ritz_coeffs_kernel<<<1, LZ_THREADS, 0, st>>>(s);
+            lz_ritz_vector_kernel<<<grid, LZ_THREADS, 0, st>>>(V, xw, N, s);
+            lz_decide_kernel<<<1, 32, 0, st>>>(s, h_out, maxR, N, mm);
+            return cudaGetLastError() == cudaSuccess ? TN_OK : TN_CUDA_ERROR;
+        }, nullptr);
+        if (rc != TN_OK) return fail(rc);
+        // the summary, then the final normalisation of the Ritz vector
+        rc = capture_into(st, g.graph, {n_out}, [&]() -> int {
+            lz_summary_kernel<<<1, 32, 0, st>>>(s, sum, (int)kpi);
+            lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0, mm);
+            lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, N, partial, s);
+            lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, xw, N, s, 0, nullptr);
+            return cudaGetLastError() == cudaSuccess ? TN_OK : TN_CUDA_ERROR;
+        }, nullptr);
+        if (rc != TN_OK) return fail(rc);
+        if (cudaGraphInstantiate(&g.exec, g.graph, 0) != cudaSuccess) return fail(TN_OK);
+        g.kernels_per_iter = kpi;
+        it = c.lzgraphs.emplace(key, g).first;
+    }
+    TN_CUDA_CHECK(cudaMemcpyAsync(xw, x, sizeof(double) * (size_t)N, cudaMemcpyDeviceToDevice, st));
+    TN_CUDA_CHECK(cudaGraphLaunch(it->second.exec, st));
+    TN_CUDA_CHECK(cudaMemcpyAsync(x, xw, sizeof(double) * (size_t)N, cudaMemcpyDeviceToDevice, st));
+    TN_CUDA_CHECK(cudaMemcpyAsync(host_out, sum, sizeof(LzSummary), cudaMemcpyDeviceToHost, st));
     return TN_OK;
 }
 

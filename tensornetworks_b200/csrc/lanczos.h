@@ -23,11 +23,22 @@ struct LzState {
     double h[LZ_MAXK], h2[LZ_MAXK];
     double y[LZ_MAXK];
     double rhist[LZ_MAXK];  // residual estimate after each step of the current restart
+    // device-driven restarts: restarts done, Krylov steps over all restarts,
+    // and the residual of the previous restart
+    int restarts, steps;
+    double prev_resid;
 };
 
 struct LzResult {
     double theta, theta2, resid;
     int matvecs, restarts, converged;
+};
+
+// What a device-driven solve leaves for the host (copied once it finishes).
+struct LzSummary {
+    double theta, theta2, resid;
+    int matvecs, restarts, converged, steps;
+    long long launches;  // kernels the solve ran
 };
 
 // mv(x, y, skip): enqueue y = Heff x on the context stream; the launches must
@@ -53,5 +64,14 @@ int rayleigh_residual_async(cudaStream_t st, int sm_count, long long N, const do
 // device-driven WHILE loop, recorded on first use of the key and replayed.
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
                   LzResult* out, double tol_rel = 0.0, unsigned long long graph_key = 0);
+
+// The same solve with the restart loop on the device too (a WHILE node around
+// the WHILE node of the steps), so that nothing waits for the host: enqueues
+// the whole solve and, after it, the copy of its summary to host_out (pinned).
+// Returns LZ_ASYNC_UNAVAILABLE (nothing enqueued) when graphs are off or the
+// nested graph cannot be built; the caller then uses lanczos_solve.
+constexpr int LZ_ASYNC_UNAVAILABLE = -1;
+int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
+                        double tol_rel, unsigned long long graph_key, LzSummary* host_out);
 
 }  // namespace tnb

@@ -153,6 +153,7 @@ struct Ctx {
     // scratch
     DevBuf P, Q;           // contraction intermediates
     DevBuf lz;             // Lanczos basis + work vectors
+    DevBuf lzsum;          // summary of a device-driven Lanczos solve
     DevBuf lzstate;        // Lanczos device state
     DevBuf rq;             // Rayleigh-quotient state + partials
     DevBuf dv, dvstate;    // Davidson basis + work vectors, device state

@@ -50,13 +50,15 @@ __device__ double block_eig_k(int n, const double* a, const double* b, int k) {
     lo -= 1e-14 * scale + 1e-300;
     hi += 1e-14 * scale + 1e-300;
     const int T = blockDim.x;
+    // the trial points' fractions of the bracket, divided once rather than every round
+    const double inv = 1.0 / (double)(T + 1), frac = (double)(threadIdx.x + 1) * inv;
     for (int round = 0; round < 12; ++round) {
-        double x = lo + (hi - lo) * (double)(threadIdx.x + 1) / (double)(T + 1);
+        double x = lo + (hi - lo) * frac;
         int ok = sturm_count(n, a, b, x) <= k;
         int cnt = __syncthreads_count(ok);
         if (threadIdx.x == 0) {
-            double nlo = cnt > 0 ? lo + (hi - lo) * (double)cnt / (double)(T + 1) : lo;
-            double nhi = cnt < T ? lo + (hi - lo) * (double)(cnt + 1) / (double)(T + 1) : hi;
+            double nlo = cnt > 0 ? lo + (hi - lo) * ((double)cnt * inv) : lo;
+            double nhi = cnt < T ? lo + (hi - lo) * ((double)(cnt + 1) * inv) : hi;
             s_lo = nlo;
             s_hi = nhi;
         }
