@@ -212,24 +212,18 @@ __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __res
     }
 }
 
-// w' = w - V h;  h2 = V^T w';  nrm2 = |w'|^2.  The last block forms alpha_j,
-// beta_j, solves the tridiagonal problem and sets the convergence flag.  Inside
-// a graph loop (cond != 0) it also decides whether the loop runs another step:
-// every step reaches this last block, and it ends the loop at the latest when
-// the basis limit is reached, so the loop always terminates.
+// w' = w - V h;  h2 = V^T w';  nrm2 = |w'|^2.  The last block forms alpha_j and
+// beta_j; the tridiagonal eigenproblem and the decision to stop follow in
+// block 0 of lz_next_kernel, beside the other blocks' vector work.
 __global__ void lz_update_kernel(const double* __restrict__ V, double* __restrict__ w, long long N,
-                                 double* partial, LzState* st, cudaGraphConditionalHandle cond) {
+                                 double* partial, LzState* st) {
     pdl_wait();
-    if (st->done) {
-        if (cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
-        return;
-    }
+    if (st->done) return;
     __shared__ double sh[KCHUNK * 32];
     __shared__ double res[KCHUNK];
     __shared__ double hs[LZ_MAXK];
     __shared__ bool last;
     const int j = st->j;
-    const int mmax = st->mmax;
     const int nk = j + 1;
     for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h[k];
     __syncthreads();
@@ -273,50 +267,65 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
         st->beta[j] = sqrt(fmax(nrm2 - ss, 0.0));
         st->counter = 0;
         st->matvecs += 1;
-    }
-    __syncthreads();
-    const double* a = st->alpha;
-    const double* b = st->beta;
-    double th = block_eig_k(nk, a, b, 0);
-    if (threadIdx.x == 0) {
-        double yl = last_component(nk, a, b, th);
-        double bj = b[j];
-        double resid = bj * yl;
-        double tolEff = fmax(st->tol, 1e-13 * fmax(1.0, fabs(th)));
-        if (st->tol_rel > 0) {
-            double tn = 0;
-            for (int i = 0; i < nk; ++i)
-                tn = fmax(tn, fabs(a[i]) + fabs(b[i]) + (i > 0 ? fabs(b[i - 1]) : 0.0));
-            tolEff = fmax(tolEff, st->tol_rel * tn);
-        }
-        st->theta = th;
-        st->resid = resid;
-        st->nb = nk;
-        st->rhist[j] = resid;
-        bool conv = (resid <= tolEff) || (bj <= 1e-14 * fmax(1.0, fabs(th)));
-        if (conv) { st->done = 1; st->converged = 1; }
-        // split-precision operator: a residual that no longer halves over two
-        // steps has reached the operator's noise floor
-        if (st->tol_rel > 0 && j >= 2 && resid > 0.5 * st->rhist[j - 2]) st->done = 1;
-        if (nk >= mmax || nk >= LZ_MAXK - 1) st->done = 1;  // basis exhausted for this restart
         st->jn = j + 1;
-        if (cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
     }
 }
 
 // V_{j+1} = (w' - V h2) / beta_j, also into the matvec input xcur; the last
-// block advances the step index (the other blocks read only jn).
+// block advances the step index (the other blocks read only jn).  Block 0
+// first solves the tridiagonal problem of step j, sets the convergence flag
+// and, inside a graph loop (cond != 0), whether the loop runs another step:
+// every step reaches it, and it ends the loop at the latest when the basis
+// limit is reached, so the loop always terminates.  Blocks that start after
+// block 0 has set the flag return at once; the loop then ends, so the step's
+// vector (and the half-counted ticket, which the next reset clears) is unused.
 __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N, LzState* st,
-                               double* __restrict__ xcur) {
+                               double* __restrict__ xcur, cudaGraphConditionalHandle cond = 0) {
     pdl_wait();
-    if (st->done) return;
+    if (st->done) {
+        if (cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+        return;
+    }
     __shared__ double hs[LZ_MAXK];
     __shared__ double inv;
     __shared__ bool last;
     const int j = st->jn - 1;
     const int nk = j + 1;
+    if (blockIdx.x == 0) {
+        const double* a = st->alpha;
+        const double* b = st->beta;
+        const double th = block_eig_k(nk, a, b, 0);
+        if (threadIdx.x == 0) {
+            const double yl = last_component(nk, a, b, th);
+            const double bj = b[j];
+            const double resid = bj * yl;
+            double tolEff = fmax(st->tol, 1e-13 * fmax(1.0, fabs(th)));
+            if (st->tol_rel > 0) {
+                double tn = 0;
+                for (int i = 0; i < nk; ++i)
+                    tn = fmax(tn, fabs(a[i]) + fabs(b[i]) + (i > 0 ? fabs(b[i - 1]) : 0.0));
+                tolEff = fmax(tolEff, st->tol_rel * tn);
+            }
+            st->theta = th;
+            st->resid = resid;
+            st->nb = nk;
+            st->rhist[j] = resid;
+            int done = 0;
+            const bool conv = (resid <= tolEff) || (bj <= 1e-14 * fmax(1.0, fabs(th)));
+            if (conv) { done = 1; st->converged = 1; }
+            // split-precision operator: a residual that no longer halves over two
+            // steps has reached the operator's noise floor
+            if (st->tol_rel > 0 && j >= 2 && resid > 0.5 * st->rhist[j - 2]) done = 1;
+            if (nk >= st->mmax || nk >= LZ_MAXK - 1) done = 1;  // basis exhausted for this restart
+            if (done) st->done = 1;
+            if (cond) cudaGraphSetConditional(cond, done ? 0u : 1u);
+        }
+    }
     for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h2[k];
-    if (threadIdx.x == 0) inv = 1.0 / st->beta[j];
+    if (threadIdx.x == 0) {
+        const double bj = st->beta[j];
+        inv = bj > 0 ? 1.0 / bj : 0.0;
+    }
     __syncthreads();
     double* vn = V + (long long)(j + 1) * N;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
@@ -478,8 +487,8 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
     auto enqueue_step = [&](cudaGraphConditionalHandle cond) -> int {
         TN_CHECK(mv(xcur, w, &s->done));
         TN_CHECK(launch_pdl(lz_dots_kernel, grid, LZ_THREADS, 0, st, (const double*)V, (const double*)w, N, partial, s));
-        TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, st, (const double*)V, w, N, partial, s, cond));
-        TN_CHECK(launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, st, V, (const double*)w, N, s, xcur));
+        TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, st, (const double*)V, w, N, partial, s));
+        TN_CHECK(launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, st, V, (const double*)w, N, s, xcur, cond));
         return TN_OK;
     };
 
@@ -712,8 +721,8 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
             TN_CHECK(mv(xcur, w, &s->done));
             TN_CHECK(launch_pdl(lz_dots_kernel, grid, LZ_THREADS, 0, st, (const double*)V, (const double*)w, N,
                                 partial, s));
-            TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, st, (const double*)V, w, N, partial, s, h_in));
-            TN_CHECK(launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, st, V, (const double*)w, N, s, xcur));
+            TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, st, (const double*)V, w, N, partial, s));
+            TN_CHECK(launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, st, V, (const double*)w, N, s, xcur, h_in));
             return TN_OK;
         }, nullptr);
         const unsigned long long kpi = launch_count() - n0;

@@ -228,9 +228,17 @@ __global__ void __launch_bounds__(THREADS, 1)
                         }
                     } else if (p.out_mode == TC_OUT_F32_ROWMAJOR) {
                         float* dst = p.c32 + (long long)b * p.c_batch + (long long)row * p.ldc + n0 + c0;
+                        if (n0 + c0 + 16 <= p.N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                            // a thread owns a row: 16-byte stores (a quarter of the transactions)
 #pragma unroll
-                        for (int i = 0; i < 16; ++i)
-                            if (n0 + c0 + i < p.N) dst[i] = v[i] * p.alpha;
+                            for (int i = 0; i < 16; i += 4)
+                                *reinterpret_cast<float4*>(dst + i) = make_float4(v[i] * p.alpha, v[i + 1] * p.alpha,
+                                                                                  v[i + 2] * p.alpha, v[i + 3] * p.alpha);
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 16; ++i)
+                                if (n0 + c0 + i < p.N) dst[i] = v[i] * p.alpha;
+                        }
                     } else {
                         double* dst = p.c64 + (long long)b * p.c_batch + row;
 #pragma unroll
