@@ -234,13 +234,31 @@ def matvec_microbench(T, ctx, torch, D, precision, reps=50):
         for _ in range(5):
             T._capi.check(lib.tn_heff_apply(h, x.data_ptr(), y.data_ptr()), "tn_heff_apply")
         torch.cuda.synchronize()
+        # the applications recorded once in a CUDA graph and replayed, so that the
+        # time is the device's and not the host's launch rate (eager loop if the
+        # capture is refused)
+        graph = None
+        try:
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=stream):
+                for _ in range(reps):
+                    T._capi.check(lib.tn_heff_apply(h, x.data_ptr(), y.data_ptr()), "tn_heff_apply")
+            graph.replay()
+            torch.cuda.synchronize()
+        except Exception:
+            graph = None
+            torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        for _ in range(reps):
-            T._capi.check(lib.tn_heff_apply(h, x.data_ptr(), y.data_ptr()), "tn_heff_apply")
+        if graph is not None:
+            graph.replay()
+        else:
+            for _ in range(reps):
+                T._capi.check(lib.tn_heff_apply(h, x.data_ptr(), y.data_ptr()), "tn_heff_apply")
         e.record(stream)
         e.synchronize()
         t = s.elapsed_time(e) / 1e3 / reps
+        del graph
         T._capi.check(lib.tn_heff_destroy(h), "tn_heff_destroy")
     finally:
         lib.tn_ctx_set_stream(ctx.handle, None)
