@@ -1233,7 +1233,10 @@ int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double
     }
     const int nwb = (n + QRP_WB - 1) / QRP_WB, nqb = Qout ? (m + QRP_QB - 1) / QRP_QB : 0;
     const int tasks = std::max(1, (n - 32 + QRP_WB - 1) / QRP_WB) + nqb;  // most tasks of one reflector
-    const int G = std::min(max_per_sm * c.sm_count, 1 + tasks);
+    // 64 workers keep ahead of the panel chain (a reflector's ~180 tasks at
+    // m = 512 take them ~30 us of a ~50 us panel period) and leave SMs to other
+    // contexts sharing the device
+    const int G = std::min(std::min(max_per_sm * c.sm_count, 1 + tasks), 65);
     if (G < 2) return QRP_UNAVAILABLE;
     const size_t words = 4 + (size_t)nwb + (size_t)nqb;
     TN_CHECK(c.qrsync.ensure(sizeof(int) * words));
