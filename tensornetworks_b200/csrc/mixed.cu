@@ -212,6 +212,15 @@ int heff_matvec_mixed(Ctx& c, MixedSite& ms, const double* x, double* y, const i
     TcGemmPlan p3 = ms.plan3;
     p3.args.skip = skip;
     TN_CHECK(tc_gemm_run(p3, st));
+    if (c.take_tail) {  // the caller forms y with its own next kernel
+        MatvecTail& t = *c.take_tail;
+        t.deferred = true;
+        t.Yp = ms.P32.as<float>();
+        t.d = s.d;
+        t.Dw2 = s.Dw2;
+        t.blk = blk;
+        return TN_OK;
+    }
     TN_CHECK(launch_pdl(reduce_w2_kernel, g1d(nX), 256, 0, st, (const float*)ms.P32.as<float>(), s.d, s.Dw2, blk, y,
                         skip));
     return TN_OK;
