@@ -34,7 +34,7 @@ def worker(rank, world, port, out):
 @pytest.mark.parametrize("world", [2])
 def test_max_over_ranks_gloo(world):
     port = free_port()
-    manager = mp.Manager()
+    manager = mp.get_context("spawn").Manager()  # no fork of a multi-threaded process
     out = manager.dict()
     mp.spawn(worker, args=(world, port, out), nprocs=world, join=True)
     assert [out[r] for r in range(world)] == [0.25 + 0.5 * (world - 1)] * world
