@@ -280,10 +280,20 @@ int tn_itebd_get_bond(tn_itebd st, int bond, int* D, double* host);
 int tn_itebd_set_bond(tn_itebd st, int bond, int D, const double* host);
 /* nsteps second-order Trotter steps at time step dt, truncation to Dmax. */
 int tn_itebd_step(tn_itebd st, double dt, int Dmax, int nsteps);
-/* Schedule of time steps dts[0..ndt): each line runs steps until the bond
- * values move by at most eps_factor*dt or max_iter steps (steps_out[i]). */
+/* iTEBDStateImp::FindiTimeGroundState(H, iH, schedule)
+ * (iTEBDStateImp_iTime.C:25-104) over the time steps dts[0..ndt), one
+ * schedule line each: OrthogonalizeI, then for D = current .. Dmax by deltaD
+ * (IncreaseBondDimensions) steps until both bond vectors move by at most
+ * eps_factor*dt or max_iter steps, then OrthogonalizeI again.  steps_out[i]
+ * receives the Trotter steps of line i. */
 int tn_itebd_find_ground_state(tn_itebd st, const double* dts, int ndt, int max_iter, int Dmax,
-                               double eps_factor, int* steps_out);
+                               int deltaD, double eps_factor, int* steps_out);
+/* iTEBDStateImp::OrthogonalizeI(comp, eps, niter) (iTEBDStateImp_OrthoNorm.C:
+ * 110-128, 511-637) at centre 1 with the (Dmax, 1e-16) compressor: the
+ * iterative re-orthogonalisation to canonical Vidal form.  *delta: last change
+ * of the bond values, *iters: iterations run.  TN_NOT_CONVERGED when a norm
+ * matrix was singular (the reference's bail-out; the state is still unpacked). */
+int tn_itebd_orthogonalize(tn_itebd st, int Dmax, double eps, int max_iter, double* delta, int* iters);
 /* Energy per bond (iTEBDState::GetExpectation): transfer-matrix fixed points by
  * power iteration (max_iters, tolerance tol on the normalised fixed point). */
 int tn_itebd_energy(tn_itebd st, int max_iters, double tol, double* E);

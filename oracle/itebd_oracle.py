@@ -163,3 +163,139 @@ def expectation(st, h):
         den = np.einsum("ik,pij,pkl,jl->", lft, B, B, rgt)
         es.append(num / den)
     return float(0.5 * (es[0] + es[1]))
+
+
+# ---------------------------------------------------------------------------
+# Re-orthogonalisation between schedule lines and the reference's line driver
+# ---------------------------------------------------------------------------
+def norm_matrices(gam, lam):
+    """GetNormMatrix (iTEBDStateImp_Contractions.C:293-333) of gamma*lambda
+    (DRight: sum_n M_n M_n^T) and of lambda*gamma (DLeft: sum_n M_n^T M_n)."""
+    Mr = gam * lam[None, None, :]
+    Ml = lam[None, :, None] * gam
+    Vr = np.einsum("nij,nkj->ik", Mr, Mr)
+    Vl = np.einsum("nij,nik->jk", Ml, Ml)
+    return Vr, Vl
+
+
+def factor(V):
+    """Factor (iTEBDStateImp_OrthoNorm.C:486-509): V = X X^T with X = U sqrt(e),
+    Xinv = sqrt(e)^-1 U^T, from the eigen-decomposition of the symmetrised V."""
+    e, U = np.linalg.eigh(0.5 * (V + V.T))
+    X = U * np.sqrt(e)[None, :]
+    Xinv = (U / np.sqrt(e)[None, :]).T
+    return X, Xinv
+
+
+def orthogonalize_gamma(gam, lam, eps, max_iter):
+    """OrthogonalizeI(gamma, lambda, eps, maxIter), iTEBDStateImp_OrthoNorm.C:511-637:
+    the iterative re-orthogonalisation of Phien, McCulloch and Vidal (PRB 91,
+    115137, 2015).  gam is (d*d, D, D), lam (D,).  Returns (gam, lam, bailed)."""
+    gam = gam.copy()
+    lam = lam.copy()
+    er = 1.0
+    for it in range(max_iter):
+        Vr, Vl = norm_matrices(gam, lam)
+        if min(np.abs(np.diag(Vr)).min(), np.abs(np.diag(Vl)).min()) < 1e-10:
+            return gam, lam, True       # singular: bail out without the final normalisation (:547-554)
+        er, el = Vr[0, 0], Vl[0, 0]
+        Vr = Vr / er
+        Vl = Vl / el
+        gam = gam / np.sqrt(el)
+        X, Xinv = factor(Vr)
+        Yd, Ydinv = factor(Vl)
+        if np.isnan(X).any() or np.isnan(Yd).any():
+            return gam, lam, True
+        YT, YTinv = Yd.T, Ydinv.T
+        U, lp, VT = np.linalg.svd(YT @ (lam[:, None] * X))
+        lp = lp / np.sqrt(np.dot(lp, lp))
+        VX, YU = VT @ Xinv, YTinv @ U
+        gam = np.einsum("ij,njk,kl->nil", VX, gam, YU)
+        deltal = np.abs(lam - lp).max()
+        lam = lp
+        if deltal < eps:
+            break
+    gam = gam / np.sqrt(er)
+    return gam, lam, False
+
+
+def unpack_orthonormal(st, gam, Dmax, eps_compress=1e-16):
+    """UnpackOrthonormal (iTEBDStateImp_OrthoNorm.C:148-200) at centre 1:
+    lambdaB gamma[na + d nb] lambdaB reshaped (row i + D na, column j + D nb),
+    SVD, SVCompressor(Dmax, eps), lambdaA = s/|s|, GA = lB^-1 P, GB = Q lB^-1."""
+    d = st.d
+    lB = st.l[1]
+    D = lB.size
+    M = np.empty((d * D, d * D))
+    for nb in range(d):
+        for na in range(d):
+            M[na * D:(na + 1) * D, nb * D:(nb + 1) * D] = lB[:, None] * gam[na + d * nb] * lB[None, :]
+    U, s, Vt = np.linalg.svd(M, full_matrices=False)
+    keep, sk = compress(s, Dmax, eps_compress)
+    st.l[0] = sk / np.linalg.norm(sk)
+    st.G[0] = np.stack([U[n * D:(n + 1) * D, :keep] / lB[:, None] for n in range(d)])
+    st.G[1] = np.stack([Vt[:keep, n * D:(n + 1) * D] / lB[None, :] for n in range(d)])
+
+
+def orthogonalize_i(st, Dmax, eps, max_iter=100):
+    """iTEBDStateImp::OrthogonalizeI(comp, eps, niter) (iTEBDStateImp_OrthoNorm.C:110-128)
+    at centre 1: gamma[na + d nb] = GA[na] lA GB[nb] (ContractAlB), the
+    iteration above on (gamma, lambdaB), lambdaB := the result normalised,
+    then UnpackOrthonormal with the (Dmax, 1e-16) compressor."""
+    d = st.d
+    GA, GB, lA = st.G[0], st.G[1], st.l[0]
+    gam = np.stack([(GA[na] * lA[None, :]) @ GB[nb] for nb in range(d) for na in range(d)])
+    # the stack above runs nb outer, na inner: index na + d*nb, as ContractAlB
+    gam, lam, _ = orthogonalize_gamma(gam, st.l[1], eps, max_iter)
+    st.l[1] = lam / np.linalg.norm(lam)
+    unpack_orthonormal(st, gam, Dmax)
+
+
+def grow(st, D):
+    """IncreaseBondDimensions (iTEBDStateImp.C:63, MPSSite::NewBondDimensions,
+    Bond::NewBondDimension Bond.C:60-84): Gammas zero-padded to D x D, bond
+    values padded with min(s)/10 and renormalised."""
+    for b in range(2):
+        l = st.l[b]
+        if l.size < D:
+            st.l[b] = np.concatenate([l, np.full(D - l.size, l.min() / 10.0)])
+            st.l[b] /= np.linalg.norm(st.l[b])
+    for s in range(2):
+        g = st.G[s]
+        out = np.zeros((st.d, D, D))
+        out[:, :g.shape[1], :g.shape[2]] = g
+        st.G[s] = out
+
+
+def find_ground_state_lines(S, Dstart, Dmax, deltaD, dts, max_iter, Jxy=1.0, Jz=1.0, hz=0.0, seed=1,
+                            eps_factor=5e-5, orth_iter=100):
+    """iTEBDStateImp::FindiTimeGroundState(H, iH, H2, line), iTEBDStateImp_iTime.C:44-104,
+    over the schedule of iTEBDTests.C (MakeSchedule: dt lines, dlambda epsilon
+    eps_factor*dt, D grown from the current D to Dmax by deltaD inside each
+    line): per line OrthogonalizeI (eps dt^2/1000, 1e-13 for dt = 0), then
+    for each D the second-order steps until both bond vectors change by at
+    most eps_factor*dt, then OrthogonalizeI again.  Returns (E, state, steps)."""
+    st = State(S, Dstart, seed)
+    h = O.local_h12(S, Jxy, Jz, hz)
+    steps = []
+    for dt in dts:
+        gates = [gate(S, Jxy, Jz, hz, dt / 2), gate(S, Jxy, Jz, hz, dt), gate(S, Jxy, Jz, hz, dt / 2)]
+        eps_orth = 1e-13 if dt == 0.0 else dt * dt / 1000.0
+        Dcur = max(st.l[0].size, st.l[1].size)
+        orthogonalize_i(st, Dcur, eps_orth, orth_iter)
+        D = Dcur
+        while D <= Dmax:
+            if D > Dcur:
+                grow(st, D)
+            n = 0
+            for n in range(1, max_iter + 1):
+                old = [x.copy() for x in st.l]
+                st.step(gates, D)
+                dl = max(np.abs(o - x).max() if o.size == x.size else 1.0 for o, x in zip(old, st.l))
+                if dl <= eps_factor * dt:
+                    break
+            steps.append(n)
+            orthogonalize_i(st, D, eps_orth, orth_iter)
+            Dcur = D
+            D += deltaD
+    return expectation(st, h), st, steps

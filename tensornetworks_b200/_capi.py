@@ -96,7 +96,8 @@ SIGNATURES = {
     "tn_itebd_get_bond": (_I, [_V, _I, _PI, _V]),
     "tn_itebd_set_bond": (_I, [_V, _I, _I, _V]),
     "tn_itebd_step": (_I, [_V, _D, _I, _I]),
-    "tn_itebd_find_ground_state": (_I, [_V, _V, _I, _I, _I, _D, _V]),
+    "tn_itebd_find_ground_state": (_I, [_V, _V, _I, _I, _I, _I, _D, _V]),
+    "tn_itebd_orthogonalize": (_I, [_V, _I, _D, _I, _PD, _PI]),
     "tn_itebd_energy": (_I, [_V, _I, _D, _PD]),
     "tn_mlp_create": (_I, [_V, _ULL, _PV]),
     "tn_mlp_destroy": (_I, [_V]),

@@ -372,15 +372,26 @@ class iTEBDState:
     def Step(self, dt: float, Dmax: int, nsteps: int = 1):
         check(self._lib.tn_itebd_step(self.handle, float(dt), int(Dmax), int(nsteps)), "tn_itebd_step")
 
-    def FindiTimeGroundState(self, dts, max_iter: int, Dmax: int, eps_factor: float = 5e-5) -> List[int]:
-        """One schedule line per dt (IterationScheduleLine itsdt): steps until the
-        bond values move by at most eps_factor*dt, or max_iter steps."""
+    def FindiTimeGroundState(self, dts, max_iter: int, Dmax: int, eps_factor: float = 5e-5,
+                             deltaD: int = 1) -> List[int]:
+        """One schedule line per dt (IterationScheduleLine itsdt, itsDmax,
+        itsDeltaD; dlambda epsilon eps_factor*dt as iTEBDTests.C MakeSchedule):
+        OrthogonalizeI, bond dimension grown to Dmax by deltaD with steps until
+        the bond values move by at most eps_factor*dt (or max_iter steps) at
+        each D, OrthogonalizeI again.  Returns the Trotter steps per line."""
         dts = np.ascontiguousarray(dts, dtype=np.float64)
         steps = np.zeros(dts.size, dtype=np.int32)
         check(self._lib.tn_itebd_find_ground_state(self.handle, dts.ctypes.data, dts.size, int(max_iter), int(Dmax),
-                                                   float(eps_factor), steps.ctypes.data),
+                                                   int(deltaD), float(eps_factor), steps.ctypes.data),
               "tn_itebd_find_ground_state")
         return steps.tolist()
+
+    def OrthogonalizeI(self, Dmax: int, eps: float, max_iter: int = 100):
+        """iTEBDStateImp::OrthogonalizeI: returns (last bond-value change, iterations)."""
+        delta, iters = C.c_double(), C.c_int()
+        check(self._lib.tn_itebd_orthogonalize(self.handle, int(Dmax), float(eps), int(max_iter), C.byref(delta),
+                                               C.byref(iters)), "tn_itebd_orthogonalize")
+        return delta.value, iters.value
 
     def GetExpectation(self, max_iters: int = 20000, tol: float = 1e-13) -> float:
         """Energy per bond of the infinite chain."""

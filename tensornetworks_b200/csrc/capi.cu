@@ -152,7 +152,7 @@ int tn_ctx_create(int device, tn_ctx* out) {
         set_error("device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
         return TN_NO_DEVICE;
     }
-    TN_CUDA_CHECK(cudaSetDevice(device));
+    TN_ON_DEVICE(device);
     tn_ctx c = new tn_ctx_s();
     c->c.device = device;
     c->c.sm_count = prop.multiProcessorCount;
@@ -173,7 +173,7 @@ int tn_ctx_create(int device, tn_ctx* out) {
 
 int tn_ctx_destroy(tn_ctx c) {
     if (!c) return TN_BAD_ARG;
-    cudaSetDevice(c->c.device);
+    TN_ON_DEVICE(c->c.device);
     cudaStreamSynchronize(c->c.stream);
     c->c.clear_graphs();
     if (c->c.aux) cudaStreamSynchronize(c->c.aux);
@@ -201,6 +201,7 @@ int tn_ctx_set_stream(tn_ctx c, void* stream) {
 
 int tn_ctx_synchronize(tn_ctx c) {
     if (!c) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     TN_CUDA_CHECK(cudaStreamSynchronize(c->c.stream));
     return TN_OK;
 }
@@ -223,7 +224,7 @@ int tn_hamiltonian_create_heisenberg(tn_ctx c, int L, double S, int form, double
         set_error("Jxy and Jz both zero");
         return TN_BAD_ARG;
     }
-    TN_CUDA_CHECK(cudaSetDevice(c->c.device));
+    TN_ON_DEVICE(c->c.device);
     tn_hamiltonian h = new tn_hamiltonian_s();
     h->h.ctx = &c->c;
     h->h.L = L;
@@ -244,6 +245,7 @@ int tn_hamiltonian_create_heisenberg(tn_ctx c, int L, double S, int form, double
 
 int tn_hamiltonian_destroy(tn_hamiltonian h) {
     if (!h) return TN_BAD_ARG;
+    TN_ON_DEVICE(h->h.ctx->device);
     delete h;
     return TN_OK;
 }
@@ -267,7 +269,7 @@ int tn_hamiltonian_get_w(tn_hamiltonian h, int site, double* W) {
 int tn_mps_create(tn_hamiltonian h, int D, double normEps, double epsSV, tn_mps* out) {
     if (!h || !out || D < 1) return TN_BAD_ARG;
     *out = nullptr;
-    TN_CUDA_CHECK(cudaSetDevice(h->h.ctx->device));
+    TN_ON_DEVICE(h->h.ctx->device);
     tn_mps m = new tn_mps_s();
     m->m.normEps = normEps;
     m->m.epsSV = epsSV;
@@ -282,6 +284,7 @@ int tn_mps_create(tn_hamiltonian h, int D, double normEps, double epsSV, tn_mps*
 
 int tn_mps_destroy(tn_mps m) {
     if (!m) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     cudaStreamSynchronize(m->m.ctx->stream);
     delete m;
     return TN_OK;
@@ -289,6 +292,7 @@ int tn_mps_destroy(tn_mps m) {
 
 int tn_mps_initialize_random(tn_mps m, uint64_t seed) {
     if (!m) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     return m->m.initialize_random(seed);
 }
 
@@ -301,6 +305,7 @@ int tn_mps_get_site_dims(tn_mps m, int site, int* D1, int* D2) {
 
 int tn_mps_get_site(tn_mps m, int site, double* A) {
     if (!m || !A || site < 1 || site > m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     auto& s = m->m;
     TN_CUDA_CHECK(cudaStreamSynchronize(s.ctx->stream));
     TN_CUDA_CHECK(cudaMemcpy(A, s.A[site]->p, sizeof(double) * (size_t)s.d * s.D1[site] * s.D2[site],
@@ -310,6 +315,7 @@ int tn_mps_get_site(tn_mps m, int site, double* A) {
 
 int tn_mps_set_site(tn_mps m, int site, int D1, int D2, const double* A) {
     if (!m || !A || site < 1 || site > m->m.L || D1 < 1 || D2 < 1) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     auto& s = m->m;
     TN_CHECK(s.ensure_capacity(std::max(D1, D2)));
     TN_CUDA_CHECK(cudaStreamSynchronize(s.ctx->stream));
@@ -324,6 +330,7 @@ int tn_mps_set_site(tn_mps m, int site, int D1, int D2, const double* A) {
 
 int tn_mps_get_bond(tn_mps m, int bond, int* D, double* s_host) {
     if (!m || bond < 1 || bond >= m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     TN_CHECK(m->m.ensure_bond_values());
     const auto& s = m->m.bond_s[bond];
     if (D) *D = (int)s.size();
@@ -333,6 +340,7 @@ int tn_mps_get_bond(tn_mps m, int bond, int* D, double* s_host) {
 
 int tn_mps_normalize(tn_mps m, int direction) {
     if (!m) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     TN_CHECK(m->m.normalize_all(direction == TN_DLEFT));
     TN_CUDA_CHECK(cudaStreamSynchronize(m->m.ctx->stream));
     return TN_OK;
@@ -346,17 +354,20 @@ int tn_mps_get_max_d(tn_mps m, int* D) {
 
 int tn_mps_get_expectation(tn_mps m, tn_hamiltonian h, double* E) {
     if (!m || !h || !E || h->h.L != m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     return m->m.expectation(h->h.ops, E);
 }
 
 int tn_mps_get_expectation_h2(tn_mps m, tn_hamiltonian h, double* E2) {
     if (!m || !h || !E2 || h->h.L != m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     return m->m.expectation(h->h.ops2, E2);
 }
 
 int tn_mps_find_variational_ground_state(tn_mps m, tn_hamiltonian h, const tn_sched_line* lines, int nlines,
                                          const tn_solver_options* opt, tn_sweep_stats* stats, double* variance) {
     if (!m || !h || !lines || nlines < 1 || h->h.L != m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     for (int i = 0; i < nlines; ++i)
         if (lines[i].max_sweeps < 1 || lines[i].Dmax < 1) {
             set_error("schedule line %d invalid", i);
@@ -374,12 +385,14 @@ int tn_mps_find_variational_ground_state(tn_mps m, tn_hamiltonian h, const tn_sc
 int tn_mps_sweep(tn_mps m, tn_hamiltonian h, int nsweeps, double eps_eigen, const tn_solver_options* opt,
                  tn_sweep_stats* stats) {
     if (!m || !h || nsweeps < 1 || h->h.L != m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     m->m.H = &h->h;
     return m->m.sweep_pairs(nsweeps, eps_eigen, opt, stats);
 }
 
 int tn_mps_prepare_sweeps(tn_mps m, tn_hamiltonian h) {
     if (!m || !h || h->h.L != m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     m->m.H = &h->h;
     return m->m.prepare_sweeps();
 }
@@ -411,6 +424,7 @@ extern "C" {
 int tn_heff_create(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
                    const double* F, const double* G, tn_heff* out) {
     if (!c || !W_host || !F || !G || !out) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     *out = nullptr;
     if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
     if (precision < TN_PREC_FP64 || precision > TN_PREC_MIXED_HI) return TN_BAD_ARG;
@@ -452,6 +466,7 @@ long long tn_heff_size(tn_heff h) { return h ? (long long)h->s.d * h->s.D1 * h->
 
 int tn_heff_apply(tn_heff h, const double* x, double* y) {
     if (!h || !x || !y) return TN_BAD_ARG;
+    TN_ON_DEVICE(h->ctx->c.device);
     Ctx& cx = h->ctx->c;
     if (h->precision == TN_PREC_FP64)
         return heff_matvec_f64(h->s, h->terms.as<WTermDev>(), h->nterms, h->F, h->G, x, y, h->P.as<double>(),
@@ -461,6 +476,7 @@ int tn_heff_apply(tn_heff h, const double* x, double* y) {
 
 int tn_heff_destroy(tn_heff h) {
     if (!h) return TN_BAD_ARG;
+    TN_ON_DEVICE(h->ctx->c.device);
     cudaStreamSynchronize(h->ctx->c.stream);
     int st = TN_OK;
     if (h->precision != TN_PREC_FP64 && h->ms.ready) st = mixed_check_error(h->ms, h->ctx->c.stream);
@@ -471,6 +487,7 @@ int tn_heff_destroy(tn_heff h) {
 int tn_heff_matvec(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
                    const double* F, const double* G, const double* x, double* y) {
     if (!c || !W_host || !F || !G || !x || !y) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
     if (precision != TN_PREC_FP64) {
         tn_heff h = nullptr;
@@ -494,6 +511,7 @@ int tn_heff_matvec(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int
 int tn_heff_diag(tn_ctx c, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host, const double* F,
                  const double* G, double* diag) {
     if (!c || !W_host || !F || !G || !diag) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
     Ctx& cx = c->c;
     size_t nw = (size_t)Dw1 * Dw2 * d * d;
@@ -508,6 +526,7 @@ int tn_heff_diag(tn_ctx c, int d, int Dw1, int Dw2, int D1, int D2, const double
 int tn_env_left(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
                 const double* A, const double* F, double* Fout) {
     if (!c || !W_host || !A || !F || !Fout) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
     if (precision != TN_PREC_FP64) return TN_BAD_ARG;
     Ctx& cx = c->c;
@@ -524,6 +543,7 @@ int tn_env_left(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2
 int tn_env_right(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int D2, const double* W_host,
                  const double* A, const double* G, double* Gout) {
     if (!c || !W_host || !A || !G || !Gout) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
     if (precision != TN_PREC_FP64) return TN_BAD_ARG;
     Ctx& cx = c->c;
@@ -541,6 +561,7 @@ int tn_eigensolve_heff(tn_ctx c, const tn_solver_options* opt, int d, int Dw1, i
                        const double* W_host, const double* F, const double* G, double* x, double tol,
                        double* theta, double* residual, int* matvecs) {
     if (!c || !W_host || !F || !G || !x) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     if (!valid_shape(d, Dw1, Dw2, D1, D2)) return TN_BAD_SHAPE;
     Ctx& cx = c->c;
     int krylov = (opt && opt->krylov > 0) ? opt->krylov : 20;
@@ -586,6 +607,7 @@ int tn_eigensolve_heff(tn_ctx c, const tn_solver_options* opt, int d, int Dw1, i
 int tn_eigensolve_dense(tn_ctx c, int N, const double* A, int lda, int k, double tol, double* w_host, double* U,
                         int ldu) {
     if (!c || !A || !w_host || !U || N < 1 || k < 1 || k > N || lda < N || ldu < N) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     Ctx& cx = c->c;
     // Lowest k pairs by Lanczos with shift deflation: A' = A + sigma sum_i u_i u_i^T.
     // sigma above the spectral radius bound (max row sum).
@@ -641,6 +663,7 @@ int tn_eigensolve_dense(tn_ctx c, int N, const double* A, int lda, int k, double
 static int svd_common(tn_ctx c, int m, int n, const double* A, int lda, double* U, int ldu, double* s, double* Vt,
                       int ldvt, bool vectors) {
     if (!c || !A || !s || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     if (vectors && (!U || !Vt || ldu < m || ldvt < std::min(m, n))) return TN_BAD_ARG;
     Ctx& cx = c->c;
     const bool tall = m >= n;
@@ -683,6 +706,7 @@ int tn_svd_values(tn_ctx c, int m, int n, const double* A, int lda, double* s) {
 
 int tn_qr(tn_ctx c, int m, int n, const double* A, int lda, double* Q, int ldq, double* R, int ldr) {
     if (!c || !A || !Q || !R || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     const int k = std::min(m, n);
     if (ldq < m || ldr < k) return TN_BAD_ARG;
     Ctx& cx = c->c;
@@ -696,6 +720,7 @@ int tn_qr(tn_ctx c, int m, int n, const double* A, int lda, double* Q, int ldq, 
 
 int tn_lq(tn_ctx c, int m, int n, const double* A, int lda, double* L, int ldl, double* Q, int ldq) {
     if (!c || !A || !Q || !L || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     const int k = std::min(m, n);
     if (ldl < m || ldq < k) return TN_BAD_ARG;
     Ctx& cx = c->c;
@@ -715,6 +740,7 @@ int tn_lq(tn_ctx c, int m, int n, const double* A, int lda, double* L, int ldl, 
 // SVCompressorImp<T>::Compress (SVCompressorImp.C:19-73) on a device s vector.
 int tn_compress(tn_ctx c, int Dmax, double eps, int k, double* s, int* D_out, double* discarded) {
     if (!c || !s || k < 1 || !D_out) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     Ctx& cx = c->c;
     std::vector<double> h(k);
     TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
@@ -759,6 +785,7 @@ struct tn_dataset_s {
 
 int tn_mlp_create(tn_ctx c, uint64_t seed, tn_mlp* out) {
     if (!c || !out) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     auto* h = new tn_mlp_s();
     const int st = tnb::mlp_init(h->m, c->c, seed);
     if (st != TN_OK) {
@@ -771,6 +798,7 @@ int tn_mlp_create(tn_ctx c, uint64_t seed, tn_mlp* out) {
 
 int tn_mlp_destroy(tn_mlp m) {
     if (!m) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     delete m;
     return TN_OK;
 }
@@ -779,16 +807,19 @@ int tn_mlp_num_params(void) { return tnb::MLP_NP; }
 
 int tn_mlp_get_params(tn_mlp m, float* host) {
     if (!m || !host) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     return tnb::mlp_get_params(m->m, host);
 }
 
 int tn_mlp_set_params(tn_mlp m, const float* host) {
     if (!m || !host) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     return tnb::mlp_set_params(m->m, host);
 }
 
 int tn_mlp_forward(tn_mlp m, const float* F, long long n, float* Y) {
     if (!m || !F || !Y || n < 0) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     TN_CHECK(tnb::mlp_forward(m->m, F, n, Y, m->m.ctx->stream));
     TN_CUDA_CHECK(cudaStreamSynchronize(m->m.ctx->stream));
     return TN_OK;
@@ -796,18 +827,21 @@ int tn_mlp_forward(tn_mlp m, const float* F, long long n, float* Y) {
 
 int tn_mlp_gradient(tn_mlp m, const float* F, const float* T, long long n, float* grad_host, double* loss) {
     if (!m || !F || !T || !grad_host || n < 1) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     return tnb::mlp_gradient(m->m, F, T, n, grad_host, loss);
 }
 
 int tn_mlp_train(tn_mlp m, const float* F, const float* T, long long n, int steps, int batch, double lr,
                  uint64_t seed, double* final_loss) {
     if (!m || !F || !T || n < 1 || steps < 1 || !(lr > 0)) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
     if (n > 2000000000LL) return TN_BAD_SHAPE;
     return tnb::mlp_train(m->m, F, T, n, steps, batch, lr, seed, final_loss);
 }
 
 int tn_dataset_create(tn_ctx c, long long capacity, tn_dataset* out) {
     if (!c || !out || capacity < 1) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     auto* h = new tn_dataset_s();
     const int st = tnb::recorder_init(h->r, c->c, capacity);
     if (st != TN_OK) {
@@ -820,6 +854,7 @@ int tn_dataset_create(tn_ctx c, long long capacity, tn_dataset* out) {
 
 int tn_dataset_destroy(tn_dataset ds) {
     if (!ds) return TN_BAD_ARG;
+    TN_ON_DEVICE(ds->r.ctx->device);
     delete ds;
     return TN_OK;
 }
@@ -852,6 +887,7 @@ struct tn_itebd_s {
 
 int tn_itebd_create(tn_ctx c, double S, double Jxy, double Jz, double hz, int D, uint64_t seed, tn_itebd* out) {
     if (!c || !out || D < 1 || S <= 0) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
     auto* h = new tn_itebd_s();
     const int st = h->s.init(c->c, S, Jxy, Jz, hz, D, seed);
     if (st != TN_OK) {
@@ -864,12 +900,14 @@ int tn_itebd_create(tn_ctx c, double S, double Jxy, double Jz, double hz, int D,
 
 int tn_itebd_destroy(tn_itebd st) {
     if (!st) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
     delete st;
     return TN_OK;
 }
 
 int tn_itebd_get_site(tn_itebd st, int site, int* Dl, int* Dr, double* host) {
     if (!st || site < 0 || site > 1) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
     auto& s = st->s;
     const int l = s.dim(1 - site), r = s.dim(site);
     if (Dl) *Dl = l;
@@ -883,6 +921,7 @@ int tn_itebd_get_site(tn_itebd st, int site, int* Dl, int* Dr, double* host) {
 
 int tn_itebd_set_site(tn_itebd st, int site, int Dl, int Dr, const double* host) {
     if (!st || site < 0 || site > 1 || !host) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
     auto& s = st->s;
     if (Dl != s.dim(1 - site) || Dr != s.dim(site)) {
         tnb::set_error("tn_itebd_set_site: site %d is %d x %d (set the bond values first)", site, s.dim(1 - site),
@@ -905,6 +944,7 @@ int tn_itebd_get_bond(tn_itebd st, int bond, int* D, double* host) {
 
 int tn_itebd_set_bond(tn_itebd st, int bond, int D, const double* host) {
     if (!st || bond < 0 || bond > 1 || D < 1 || !host) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
     auto& s = st->s;
     s.lam_h[bond].assign(host, host + D);
     TN_CHECK(s.lam[bond].ensure(sizeof(double) * D));
@@ -915,39 +955,70 @@ int tn_itebd_set_bond(tn_itebd st, int bond, int D, const double* host) {
 
 int tn_itebd_step(tn_itebd st, double dt, int Dmax, int nsteps) {
     if (!st || Dmax < 1 || nsteps < 0) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
     for (int k = 0; k < nsteps; ++k) TN_CHECK(st->s.step2(dt, Dmax));
     return TN_OK;
 }
 
-int tn_itebd_find_ground_state(tn_itebd st, const double* dts, int ndt, int max_iter, int Dmax, double eps_factor,
-                               int* steps_out) {
-    if (!st || !dts || ndt < 1 || max_iter < 1 || Dmax < 1) return TN_BAD_ARG;
+// iTEBDStateImp::FindiTimeGroundState(H, iH, H2, line), iTEBDStateImp_iTime.C:44-104:
+// per schedule line (one dt each) OrthogonalizeI with eps dt^2/1000 (1e-13 at
+// dt = 0) and the current D as compressor, then for D = current .. Dmax in
+// steps of deltaD: bond dimensions grown to D (IncreaseBondDimensions), second-
+// order Trotter steps until both bond vectors move by at most eps_factor*dt
+// (or max_iter steps), OrthogonalizeI again.  steps_out[l] = Trotter steps of line l.
+int tn_itebd_find_ground_state(tn_itebd st, const double* dts, int ndt, int max_iter, int Dmax, int deltaD,
+                               double eps_factor, int* steps_out) {
+    if (!st || !dts || ndt < 1 || max_iter < 1 || Dmax < 1 || deltaD < 1) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
     auto& s = st->s;
+    constexpr int ORTH_ITER = 100;  // nOrthIter, iTEBDStateImp_iTime.C:57
     for (int l = 0; l < ndt; ++l) {
         const double dt = dts[l];
-        int n = 0;
-        for (n = 1; n <= max_iter; ++n) {
-            const std::vector<double> old0 = s.lam_h[0], old1 = s.lam_h[1];
-            TN_CHECK(s.step2(dt, Dmax));
-            double dl = 0;
-            for (int b = 0; b < 2; ++b) {
-                const auto& o = b == 0 ? old0 : old1;
-                const auto& x = s.lam_h[b];
-                if (o.size() != x.size()) {
-                    dl = 1.0;
-                    continue;
+        const double eps_orth = dt == 0.0 ? 1e-13 : dt * dt / 1000.0;
+        int Dcur = std::max(s.dim(0), s.dim(1));
+        TN_CHECK(s.orthogonalize_i(Dcur, eps_orth, ORTH_ITER, nullptr, nullptr, nullptr));
+        int total = 0;
+        for (int D = Dcur; D <= Dmax; D += deltaD) {
+            if (D > Dcur) TN_CHECK(s.grow(D));
+            for (int n = 1; n <= max_iter; ++n) {
+                const std::vector<double> old0 = s.lam_h[0], old1 = s.lam_h[1];
+                TN_CHECK(s.step2(dt, D));
+                ++total;
+                double dl = 0;
+                for (int b = 0; b < 2; ++b) {
+                    const auto& o = b == 0 ? old0 : old1;
+                    const auto& x = s.lam_h[b];
+                    if (o.size() != x.size()) {
+                        dl = 1.0;
+                        continue;
+                    }
+                    for (size_t i = 0; i < x.size(); ++i) dl = std::max(dl, std::fabs(o[i] - x[i]));
                 }
-                for (size_t i = 0; i < x.size(); ++i) dl = std::max(dl, std::fabs(o[i] - x[i]));
+                if (dl <= eps_factor * dt) break;
             }
-            if (dl <= eps_factor * dt) break;
+            TN_CHECK(s.orthogonalize_i(D, eps_orth, ORTH_ITER, nullptr, nullptr, nullptr));
+            Dcur = D;
         }
-        if (steps_out) steps_out[l] = std::min(n, max_iter);
+        if (steps_out) steps_out[l] = total;
+    }
+    return TN_OK;
+}
+
+int tn_itebd_orthogonalize(tn_itebd st, int Dmax, double eps, int max_iter, double* delta, int* iters) {
+    if (!st || Dmax < 1 || !(eps > 0) || max_iter < 1) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
+    bool bailed = false;
+    TN_CHECK(st->s.orthogonalize_i(Dmax, eps, max_iter, delta, iters, &bailed));
+    if (bailed) {
+        tnb::set_error("OrthogonalizeI: singular norm matrix, iteration abandoned (state unpacked as it stood)");
+        return TN_NOT_CONVERGED;
     }
     return TN_OK;
 }
 
 int tn_itebd_energy(tn_itebd st, int max_iters, double tol, double* E) {
     if (!st || !E || max_iters < 1) return TN_BAD_ARG;
+    TN_ON_DEVICE(st->s.ctx->device);
     return st->s.energy(E, max_iters, tol);
 }
 

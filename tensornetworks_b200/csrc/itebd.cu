@@ -139,6 +139,76 @@ __global__ void maxdiff_kernel(const double* __restrict__ x, const double* __res
     }
 }
 
+// M(i + D na, j + D nb) = lB[i] gam[na + d nb](i, j) lB[j]   (ReshapeForSVD of lambdaB gamma lambdaB)
+__global__ void gamma_reshape_kernel(const double* __restrict__ gam, int d, int D, const double* __restrict__ lB,
+                                     double* __restrict__ M) {
+    const int m = d * D;
+    const long long total = (long long)m * m;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e % m), c = (int)(e / m);
+        const int i = r % D, na = r / D, j = c % D, nb = c / D;
+        M[e] = lB[i] * gam[(size_t)(na + d * nb) * D * D + (size_t)j * D + i] * lB[j];
+    }
+}
+
+// out = {Vr(0,0), Vl(0,0), min_i |Vr(i,i)|, min_i |Vl(i,i)|} (one block)
+__global__ void norm_stats_kernel(const double* __restrict__ Vr, const double* __restrict__ Vl, int D, double* out) {
+    __shared__ double sr[32], sl[32];
+    double mr = 1e300, ml = 1e300;
+    for (int i = threadIdx.x; i < D; i += blockDim.x) {
+        mr = fmin(mr, fabs(Vr[(size_t)i * D + i]));
+        ml = fmin(ml, fabs(Vl[(size_t)i * D + i]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mr = fmin(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+        ml = fmin(ml, __shfl_xor_sync(0xffffffffu, ml, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sr[threadIdx.x >> 5] = mr;
+        sl[threadIdx.x >> 5] = ml;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            mr = fmin(mr, sr[w]);
+            ml = fmin(ml, sl[w]);
+        }
+        out[0] = Vr[0];
+        out[1] = Vl[0];
+        out[2] = fmin(mr, sr[0]);
+        out[3] = fmin(ml, sl[0]);
+    }
+}
+
+// sq = sqrt(s), isq = 1/sqrt(s) for both factors; flag[0] = 1 when a value is not positive
+__global__ void sqrt_pair_kernel(const double* __restrict__ sr, const double* __restrict__ sl, int D,
+                                 double* __restrict__ out, double* flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D; i += gridDim.x * blockDim.x) {
+        const double a = sr[i], b = sl[i];
+        if (!(a > 1e-300) || !(b > 1e-300)) *flag = 1.0;
+        out[i] = sqrt(a);
+        out[D + i] = 1.0 / sqrt(a);
+        out[2 * D + i] = sqrt(b);
+        out[3 * D + i] = 1.0 / sqrt(b);
+    }
+}
+
+__global__ void scal_kernel(double* __restrict__ x, long long n, double a) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        x[e] *= a;
+}
+
+// dst[n](i, j) = src[n](i, j) for i < Dl, j < Dr, else 0; dst is (d, D1, D2)
+__global__ void pad_kernel(const double* __restrict__ src, int d, int Dl, int Dr, double* __restrict__ dst, int D1,
+                           int D2) {
+    const long long total = (long long)d * D1 * D2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % D1), j = (int)((e / D1) % D2), n = (int)(e / ((long long)D1 * D2));
+        dst[e] = (i < Dl && j < Dr) ? src[(size_t)n * Dl * Dr + (size_t)j * Dl + i] : 0.0;
+    }
+}
+
 // Symmetric eigen-decomposition by cyclic Jacobi (host, n <= 36): A = Q diag(w) Q^T.
 void jacobi_eigh_host(std::vector<double> A, int n, std::vector<double>& w, std::vector<double>& Q) {
     Q.assign((size_t)n * n, 0.0);
@@ -273,6 +343,19 @@ int ITebdState::apply_gate(int bond, int Dmax, double eps) {
     gate_reshape_kernel<<<g1d((long long)m * m), 256, 0, st>>>(TH.as<double>(), d, Dl, gate.as<double>(),
                                                                M.as<double>());
     TN_LAUNCH_CHECK();
+    TN_CHECK(svd_unpack(bond, Dl, Dmax, eps));
+    ++gates_applied;
+    return TN_OK;
+}
+
+int ITebdState::svd_unpack(int bond, int Dl, int Dmax, double eps) {
+    cudaStream_t st = ctx->stream;
+    const int A = bond, B = 1 - bond;
+    const int m = d * Dl;
+    TN_CHECK(U.ensure(sizeof(double) * (size_t)m * m));
+    TN_CHECK(Vt.ensure(sizeof(double) * (size_t)m * m));
+    TN_CHECK(V.ensure(sizeof(double) * (size_t)m * m));
+    TN_CHECK(s.ensure(sizeof(double) * (size_t)m));
     SvdJob job{M.as<double>(), m, m, V.as<double>(), U.as<double>(), m, Vt.as<double>(), m, s.as<double>(), nullptr};
     TN_CHECK(svd_batched(*ctx, {job}, true));
     // SVCompressor rule on the host (a few values), then lambda normalised
@@ -310,7 +393,6 @@ int ITebdState::apply_gate(int bond, int Dmax, double eps) {
     TN_CUDA_CHECK(cudaMemcpyAsync(G[A].p, GA, sizeof(double) * (size_t)d * Dl * keep, cudaMemcpyDeviceToDevice, st));
     TN_CUDA_CHECK(cudaMemcpyAsync(G[B].p, GB, sizeof(double) * (size_t)d * Dl * keep, cudaMemcpyDeviceToDevice, st));
     TN_CUDA_CHECK(cudaStreamSynchronize(st));
-    ++gates_applied;
     return TN_OK;
 }
 
@@ -321,6 +403,235 @@ int ITebdState::step2(double dt, int Dmax) {
     TN_CHECK(apply_gate(1, Dmax, 1e-16));
     TN_CHECK(set_gate(0.5 * dt));
     TN_CHECK(apply_gate(0, Dmax, 1e-16));
+    return TN_OK;
+}
+
+// iTEBDStateImp::OrthogonalizeI(comp, eps, niter), iTEBDStateImp_OrthoNorm.C:110-128,
+// with the iteration of :511-637 (Phien, McCulloch, Vidal, PRB 91, 115137):
+//   gamma[na + d nb] = GA[na] lA GB[nb]                  (ContractAlB)
+//   repeat: Vr = sum_n (g_n l)(g_n l)^T, Vl = sum_n (l g_n)^T (l g_n) (GetNormMatrix),
+//           bail when a diagonal is below 1e-10, Vr /= Vr(0,0), Vl /= Vl(0,0),
+//           g /= sqrt(Vl(0,0)), Vr = X X^T, Vl = Yd Yd^T (Factor), SVD of
+//           Yd^T l X = U l' VT, l' normalised, g_n = (VT X^-1) g_n (Yd^-T U),
+//           until max |l - l'| < eps;  g /= sqrt(Vr(0,0))
+//   lambdaB = l (normalised), then UnpackOrthonormal: lB g lB reshaped and
+//   SVD-split into GA lA GB with the (Dmax, 1e-16) compressor.
+// Factor takes the eigen-decomposition of the symmetric positive matrix; here
+// it is the Jacobi SVD of that matrix (the same U and values), so the FP64
+// rotations stay on the device.
+int ITebdState::orthogonalize_i(int Dmax, double eps, int max_iter, double* delta, int* iters, bool* bailed) {
+    cudaStream_t st = ctx->stream;
+    const int D = dim(1), Dm = dim(0);
+    const int dd = d * d;
+    const size_t D2 = (size_t)D * D, nG = (size_t)dd * D2;
+    if (delta) *delta = 0;
+    if (iters) *iters = 0;
+    if (bailed) *bailed = false;
+    // workspace
+    const size_t need = 2 * nG + 20 * D2 + 12 * (size_t)D + 16;
+    TN_CHECK(og.ensure(sizeof(double) * need));
+    double* gam = og.as<double>();
+    double* tmp = gam + nG;
+    double* Vr = tmp + nG;
+    double* Vl = Vr + D2;
+    double* Wr = Vl + D2;
+    double* Wl = Wr + D2;
+    double* Vwr = Wl + D2;
+    double* Vwl = Vwr + D2;
+    double* Ur = Vwl + D2;
+    double* Ul = Ur + D2;
+    double* Vtr = Ul + D2;
+    double* Vtl = Vtr + D2;
+    double* Z = Vtl + D2;
+    double* Ys = Z + D2;
+    double* YlX = Ys + D2;
+    double* Vwy = YlX + D2;
+    double* Up = Vwy + D2;
+    double* VTp = Up + D2;
+    double* Ri = VTp + D2;
+    double* Li = Ri + D2;
+    double* VX = Li + D2;
+    double* YU = VX + D2;
+    double* sr = YU + D2;
+    double* sl = sr + D;
+    double* sqv = sl + D;          // 4 D: sqrt(sr), 1/sqrt(sr), sqrt(sl), 1/sqrt(sl)
+    double* lp = sqv + 4 * (size_t)D;
+    double* lamv = lp + D;
+    double* stats = lamv + D;      // 8 values
+    auto gemm = [&](int M_, int N_, int K_, const double* a, IdxMap amn, IdxMap ak, const double* b, IdxMap bk,
+                    IdxMap bmn, double* c) {
+        GemmArgs g;
+        g.M = M_; g.N = N_; g.K = K_;
+        g.A.ptr = a; g.A.mn = amn; g.A.k = ak;
+        g.B.ptr = b; g.B.k = bk; g.B.mn = bmn;
+        g.C.ptr = c; g.C.m = idx(1); g.C.n = idx(M_);
+        return gemm_f64(g, st);
+    };
+    // gamma[na + d nb] = (GA[na] lA) GB[nb]
+    TN_CHECK(X.ensure(sizeof(double) * (size_t)d * D * Dm));
+    scale_kernel<<<g1d((long long)d * D * Dm), 256, 0, st>>>(G[0].as<double>(), d, D, Dm, nullptr,
+                                                             lam[0].as<double>(), X.as<double>());
+    TN_LAUNCH_CHECK();
+    {
+        GemmArgs g;
+        g.M = D; g.N = D; g.K = Dm; g.nb0 = d; g.nb1 = d;
+        g.A.ptr = X.as<double>(); g.A.mn = idx(1); g.A.k = idx(D); g.A.sb0 = (long long)D * Dm; g.A.sb1 = 0;
+        g.B.ptr = G[1].as<double>(); g.B.k = idx(1); g.B.mn = idx(Dm); g.B.sb0 = 0; g.B.sb1 = (long long)Dm * D;
+        g.C.ptr = gam; g.C.m = idx(1); g.C.n = idx(D); g.C.sb0 = (long long)D2; g.C.sb1 = (long long)d * D2;
+        TN_CHECK(gemm_f64(g, st));
+    }
+    TN_CUDA_CHECK(cudaMemcpyAsync(lamv, lam[1].p, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+    double er = 1.0;
+    bool bail = false;
+    int it = 0;
+    double dl = 0.0;
+    for (it = 0; it < max_iter; ++it) {
+        // norm matrices
+        scale_kernel<<<g1d((long long)nG), 256, 0, st>>>(gam, dd, D, D, nullptr, lamv, tmp);
+        TN_LAUNCH_CHECK();
+        TN_CHECK(gemm(D, D, dd * D, tmp, idx(1), idx2(D, D, (long long)D2), tmp, idx2(D, D, (long long)D2), idx(1), Vr));
+        scale_kernel<<<g1d((long long)nG), 256, 0, st>>>(gam, dd, D, D, lamv, nullptr, tmp);
+        TN_LAUNCH_CHECK();
+        TN_CHECK(gemm(D, D, dd * D, tmp, idx(D), idx2(1, D, (long long)D2), tmp, idx2(1, D, (long long)D2), idx(D), Vl));
+        norm_stats_kernel<<<1, 256, 0, st>>>(Vr, Vl, D, stats);
+        TN_LAUNCH_CHECK();
+        double hs[4];
+        TN_CUDA_CHECK(cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, st));
+        TN_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (!(hs[2] >= 1e-10) || !(hs[3] >= 1e-10)) {  // singular: bail out (as :547-554)
+            bail = true;
+            break;
+        }
+        er = hs[0];
+        const double el = hs[1];
+        scal_kernel<<<g1d((long long)D2), 256, 0, st>>>(Vr, (long long)D2, 1.0 / er);
+        TN_LAUNCH_CHECK();
+        scal_kernel<<<g1d((long long)D2), 256, 0, st>>>(Vl, (long long)D2, 1.0 / el);
+        TN_LAUNCH_CHECK();
+        scal_kernel<<<g1d((long long)nG), 256, 0, st>>>(gam, (long long)nG, 1.0 / std::sqrt(el));
+        TN_LAUNCH_CHECK();
+        // Factor: Vr = Ur sr Ur^T, Vl = Ul sl Ul^T
+        TN_CUDA_CHECK(cudaMemcpyAsync(Wr, Vr, sizeof(double) * D2, cudaMemcpyDeviceToDevice, st));
+        TN_CUDA_CHECK(cudaMemcpyAsync(Wl, Vl, sizeof(double) * D2, cudaMemcpyDeviceToDevice, st));
+        TN_CUDA_CHECK(cudaMemsetAsync(stats + 4, 0, sizeof(double), st));
+        {
+            SvdJob jr{Wr, D, D, Vwr, Ur, D, Vtr, D, sr, nullptr};
+            SvdJob jl{Wl, D, D, Vwl, Ul, D, Vtl, D, sl, nullptr};
+            TN_CHECK(svd_batched(*ctx, {jr, jl}, true));
+        }
+        sqrt_pair_kernel<<<(D + 255) / 256, 256, 0, st>>>(sr, sl, D, sqv, stats + 4);
+        TN_LAUNCH_CHECK();
+        double flag = 0;
+        TN_CUDA_CHECK(cudaMemcpyAsync(&flag, stats + 4, sizeof(double), cudaMemcpyDeviceToHost, st));
+        TN_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (flag != 0.0) {  // a singular factor (the reference's isnan(X) / isnan(Yd) bail-out)
+            bail = true;
+            break;
+        }
+        const double* sqr = sqv;
+        const double* isqr = sqv + D;
+        const double* sql = sqv + 2 * D;
+        const double* isql = sqv + 3 * D;
+        // Z = l X = l Ur sqrt(sr);  Ys = Yd = Ul sqrt(sl);  YlX = Ys^T Z
+        scale_kernel<<<g1d((long long)D2), 256, 0, st>>>(Ur, 1, D, D, lamv, sqr, Z);
+        TN_LAUNCH_CHECK();
+        scale_kernel<<<g1d((long long)D2), 256, 0, st>>>(Ul, 1, D, D, nullptr, sql, Ys);
+        TN_LAUNCH_CHECK();
+        TN_CHECK(gemm(D, D, D, Ys, idx(D), idx(1), Z, idx(1), idx(D), YlX));
+        {
+            SvdJob jy{YlX, D, D, Vwy, Up, D, VTp, D, lp, nullptr};
+            TN_CHECK(svd_batched(*ctx, {jy}, true));
+        }
+        normalize_kernel<<<1, 256, 0, st>>>(lp, D, nullptr);
+        TN_LAUNCH_CHECK();
+        // VX = VT X^-1 = VTp (Ur / sqrt(sr))^T ;  YU = Yd^-T U = (Ul / sqrt(sl)) Up
+        scale_kernel<<<g1d((long long)D2), 256, 0, st>>>(Ur, 1, D, D, nullptr, isqr, Ri);
+        TN_LAUNCH_CHECK();
+        scale_kernel<<<g1d((long long)D2), 256, 0, st>>>(Ul, 1, D, D, nullptr, isql, Li);
+        TN_LAUNCH_CHECK();
+        TN_CHECK(gemm(D, D, D, VTp, idx(1), idx(D), Ri, idx(D), idx(1), VX));
+        TN_CHECK(gemm(D, D, D, Li, idx(1), idx(D), Up, idx(1), idx(D), YU));
+        {
+            GemmArgs g;  // tmp_n = VX gam_n
+            g.M = D; g.N = D; g.K = D; g.nb0 = dd;
+            g.A.ptr = VX; g.A.mn = idx(1); g.A.k = idx(D);
+            g.B.ptr = gam; g.B.k = idx(1); g.B.mn = idx(D); g.B.sb0 = (long long)D2;
+            g.C.ptr = tmp; g.C.m = idx(1); g.C.n = idx(D); g.C.sb0 = (long long)D2;
+            TN_CHECK(gemm_f64(g, st));
+            GemmArgs h;  // gam_n = tmp_n YU
+            h.M = D; h.N = D; h.K = D; h.nb0 = dd;
+            h.A.ptr = tmp; h.A.mn = idx(1); h.A.k = idx(D); h.A.sb0 = (long long)D2;
+            h.B.ptr = YU; h.B.k = idx(1); h.B.mn = idx(D);
+            h.C.ptr = gam; h.C.m = idx(1); h.C.n = idx(D); h.C.sb0 = (long long)D2;
+            TN_CHECK(gemm_f64(h, st));
+        }
+        maxdiff_kernel<<<1, 256, 0, st>>>(lamv, lp, D, stats + 5);
+        TN_LAUNCH_CHECK();
+        TN_CUDA_CHECK(cudaMemcpyAsync(lamv, lp, sizeof(double) * D, cudaMemcpyDeviceToDevice, st));
+        TN_CUDA_CHECK(cudaMemcpyAsync(&dl, stats + 5, sizeof(double), cudaMemcpyDeviceToHost, st));
+        TN_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (dl < eps) {
+            ++it;
+            break;
+        }
+    }
+    if (!bail) {
+        scal_kernel<<<g1d((long long)nG), 256, 0, st>>>(gam, (long long)nG, 1.0 / std::sqrt(er));
+        TN_LAUNCH_CHECK();
+    }
+    if (delta) *delta = dl;
+    if (iters) *iters = it;
+    if (bailed) *bailed = bail;
+    // lambdaB = l / |l| (Bond::SetSingularValues)
+    std::vector<double> hl(D);
+    TN_CUDA_CHECK(cudaMemcpyAsync(hl.data(), lamv, sizeof(double) * D, cudaMemcpyDeviceToHost, st));
+    TN_CUDA_CHECK(cudaStreamSynchronize(st));
+    double nrm = 0;
+    for (double x : hl) nrm += x * x;
+    nrm = std::sqrt(nrm);
+    for (double& x : hl) x /= nrm;
+    lam_h[1] = hl;
+    TN_CUDA_CHECK(cudaMemcpyAsync(lam[1].p, hl.data(), sizeof(double) * D, cudaMemcpyHostToDevice, st));
+    // UnpackOrthonormal
+    const int m = d * D;
+    TN_CHECK(M.ensure(sizeof(double) * (size_t)m * m));
+    gamma_reshape_kernel<<<g1d((long long)m * m), 256, 0, st>>>(gam, d, D, lam[1].as<double>(), M.as<double>());
+    TN_LAUNCH_CHECK();
+    return svd_unpack(0, D, Dmax, 1e-16);
+}
+
+int ITebdState::grow(int D) {
+    cudaStream_t st = ctx->stream;
+    const int old[2] = {dim(0), dim(1)};
+    if (old[0] >= D && old[1] >= D) return TN_OK;
+    // Gammas: site 0 is (d, dim 1, dim 0), site 1 is (d, dim 0, dim 1); zero-padded to (d, D, D)
+    for (int site = 0; site < 2; ++site) {
+        const int Dl = site == 0 ? old[1] : old[0];
+        const int Dr = site == 0 ? old[0] : old[1];
+        const int N1 = std::max(D, Dl), N2 = std::max(D, Dr);
+        TN_CHECK(work.ensure(sizeof(double) * (size_t)d * N1 * N2));
+        pad_kernel<<<g1d((long long)d * N1 * N2), 256, 0, st>>>(G[site].as<double>(), d, Dl, Dr, work.as<double>(),
+                                                                N1, N2);
+        TN_LAUNCH_CHECK();
+        TN_CUDA_CHECK(cudaStreamSynchronize(st));
+        TN_CHECK(G[site].ensure(sizeof(double) * (size_t)d * N1 * N2));
+        TN_CUDA_CHECK(cudaMemcpyAsync(G[site].p, work.p, sizeof(double) * (size_t)d * N1 * N2,
+                                      cudaMemcpyDeviceToDevice, st));
+    }
+    // bond values: padded with min/10, renormalised (Bond::NewBondDimension, Bond.C:60-84)
+    for (int b = 0; b < 2; ++b) {
+        auto& l = lam_h[b];
+        if ((int)l.size() >= D) continue;
+        const double fill = *std::min_element(l.begin(), l.end()) / 10.0;
+        l.resize(D, fill);
+        double nrm = 0;
+        for (double x : l) nrm += x * x;
+        nrm = std::sqrt(nrm);
+        for (double& x : l) x /= nrm;
+        TN_CHECK(lam[b].ensure(sizeof(double) * D));
+        TN_CUDA_CHECK(cudaMemcpyAsync(lam[b].p, l.data(), sizeof(double) * D, cudaMemcpyHostToDevice, st));
+    }
+    TN_CUDA_CHECK(cudaStreamSynchronize(st));
     return TN_OK;
 }
 

@@ -19,6 +19,7 @@ struct ITebdState {
     std::vector<double> lam_h[2];
     DevBuf gate;                 // exp(-dt h), d^2 x d^2 (symmetric)
     DevBuf X, Y, TH, M, U, Vt, V, s, work;
+    DevBuf og;                   // OrthogonalizeI workspace
     std::vector<double> h12;     // two-site Hamiltonian, rows (ma d + mb), columns (na d + nb)
     long long gates_applied = 0;
 
@@ -31,6 +32,16 @@ struct ITebdState {
     // second-order Trotter step: gates dt/2, dt, dt/2 on bonds 0, 1, 0; eps-only
     // compression (1e-7) on the first, Dmax on the last two
     int step2(double dt, int Dmax);
+    // SVD of the (d Dl) x (d Dl) matrix in M, SVCompressor rule (Dmax, eps),
+    // new bond values on `bond`, Gammas unpacked with the other bond's values
+    int svd_unpack(int bond, int Dl, int Dmax, double eps);
+    // OrthogonalizeI at centre 1 (the iterative re-orthogonalisation); the
+    // largest change of the bond values in the last iteration in *delta, the
+    // iterations run in *iters, *bailed when the norm matrices were singular
+    int orthogonalize_i(int Dmax, double eps, int max_iter, double* delta, int* iters, bool* bailed);
+    // IncreaseBondDimensions: Gammas zero-padded to D x D, bond values padded
+    // with min/10 and renormalised
+    int grow(int D);
     // energy per bond from the unit-cell transfer-matrix fixed points
     int energy(double* E, int max_iters, double tol);
 };

@@ -3,11 +3,13 @@
 // the call allocates no memory at all.
 //
 // The scratch is one file-scope __device__ array per device.  The first call
-// on a device looks up its address (cudaGetSymbolAddress with that device
-// current) and caches it; later calls only enqueue copies and kernels.  The
+// through a context on a device makes that device current, looks up its
+// copy's address (cudaGetSymbolAddress) and caches it per device ordinal;
+// later calls only enqueue copies and kernels on the context's stream.  The
 // kernel chain is the one of tn_heff_matvec (stage-1 GEMM, sparse MPO
 // combination, split stage-3 GEMM, deterministic slab sum): it writes every
 // scratch element it reads, so nothing has to start at zero.
+#include <algorithm>
 #include <array>
 #include <cstring>
 #include <mutex>
@@ -26,9 +28,10 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 double* g_scratch_ptr[MAX_DEVICES] = {};
 
-int scratch_for_current_device(double** out) {
-    int dev = 0;
-    TN_CUDA_CHECK(cudaGetDevice(&dev));
+// Address of this device's copy of the array.  The caller has made `dev`
+// current: the symbol address is per device, and a kernel given another
+// device's copy would run on the wrong memory.
+int scratch_for_device(int dev, double** out) {
     if (dev < 0 || dev >= MAX_DEVICES) {
         set_error("tn_heff_matvec_static: device ordinal %d out of range", dev);
         return TN_BAD_ARG;
@@ -57,6 +60,19 @@ extern "C" int tn_heff_matvec_static(tn_ctx c, int d, int Dw1, int Dw2, int D1, 
     if (!c || !W_host || !F || !G || !x || !y) return TN_BAD_ARG;
     if (d < 1 || Dw1 < 1 || Dw2 < 1 || D1 < 1 || D2 < 1) return TN_BAD_SHAPE;
     Ctx& cx = c->c;
+    // Bound every dimension before any product is formed (no size_t wrap-around
+    // can then slip past the capacity check) and before the term loop reads W.
+    {
+        const double Dm = (double)std::max(D1, D2), Dw = (double)std::max(Dw1, Dw2);
+        const double stage = (double)d * Dw * Dm * Dm;
+        const double nterm_max = (double)d * d * Dw1 * Dw2 + (double)d * Dw2;
+        if (stage * 2.0 + nterm_max * 2.0 > (double)STATIC_SCRATCH_DOUBLES) {
+            set_error("tn_heff_matvec_static: shape d=%d Dw=%dx%d D=%dx%d needs about %.0f doubles of scratch, the "
+                      "static scratch holds %zu",
+                      d, Dw1, Dw2, D1, D2, stage * 2.0, STATIC_SCRATCH_DOUBLES);
+            return TN_BAD_SHAPE;
+        }
+    }
     // MPO term list (left-to-right slab form) in a fixed host array
     std::array<WTermDev, STATIC_MAX_TERMS> terms;
     int nt = 0;
@@ -93,8 +109,9 @@ extern "C" int tn_heff_matvec_static(tn_ctx c, int d, int Dw1, int Dw2, int D1, 
                   d, Dw1, Dw2, D1, D2, need, STATIC_SCRATCH_DOUBLES);
         return TN_BAD_SHAPE;
     }
+    TN_ON_DEVICE(cx.device);
     double* base = nullptr;
-    TN_CHECK(scratch_for_current_device(&base));
+    TN_CHECK(scratch_for_device(cx.device, &base));
     WTermDev* tdev = reinterpret_cast<WTermDev*>(base);
     double* P = base + term_doubles;
     double* Q = P + stage;

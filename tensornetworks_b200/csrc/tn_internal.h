@@ -30,6 +30,36 @@ void set_error(const char* fmt, ...);
         if (s_ != TN_OK) return s_;   \
     } while (0)
 
+// Makes a handle's device current for the length of one C-ABI call and gives
+// the calling thread its own device back on return, so that a context made on
+// GPU k is used on GPU k whatever device the caller has selected.
+struct DeviceGuard {
+    int prev = -1;
+    bool restore = false;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != dev) {
+            err = cudaSetDevice(dev);
+            restore = (err == cudaSuccess);
+        }
+    }
+    ~DeviceGuard() {
+        if (restore) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+#define TN_ON_DEVICE(dev)                                                                          \
+    ::tnb::DeviceGuard tn_dev_guard_(dev);                                                         \
+    do {                                                                                           \
+        if (tn_dev_guard_.err != cudaSuccess) {                                                    \
+            ::tnb::set_error("cannot make device %d current: %s", (int)(dev),                      \
+                             cudaGetErrorString(tn_dev_guard_.err));                               \
+            return TN_CUDA_ERROR;                                                                  \
+        }                                                                                          \
+    } while (0)
+
 // Every launch site calls TN_LAUNCH_CHECK once per kernel launch: it checks the
 // launch and counts it (tn_launch_count).
 void count_launch();

@@ -38,13 +38,29 @@ def run_gpu(T, L, S, Dstart, lines, form=2, seed=1234, hz=0.0, **opt):
 
 @pytest.mark.parametrize("L,S,Dfinal,Eexp,E2exp", [
     (2, 0.5, 2, -0.750000000000000, 1e-13),
+    (2, 1.0, 3, -2.000000000000000, 1e-13),
+    (2, 1.5, 4, -3.750000000000000, 1e-13),
+    (2, 2.0, 5, -6.000000000000000, 1e-13),
+    (2, 2.5, 6, -8.750000000000000, 1e-13),
+    (3, 0.5, 2, -0.500000000000000, 1e-13),
     (3, 1.0, 3, -1.500000000000000, 1e-13),
+    (3, 1.5, 4, -3.000000000000000, 1e-13),
+    (3, 2.0, 5, -5.000000000000000, 2e-13),
+    (3, 2.5, 6, -7.500000000000000, 1e-12),
     (4, 0.5, 4, -0.538675134594813, 1e-13),
+    (4, 1.0, 9, -1.548583770354863, 1e-13),
+    (5, 0.5, 4, -0.481971563329499, 1e-13),
+    (6, 0.5, 8, -0.498715426777585, 1e-13),
     (7, 0.5, 8, -0.472706613447776, 1e-13),
+    (8, 0.5, 8, -0.482132838467071, 2e-05),
     (10, 0.5, 8, -0.473113399629092, 5e-05),
+    (16, 0.5, 8, -0.460770570536169, 5e-04),
 ])
 def test_golden_pytn(T, L, S, Dfinal, Eexp, E2exp):
-    """test_Unittest1.py:4-45 through the same API calls."""
+    """Every row of test_Unittest1.py:4-24 (Dstart 2, grown by 1 to Dfinal,
+    epsilons 1e-12, 100 sweeps at most) through the same API calls, with the
+    reference's own bounds: |E/(L-1) - Eexpected| <= 1e-11 and variance below
+    E2expected."""
     E, var, psi, H = run_gpu(T, L, S, 2, [(100, Dfinal, 1, E12, E12, E12)])
     assert abs(E / (L - 1) - Eexp) <= 1e-11
     assert var < E2exp

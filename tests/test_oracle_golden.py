@@ -15,14 +15,22 @@ E12 = 1e-12
 @pytest.mark.parametrize("L,S,Dfinal,Eexp,E2exp", [
     (2, 0.5, 2, -0.750000000000000, 1e-13),
     (2, 1.0, 3, -2.000000000000000, 1e-13),
+    (2, 1.5, 4, -3.750000000000000, 1e-13),
+    (2, 2.0, 5, -6.000000000000000, 1e-13),
+    (2, 2.5, 6, -8.750000000000000, 1e-13),
     (3, 0.5, 2, -0.500000000000000, 1e-13),
     (3, 1.0, 3, -1.500000000000000, 1e-13),
+    (3, 1.5, 4, -3.000000000000000, 1e-13),
+    (3, 2.0, 5, -5.000000000000000, 2e-13),
+    (3, 2.5, 6, -7.500000000000000, 1e-12),
     (4, 0.5, 4, -0.538675134594813, 1e-13),
+    (4, 1.0, 9, -1.548583770354863, 1e-13),
     (5, 0.5, 4, -0.481971563329499, 1e-13),
     (6, 0.5, 8, -0.498715426777585, 1e-13),
     (7, 0.5, 8, -0.472706613447776, 1e-13),
     (8, 0.5, 8, -0.482132838467071, 2e-05),
     (10, 0.5, 8, -0.473113399629092, 5e-05),
+    (16, 0.5, 8, -0.460770570536169, 5e-04),
 ])
 def test_variational_golden_pytn(oracle, L, S, Dfinal, Eexp, E2exp):
     r = oracle.find_ground_state(L, S, 2, [(100, Dfinal, 1, E12, E12, E12)], eig_mode=0, gauge=0)

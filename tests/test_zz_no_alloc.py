@@ -1,6 +1,9 @@
 """tn_heff_matvec_static (static device scratch, no allocation) against the
-allocating tn_heff_matvec in FP64.  Collected last on purpose: it must pass
-both alone and after every other test has used the library.
+allocating tn_heff_matvec in FP64.  The entry point exists for callers that
+cannot call cudaMalloc (their device memory is held by another allocator's
+fixed pool, or their solver loop cannot take cudaMalloc's device-wide
+synchronisation).  Collected last on purpose: it must pass both alone and
+after every other test has used the library.
 
 Tolerance: 1e-13 normwise relative (the same FP64 kernel chain runs in both;
 the only difference is where its scratch lives)."""
@@ -65,3 +68,44 @@ def test_static_matvec_rejects_oversize(T, ctx, oracle):
     st = ctx._lib.tn_heff_matvec_static(ctx.handle, 2, 5, 5, 256, 256, W.ctypes.data, p, p, p, p)
     assert st == 2  # TN_BAD_SHAPE
     assert "static" in T._capi.last_error()
+
+
+def test_static_matvec_allocates_nothing(T, oracle):
+    """Through a context of its own (no context buffers to fall back on), two
+    calls in a row leave the device's free memory exactly as it was, and both
+    agree with the allocating entry point run afterwards on the default
+    context."""
+    import torch
+    d, D1, D2, Dw = 2, 160, 160, 5
+    rng = np.random.default_rng(77)
+    W = np.ascontiguousarray(oracle.mpo_site(10, 0.5, 2, 1.0, 1.0, 0.1, 5).ravel())
+    F, G = dev(rng.uniform(-1, 1, Dw * D1 * D1)), dev(rng.uniform(-1, 1, Dw * D2 * D2))
+    xs = [dev(rng.uniform(-1, 1, d * D1 * D2)) for _ in range(2)]
+    ys = [torch.full_like(xs[0], float("nan")) for _ in range(2)]
+    own = T.Context(0)
+    try:
+        lib = own._lib
+        # warm-up on another array pair: the first call on a device looks up the array's address
+        w = torch.zeros_like(xs[0])
+        T._capi.check(lib.tn_heff_matvec_static(own.handle, d, Dw, Dw, D1, D2, W.ctypes.data, F.data_ptr(),
+                                                G.data_ptr(), xs[0].data_ptr(), w.data_ptr()), "warm-up")
+        own.synchronize()
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        for x, y in zip(xs, ys):
+            T._capi.check(lib.tn_heff_matvec_static(own.handle, d, Dw, Dw, D1, D2, W.ctypes.data, F.data_ptr(),
+                                                    G.data_ptr(), x.data_ptr(), y.data_ptr()),
+                          "tn_heff_matvec_static")
+            own.synchronize()
+        free1 = torch.cuda.mem_get_info()[0]
+        assert free1 == free0, (free0, free1)
+    finally:
+        own.close()
+    ctx = T.default_context()
+    for x, y in zip(xs, ys):
+        y_ref = torch.zeros_like(x)
+        T._capi.check(ctx._lib.tn_heff_matvec(ctx.handle, 0, d, Dw, Dw, D1, D2, W.ctypes.data, F.data_ptr(),
+                                              G.data_ptr(), x.data_ptr(), y_ref.data_ptr()), "tn_heff_matvec")
+        ctx.synchronize()
+        a, b = y.cpu().numpy(), y_ref.cpu().numpy()
+        assert np.linalg.norm(a - b) <= TOL * np.linalg.norm(b)
