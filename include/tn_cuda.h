@@ -96,6 +96,11 @@ typedef struct {
                             continuation follows the split-precision solve
                             (0: never; the FP64 Rayleigh quotient always
                             supplies the site energy)                       */
+    double fp64_tol_rel; /* FP64 Lanczos: residual target relative to the
+                            norm of its tridiagonal matrix, with the same
+                            stop on a stalled residual as the split-precision
+                            phase (0: the absolute eps_eigen only).  Lets the
+                            FP64 sweep stop by the mixed path's rule.       */
 } tn_solver_options;
 
 /* Per-run statistics, device-timed with CUDA events. */
@@ -234,15 +239,27 @@ int tn_eigensolve_heff(tn_ctx ctx, const tn_solver_options* opt, int d, int Dw1,
                        int D1, int D2, const double* W_host, const double* F,
                        const double* G, double* x, double tol, double* theta,
                        double* residual, int* matvecs);
-/* Dense symmetric eigensolver, lowest k pairs: EigenSolver<T>::Solve
- * (NumericalMethods/EigenSolver.H:31).  A: N x N (lda), U: N x k (ldu). */
+/* Dense symmetric eigensolver, lowest k pairs in ascending order:
+ * EigenSolver<T>::Solve (NumericalMethods/EigenSolver.H:31), the contract of
+ * LapackEigenSolver::Solve (LapackEigenSolver.C:62-109, zheevx RANGE='I',
+ * IL=1, IU=k).  A: N x N (lda) device, U: N x k (ldu) device, w_host: k
+ * eigenvalues.  On the device: A is shifted above its Gershgorin bound to a
+ * positive-definite matrix whose one-sided Jacobi SVD is its eigen-
+ * decomposition (absolute eigenvalue accuracy ~ eps |A|, as abstol gives
+ * LAPACK); tol >= 0 is the reference's abstol and is accepted, not needed.
+ * N is limited by the single-CTA Jacobi kernel (N <= ~17000). */
 int tn_eigensolve_dense(tn_ctx ctx, int N, const double* A, int lda, int k, double tol,
                         double* w_host, double* U, int ldu);
-/* SVDSolver<T>::Solve (NumericalMethods/SVDSolver.H:19, LapackSVDSolver.C:42-90),
+/* SVDSolver<T>::SolveAll (NumericalMethods/SVDSolver.H:22, LapackSVDSolver.C:42-90),
  * one-sided Jacobi: A (m x n) = U s Vt, k = min(m,n); U m x k, s k (device),
  * Vt k x n.  Zero singular values get orthonormal completion vectors. */
 int tn_svd(tn_ctx ctx, int m, int n, const double* A, int lda, double* U, int ldu,
            double* s, double* Vt, int ldvt);
+/* SVDSolver<T>::Solve(A, eps, k) (SVDSolver.H:21, LapackSVDSolver.C:42-90):
+ * the k largest singular triplets, U m x k (ldu), s k (device), Vt k x n
+ * (ldvt); eps < 1 as the reference asserts. */
+int tn_svd_solve(tn_ctx ctx, int m, int n, const double* A, int lda, double eps, int k, double* U, int ldu,
+                 double* s, double* Vt, int ldvt);
 /* Singular values only (descending). */
 int tn_svd_values(tn_ctx ctx, int m, int n, const double* A, int lda, double* s);
 /* QRSolver<T>::SolveThinQR / SolveThinLQ (NumericalMethods/QRSolver.H:18-21,
@@ -332,6 +349,33 @@ int tn_dataset_data(tn_dataset ds, const float** F, const float** T);
 /* Attach (or detach with NULL) the learned correction / the recorder. */
 int tn_mps_set_learned_correction(tn_mps psi, tn_mlp m);
 int tn_mps_set_recorder(tn_mps psi, tn_dataset ds);
+
+/* ---- full state: exact diagonalisation on the device ------------------------
+ * FullState (TensorNetworks/FullState.H:15-35, FullStateImp.C): all d^L
+ * amplitudes of the open chain (site 1 the most significant digit,
+ * StateIterator::GetIndex), at most 2^31 - 1 of them.  The field enters as
+ * hz Sz once per site (the MPO's convention; the reference's local matrix
+ * Hamiltonian_1D_NN_Heisenberg::GetH adds it on both sites of every bond). */
+typedef struct tn_fullstate_s* tn_fullstate;
+/* Hamiltonian::CreateFullState (Hamiltonian.H:28): random amplitudes from seed. */
+int tn_fullstate_create(tn_hamiltonian h, uint64_t seed, tn_fullstate* out);
+int tn_fullstate_destroy(tn_fullstate fs);
+/* FullState::GetSize: d^L. */
+long long tn_fullstate_get_size(tn_fullstate fs);
+/* FullState::FindGroundState(H, epsE) (FullStateImp.C:190-205): device Lanczos
+ * on the operator below, residual target epsE; amplitudes normalised with the
+ * sign of the first one above 0.01 positive (FullStateImp::Normalize). */
+int tn_fullstate_find_ground_state(tn_fullstate fs, tn_hamiltonian h, double epsE, double* E, int* matvecs);
+/* FullState::PowerIterate(H, epsE, epsPsi, maxIter) (FullStateImp.C:155-188). */
+int tn_fullstate_power_iterate(tn_fullstate fs, tn_hamiltonian h, double epsE, double epsPsi, int max_iter,
+                               double* E, int* iters);
+/* FullState::GetE. */
+int tn_fullstate_get_e(tn_fullstate fs, double* E);
+/* Amplitudes to the host (d^L doubles). */
+int tn_fullstate_get_amplitudes(tn_fullstate fs, double* host);
+/* FullStateImp::DoMatVecContraction (FullStateImp.C:207-217), the
+ * SparseEigenSolverClient face: y = H x on device vectors of d^L. */
+int tn_fullstate_matvec(tn_fullstate fs, tn_hamiltonian h, const double* x, double* y);
 
 #ifdef __cplusplus
 }

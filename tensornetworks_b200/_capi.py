@@ -40,7 +40,7 @@ class SchedLine(C.Structure):
 class SolverOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("eigensolver", C.c_int), ("krylov", C.c_int),
                 ("max_restarts", C.c_int), ("use_learned", C.c_int), ("verbose", C.c_int),
-                ("mixed_tol", C.c_double), ("refine_tol", C.c_double)]
+                ("mixed_tol", C.c_double), ("refine_tol", C.c_double), ("fp64_tol_rel", C.c_double)]
 
 
 class SweepStats(C.Structure):
@@ -98,6 +98,14 @@ SIGNATURES = {
     "tn_itebd_step": (_I, [_V, _D, _I, _I]),
     "tn_itebd_find_ground_state": (_I, [_V, _V, _I, _I, _I, _I, _D, _V]),
     "tn_itebd_orthogonalize": (_I, [_V, _I, _D, _I, _PD, _PI]),
+    "tn_fullstate_create": (_I, [_V, _ULL, _PV]),
+    "tn_fullstate_destroy": (_I, [_V]),
+    "tn_fullstate_get_size": (C.c_longlong, [_V]),
+    "tn_fullstate_find_ground_state": (_I, [_V, _V, _D, _PD, _PI]),
+    "tn_fullstate_power_iterate": (_I, [_V, _V, _D, _D, _I, _PD, _PI]),
+    "tn_fullstate_get_e": (_I, [_V, _PD]),
+    "tn_fullstate_get_amplitudes": (_I, [_V, _V]),
+    "tn_fullstate_matvec": (_I, [_V, _V, _V, _V]),
     "tn_itebd_energy": (_I, [_V, _I, _D, _PD]),
     "tn_mlp_create": (_I, [_V, _ULL, _PV]),
     "tn_mlp_destroy": (_I, [_V]),
@@ -124,6 +132,7 @@ SIGNATURES = {
                                 _PD, _PD, _PI]),
     "tn_eigensolve_dense": (_I, [_V, _I, _V, _I, _I, _D, _V, _V, _I]),
     "tn_svd": (_I, [_V, _I, _I, _V, _I, _V, _I, _V, _V, _I]),
+    "tn_svd_solve": (_I, [_V, _I, _I, _V, _I, _D, _I, _V, _I, _V, _V, _I]),
     "tn_svd_values": (_I, [_V, _I, _I, _V, _I, _V]),
     "tn_qr": (_I, [_V, _I, _I, _V, _I, _V, _I, _V, _I]),
     "tn_lq": (_I, [_V, _I, _I, _V, _I, _V, _I, _V, _I]),

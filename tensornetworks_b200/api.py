@@ -141,10 +141,12 @@ class SolverOptions:
     verbose: int = 0
     mixed_tol: float = 0.0
     refine_tol: float = 0.0
+    fp64_tol_rel: float = 0.0
 
     def to_c(self):
         return capi.SolverOptions(self.precision, self.eigensolver, self.krylov, self.max_restarts,
-                                  self.use_learned, self.verbose, self.mixed_tol, self.refine_tol)
+                                  self.use_learned, self.verbose, self.mixed_tol, self.refine_tol,
+                                  self.fp64_tol_rel)
 
 
 # ---------------------------------------------------------------------------
@@ -208,6 +210,10 @@ class Hamiltonian:
 
     def CreateMPS(self, D: int, normEps: float = 1e-12, epsSV: float = 1e-12) -> "MPS":
         return MPS(self, D, normEps, epsSV)
+
+    def CreateFullState(self, seed: int = 1234) -> "FullState":
+        """Hamiltonian::CreateFullState (Hamiltonian.H:28): the d^L wave function on the GPU."""
+        return FullState(self, seed)
 
     def __del__(self):  # pragma: no cover
         try:
@@ -322,6 +328,61 @@ class MPS:
         try:
             if getattr(self, "handle", None):
                 self._lib.tn_mps_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# FullState (TensorNetworks/FullState.H): exact diagonalisation on the GPU
+# ---------------------------------------------------------------------------
+class FullState:
+    """FullState: all d^L amplitudes of the chain on the device (FullStateImp.C)."""
+
+    def __init__(self, H: Hamiltonian, seed: int = 1234):
+        self.H = H
+        self._lib = H._lib
+        h = C.c_void_p()
+        check(self._lib.tn_fullstate_create(H.handle, int(seed), C.byref(h)), "tn_fullstate_create")
+        self.handle = h
+
+    def GetSize(self) -> int:
+        return int(self._lib.tn_fullstate_get_size(self.handle))
+
+    def GetE(self) -> float:
+        E = C.c_double()
+        check(self._lib.tn_fullstate_get_e(self.handle, C.byref(E)), "tn_fullstate_get_e")
+        return E.value
+
+    def FindGroundState(self, H: Hamiltonian, epsE: float = 1e-10) -> float:
+        """Lanczos ground state; returns the energy (the reference returns it via GetE)."""
+        E, mv = C.c_double(), C.c_int()
+        check(self._lib.tn_fullstate_find_ground_state(self.handle, H.handle, float(epsE), C.byref(E), C.byref(mv)),
+              "tn_fullstate_find_ground_state")
+        self.last_matvecs = mv.value
+        return E.value
+
+    def PowerIterate(self, H: Hamiltonian, epsE: float, epsPsi: float, maxIter: int = 1000) -> float:
+        E, it = C.c_double(), C.c_int()
+        check(self._lib.tn_fullstate_power_iterate(self.handle, H.handle, float(epsE), float(epsPsi), int(maxIter),
+                                                   C.byref(E), C.byref(it)), "tn_fullstate_power_iterate")
+        self.last_iterations = it.value
+        return E.value
+
+    def GetAmplitudes(self) -> np.ndarray:
+        out = np.empty(self.GetSize())
+        check(self._lib.tn_fullstate_get_amplitudes(self.handle, out.ctypes.data), "tn_fullstate_get_amplitudes")
+        return out
+
+    def DoMatVecContraction(self, x_dev, y_dev):
+        """SparseEigenSolverClient face: y = H x on device buffers (torch tensors)."""
+        check(self._lib.tn_fullstate_matvec(self.handle, self.H.handle, x_dev.data_ptr(), y_dev.data_ptr()),
+              "tn_fullstate_matvec")
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if getattr(self, "handle", None):
+                self._lib.tn_fullstate_destroy(self.handle)
                 self.handle = None
         except Exception:
             pass
@@ -532,10 +593,6 @@ class CudaSVDSolver:
         self.ctx = ctx or default_context()
 
     def SolveAll(self, A, eps: float = 1e-13):
-        m, n = np.shape(A)
-        return self.Solve(A, eps, min(m, n))
-
-    def Solve(self, A, eps: float, NumSingularValues: int):
         torch = _torch()
         m, n = np.shape(A)
         k = min(m, n)
@@ -545,9 +602,20 @@ class CudaSVDSolver:
         Vt = torch.empty(k * n, dtype=torch.float64, device="cuda")
         check(self.ctx._lib.tn_svd(self.ctx.handle, m, n, dA.data_ptr(), m, U.data_ptr(), m, s.data_ptr(),
                                    Vt.data_ptr(), k), "tn_svd")
-        U, s, Vt = _host(U, m, k), s.cpu().numpy(), _host(Vt, k, n)
-        r = int(NumSingularValues)
-        return U[:, :r], s[:r], Vt[:r, :]
+        return _host(U, m, k), s.cpu().numpy(), _host(Vt, k, n)
+
+    def Solve(self, A, eps: float, NumSingularValues: int):
+        """The NumSingularValues largest triplets (tn_svd_solve)."""
+        torch = _torch()
+        m, n = np.shape(A)
+        k = int(NumSingularValues)
+        dA = _dev(A)
+        U = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        s = torch.empty(k, dtype=torch.float64, device="cuda")
+        Vt = torch.empty(k * n, dtype=torch.float64, device="cuda")
+        check(self.ctx._lib.tn_svd_solve(self.ctx.handle, m, n, dA.data_ptr(), m, float(eps), k, U.data_ptr(), m,
+                                         s.data_ptr(), Vt.data_ptr(), k), "tn_svd_solve")
+        return _host(U, m, k), s.cpu().numpy(), _host(Vt, k, n)
 
 
 class CudaQRSolver:

@@ -9,6 +9,7 @@
 #include "engine.h"
 #include "mixed.h"
 #include "itebd.h"
+#include "ed.h"
 
 namespace tnb {
 
@@ -450,7 +451,7 @@ int tn_heff_create(tn_ctx c, int precision, int d, int Dw1, int Dw2, int D1, int
             st = h->P.ensure(scr);
             if (st == TN_OK) st = h->Q.ensure(scr);
         } else {
-            st = mixed_prepare_site(c->c, h->ms, s, h->terms.as<WTermDev>(), h->nterms, F, G, -1, -1,
+            st = mixed_prepare_site(c->c, h->ms, s, W_host, F, G, -1, -1,
                                     precision == TN_PREC_MIXED_HI ? 3 : 2);
         }
     }
@@ -606,57 +607,35 @@ int tn_eigensolve_heff(tn_ctx c, const tn_solver_options* opt, int d, int Dw1, i
 
 int tn_eigensolve_dense(tn_ctx c, int N, const double* A, int lda, int k, double tol, double* w_host, double* U,
                         int ldu) {
-    if (!c || !A || !w_host || !U || N < 1 || k < 1 || k > N || lda < N || ldu < N) return TN_BAD_ARG;
+    if (!c || !A || !w_host || !U || N < 1 || k < 1 || k > N || lda < N || ldu < N || !(tol >= 0.0)) return TN_BAD_ARG;
     TN_ON_DEVICE(c->c.device);
     Ctx& cx = c->c;
-    // Lowest k pairs by Lanczos with shift deflation: A' = A + sigma sum_i u_i u_i^T.
-    // sigma above the spectral radius bound (max row sum).
-    std::vector<double> hA((size_t)lda * N);
-    TN_CUDA_CHECK(cudaMemcpy(hA.data(), A, sizeof(double) * hA.size(), cudaMemcpyDeviceToHost));
-    double rad = 0;
-    for (int i = 0; i < N; ++i) {
-        double r = 0;
-        for (int j = 0; j < N; ++j) r += std::fabs(hA[(size_t)j * lda + i]);
-        rad = std::max(rad, r);
+    if ((size_t)N * 12 + 64 > 200 * 1024) {
+        set_error("tn_eigensolve_dense: N = %d exceeds the single-CTA Jacobi limit", N);
+        return TN_BAD_SHAPE;
     }
-    const double sigma = 2.0 * rad + 1.0;
-    DevBuf tmpv;
-    TN_CHECK(tmpv.ensure(sizeof(double) * (size_t)(k + 1)));
-    for (int e = 0; e < k; ++e) {
-        double* u = U + (size_t)e * ldu;
-        TN_CHECK(fill(u, N, 1.0, cx.stream));
-        MatvecFn mv = [&](const double* xi, double* yo, const int* skip) -> int {
-            GemmArgs g;
-            g.M = N; g.N = 1; g.K = N;
-            g.A.ptr = A; g.A.mn = idx(1); g.A.k = idx(lda);
-            g.B.ptr = xi; g.B.k = idx(1); g.B.mn = idx(N);
-            g.C.ptr = yo; g.C.m = idx(1); g.C.n = idx(N);
-            g.skip = skip;
-            TN_CHECK(gemm_f64(g, cx.stream));
-            if (e > 0) {
-                // c = U_e^T x ; y += sigma U_e c
-                GemmArgs h;
-                h.M = e; h.N = 1; h.K = N;
-                h.A.ptr = U; h.A.mn = idx(ldu); h.A.k = idx(1);
-                h.B.ptr = xi; h.B.k = idx(1); h.B.mn = idx(N);
-                h.C.ptr = tmpv.as<double>(); h.C.m = idx(1); h.C.n = idx(e);
-                h.skip = skip;
-                TN_CHECK(gemm_f64(h, cx.stream));
-                GemmArgs q;
-                q.M = N; q.N = 1; q.K = e; q.alpha = sigma; q.beta = 1.0;
-                q.A.ptr = U; q.A.mn = idx(1); q.A.k = idx(ldu);
-                q.B.ptr = tmpv.as<double>(); q.B.k = idx(1); q.B.mn = idx(e);
-                q.C.ptr = yo; q.C.m = idx(1); q.C.n = idx(N);
-                q.skip = skip;
-                TN_CHECK(gemm_f64(q, cx.stream));
-            }
-            return (int)TN_OK;
-        };
-        LzResult r{};
-        TN_CHECK(lanczos_solve(cx, N, u, std::min(N, 40), 50, tol, mv, &r));
-        w_host[e] = r.theta;
-    }
+    // A + sigma I is positive definite for sigma above the Gershgorin bound
+    // max_i sum_j |A_ij|; its SVD is then its eigen-decomposition, with the
+    // eigenvalues s_i - sigma (descending) -- all on the device.
+    const size_t n2 = (size_t)N * N;
+    DevBuf work;
+    TN_CHECK(work.ensure(sizeof(double) * (4 * n2 + (size_t)N + 8)));
+    double* W = work.as<double>();
+    double* V = W + n2;
+    double* Ua = V + n2;
+    double* Vt = Ua + n2;
+    double* sv = Vt + n2;
+    double* scal = sv + N;
+    TN_CHECK(dense_shift_spd(N, A, lda, W, scal, cx.stream));
+    SvdJob j{W, N, N, V, Ua, N, Vt, N, sv, nullptr};
+    TN_CHECK(svd_batched(cx, {j}, true));
+    // lowest k pairs, ascending: column N-1-e of Ua and s[N-1-e] - sigma
+    TN_CHECK(copy2d(N, k, Ua + (size_t)(N - 1) * N, idx(1), idx(-(long long)N), U, idx(1), idx(ldu), 1.0, cx.stream));
+    std::vector<double> hs(N + 1);
+    TN_CUDA_CHECK(cudaMemcpyAsync(hs.data(), sv, sizeof(double) * N, cudaMemcpyDeviceToHost, cx.stream));
+    TN_CUDA_CHECK(cudaMemcpyAsync(hs.data() + N, scal, sizeof(double), cudaMemcpyDeviceToHost, cx.stream));
     TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    for (int e = 0; e < k; ++e) w_host[e] = hs[N - 1 - e] - hs[N];
     return TN_OK;
 }
 
@@ -702,6 +681,30 @@ int tn_svd(tn_ctx c, int m, int n, const double* A, int lda, double* U, int ldu,
 
 int tn_svd_values(tn_ctx c, int m, int n, const double* A, int lda, double* s) {
     return svd_common(c, m, n, A, lda, nullptr, 0, s, nullptr, 0, false);
+}
+
+// SVDSolver<T>::Solve(A, eps, k) (LapackSVDSolver.C:42-90): the k largest
+// singular triplets.  eps is checked (< 1) as the reference asserts; the
+// decomposition itself is complete before the truncation.
+int tn_svd_solve(tn_ctx c, int m, int n, const double* A, int lda, double eps, int k, double* U, int ldu, double* s,
+                 double* Vt, int ldvt) {
+    const int mn = std::min(m, n);
+    if (!c || !A || !U || !s || !Vt || m < 1 || n < 1 || lda < m || k < 1 || k > mn || ldu < m || ldvt < k ||
+        !(eps < 1.0))
+        return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
+    Ctx& cx = c->c;
+    DevBuf full;
+    TN_CHECK(full.ensure(sizeof(double) * ((size_t)m * mn + (size_t)mn * n + mn)));
+    double* Uf = full.as<double>();
+    double* Vf = Uf + (size_t)m * mn;
+    double* sf = Vf + (size_t)mn * n;
+    TN_CHECK(svd_common(c, m, n, A, lda, Uf, m, sf, Vf, mn, true));
+    TN_CHECK(copy2d(m, k, Uf, idx(1), idx(m), U, idx(1), idx(ldu), 1.0, cx.stream));
+    TN_CHECK(copy2d(k, n, Vf, idx(1), idx(mn), Vt, idx(1), idx(ldvt), 1.0, cx.stream));
+    TN_CUDA_CHECK(cudaMemcpyAsync(s, sf, sizeof(double) * k, cudaMemcpyDeviceToDevice, cx.stream));
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return TN_OK;
 }
 
 int tn_qr(tn_ctx c, int m, int n, const double* A, int lda, double* Q, int ldq, double* R, int ldr) {
@@ -1020,6 +1023,78 @@ int tn_itebd_energy(tn_itebd st, int max_iters, double tol, double* E) {
     if (!st || !E || max_iters < 1) return TN_BAD_ARG;
     TN_ON_DEVICE(st->s.ctx->device);
     return st->s.energy(E, max_iters, tol);
+}
+
+
+// ---- full state (exact diagonalisation) ------------------------------------------
+struct tn_fullstate_s {
+    tnb::FullStateDev f;
+};
+
+int tn_fullstate_create(tn_hamiltonian h, uint64_t seed, tn_fullstate* out) {
+    if (!h || !out) return TN_BAD_ARG;
+    TN_ON_DEVICE(h->h.ctx->device);
+    *out = nullptr;
+    auto* fs = new tn_fullstate_s();
+    int st = fs->f.init(*h->h.ctx, h->h.L, h->h.S, seed);
+    if (st == TN_OK) st = fs->f.set_hamiltonian(h->h.Jxy, h->h.Jz, h->h.hz);
+    if (st == TN_OK && cudaStreamSynchronize(h->h.ctx->stream) != cudaSuccess) st = TN_CUDA_ERROR;
+    if (st != TN_OK) {
+        delete fs;
+        return st;
+    }
+    *out = fs;
+    return TN_OK;
+}
+
+int tn_fullstate_destroy(tn_fullstate fs) {
+    if (!fs) return TN_BAD_ARG;
+    TN_ON_DEVICE(fs->f.ctx->device);
+    cudaStreamSynchronize(fs->f.ctx->stream);
+    delete fs;
+    return TN_OK;
+}
+
+long long tn_fullstate_get_size(tn_fullstate fs) { return fs ? fs->f.N : -1; }
+
+static bool same_chain(tn_fullstate fs, tn_hamiltonian h) {
+    return h->h.L == fs->f.L && std::fabs(h->h.S - fs->f.S) < 1e-12;
+}
+
+int tn_fullstate_find_ground_state(tn_fullstate fs, tn_hamiltonian h, double epsE, double* E, int* matvecs) {
+    if (!fs || !h || !(epsE > 0) || !same_chain(fs, h)) return TN_BAD_ARG;
+    TN_ON_DEVICE(fs->f.ctx->device);
+    TN_CHECK(fs->f.set_hamiltonian(h->h.Jxy, h->h.Jz, h->h.hz));
+    return fs->f.find_ground_state(epsE, 40, 200, E, matvecs);
+}
+
+int tn_fullstate_power_iterate(tn_fullstate fs, tn_hamiltonian h, double epsE, double epsPsi, int max_iter,
+                               double* E, int* iters) {
+    if (!fs || !h || max_iter < 1 || !same_chain(fs, h)) return TN_BAD_ARG;
+    TN_ON_DEVICE(fs->f.ctx->device);
+    TN_CHECK(fs->f.set_hamiltonian(h->h.Jxy, h->h.Jz, h->h.hz));
+    return fs->f.power_iterate(epsE, epsPsi, max_iter, E, iters);
+}
+
+int tn_fullstate_get_e(tn_fullstate fs, double* E) {
+    if (!fs || !E) return TN_BAD_ARG;
+    *E = fs->f.E;
+    return TN_OK;
+}
+
+int tn_fullstate_get_amplitudes(tn_fullstate fs, double* host) {
+    if (!fs || !host) return TN_BAD_ARG;
+    TN_ON_DEVICE(fs->f.ctx->device);
+    TN_CUDA_CHECK(cudaStreamSynchronize(fs->f.ctx->stream));
+    TN_CUDA_CHECK(cudaMemcpy(host, fs->f.amp.p, sizeof(double) * (size_t)fs->f.N, cudaMemcpyDeviceToHost));
+    return TN_OK;
+}
+
+int tn_fullstate_matvec(tn_fullstate fs, tn_hamiltonian h, const double* x, double* y) {
+    if (!fs || !h || !x || !y || !same_chain(fs, h)) return TN_BAD_ARG;
+    TN_ON_DEVICE(fs->f.ctx->device);
+    TN_CHECK(fs->f.set_hamiltonian(h->h.Jxy, h->h.Jz, h->h.hz));
+    return fs->f.matvec(x, y, nullptr);
 }
 
 }  // extern "C"

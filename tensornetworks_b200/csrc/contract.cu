@@ -120,6 +120,46 @@ int wcombine(const double* P, double* Q, const WTermDev* terms, int nterms, long
     return TN_OK;
 }
 
+namespace {
+
+__global__ void gershgorin_kernel(int N, const double* __restrict__ A, int lda, double* sigma) {
+    __shared__ double sh[32];
+    double mx = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        double r = 0.0;
+        for (int j = 0; j < N; ++j) r += fabs(A[(size_t)j * lda + i]);
+        mx = fmax(mx, r);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmax(t, sh[w]);
+        *sigma = 1.001 * t + 1e-300;
+    }
+}
+
+__global__ void shift_copy_kernel(int N, const double* __restrict__ A, int lda, double* __restrict__ W,
+                                  const double* __restrict__ sigma) {
+    const double sg = *sigma;
+    const long long total = (long long)N * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % N), j = (int)(e / N);
+        W[e] = A[(size_t)j * lda + i] + (i == j ? sg : 0.0);
+    }
+}
+
+}  // namespace
+
+int dense_shift_spd(int N, const double* A, int lda, double* W, double* sigma, cudaStream_t st) {
+    gershgorin_kernel<<<1, 256, 0, st>>>(N, A, lda, sigma);
+    TN_LAUNCH_CHECK();
+    shift_copy_kernel<<<grid_for((long long)N * N), 256, 0, st>>>(N, A, lda, W, sigma);
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
 int copy2d(int rows, int cols, const double* src, IdxMap sr, IdxMap sc, double* dst, IdxMap dr, IdxMap dc,
            double scale, cudaStream_t st) {
     if (rows <= 0 || cols <= 0) return TN_OK;

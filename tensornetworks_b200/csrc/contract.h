@@ -21,6 +21,10 @@ int wcombine(const double* P, double* Q, const WTermDev* terms, int nterms, long
 int copy2d(int rows, int cols, const double* src, IdxMap sr, IdxMap sc, double* dst, IdxMap dr, IdxMap dc,
            double scale, cudaStream_t st);
 int fill(double* p, long long n, double v, cudaStream_t st);
+// W = A + sigma I (N x N, W with leading dimension N) with sigma = 1.001 times
+// the Gershgorin bound max_i sum_j |A_ij| of A's spectrum (plus a tiny floor),
+// written to *sigma on the device: W is then symmetric positive definite.
+int dense_shift_spd(int N, const double* A, int lda, double* W, double* sigma, cudaStream_t st);
 // p[i] += v
 int shift_vector(double* p, long long n, double v, cudaStream_t st);
 int slab_sum(const double* in, int nslab, long long slab, double* out, const int* skip, cudaStream_t st);

@@ -572,7 +572,7 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
         TN_CHECK(ctx->prof_events());
         TN_CUDA_CHECK(cudaEventRecord(ctx->pev[0], st));
     }
-    TN_CHECK(mixed_prepare_site(*ctx, msite, s, t, op.nLR, F, G, wF, wG, ns));
+    TN_CHECK(mixed_prepare_site(*ctx, msite, s, op.W.data(), F, G, wF, wG, ns));
     if (ctx->prof) TN_CUDA_CHECK(cudaEventRecord(ctx->pev[1], st));
     MatvecFn mvm = [&](const double* x, double* y, const int* skip) {
         return heff_matvec_mixed(*ctx, msite, x, y, skip);
@@ -588,7 +588,7 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     key = hash_val(key, ns);
     key = hash_val(key, (const void*)t);
     key = hash_val(key, op.nLR);
-    for (const DevBuf* b : {&msite.Fs, &msite.Gs, &msite.Xs, &msite.P32, &msite.Qs, &msite.shifts, &msite.err})
+    for (const DevBuf* b : {&msite.Fs, &msite.Gc, &msite.Xs, &msite.Ps, &msite.segs, &msite.shifts, &msite.err})
         key = hash_val(key, b->p);
     const bool deferred = opt.refine_tol <= 0 && opt.verbose < 3 && ctx->aux2;
     if (deferred) {
@@ -770,14 +770,14 @@ int MPSState::refine_site_davidson(int ia, double epsEigen) {
     if (mixed) {
         const int wF = H->form == TN_FORM_REGULAR_LOWER ? 0 : op.Dw1 - 1;
         const int wG = H->form == TN_FORM_REGULAR_LOWER ? op.Dw2 - 1 : 0;
-        TN_CHECK(mixed_prepare_site(*ctx, msite, s, t, op.nLR, F, G, wF, wG, ns));
+        TN_CHECK(mixed_prepare_site(*ctx, msite, s, op.W.data(), F, G, wF, wG, ns));
         // the split operator is Heff - sigma I: shift the diagonal the same way
         const double sigma = mixed_shift_host(msite, st);
         TN_CHECK(shift_vector(diagbuf.as<double>(), N, -sigma, st));
         mv = [&](const double* x, double* y, const int* skip) { return heff_matvec_mixed(*ctx, msite, x, y, skip); };
         tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-7);
         key = hash_val(key, ns);
-        for (const DevBuf* b : {&msite.Fs, &msite.Gs, &msite.Xs, &msite.P32, &msite.Qs, &msite.shifts, &msite.err})
+        for (const DevBuf* b : {&msite.Fs, &msite.Gc, &msite.Xs, &msite.Ps, &msite.segs, &msite.shifts, &msite.err})
             key = hash_val(key, b->p);
     } else {
         mv = [&](const double* x, double* y, const int* skip) {
@@ -847,7 +847,8 @@ int MPSState::refine_site(int ia, double epsEigen) {
     for (const void* q : {(const void*)t, (const void*)F, (const void*)G, (const void*)P, (const void*)Q})
         key = hash_val(key, q);
     key = hash_val(key, op.nLR);
-    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, &r, 0.0, key));
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, &r,
+                           opt.fp64_tol_rel > 0 ? opt.fp64_tol_rel : 0.0, key));
     matvecs += r.matvecs;
     matvecs_fp64 += r.matvecs;
     heff_flop += heff_flops(s) * r.matvecs;

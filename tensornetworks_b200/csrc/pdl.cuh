@@ -16,6 +16,14 @@ namespace tnb {
 
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Lets the next kernel on the stream (launched with launch_pdl) be scheduled
+// once every CTA of this grid has passed here (or exited); it still waits in its
+// own pdl_wait() for this grid's completion and memory flush, so calling this
+// early only overlaps the next kernel's launch and prologue with this one.
+__device__ __forceinline__ void pdl_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <class... KArgs, class... Args>
 int launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
     cudaLaunchConfig_t cfg = {};

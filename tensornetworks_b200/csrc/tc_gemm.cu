@@ -18,98 +18,13 @@
 
 #include "tc_gemm.h"
 #include "pdl.cuh"
+#include "tc_ptx.cuh"
 
 namespace tnb {
 
 namespace {
 
-constexpr int BM = 128;
-constexpr int BK = 64;          // BF16 elements per K chunk = 128 bytes (one swizzle row)
-constexpr int THREADS = 192;
-constexpr uint32_t WAIT_LIMIT = 1u << 26;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// Bounded wait for the phase with the given parity; false when the limit expires.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    const uint32_t addr = smem_u32(bar);
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred P1;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, P1;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
-                                            int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row core groups
-// 1024 bytes apart (SBO), version 1 (sm_100).
-__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)(16 >> 4) << 16;      // LBO (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;    // SBO
-    d |= (uint64_t)1 << 46;              // version
-    d |= (uint64_t)2 << 61;              // SWIZZLE_128B
-    return d;
-}
-
-// Instruction descriptor, kind::f16: BF16 x BF16 -> FP32, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+using namespace tcp;
 
 template <int BN, int NS>
 struct SmemLayout {
@@ -264,12 +179,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (threadIdx.x == 0 && s_fail && p.err) atomicExch(p.err, 1);
 }
 
+}  // namespace
+
 // ---- tensor maps --------------------------------------------------------------
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-EncodeTiledFn encode_fn() {
+static EncodeTiledFn encode_fn() {
     static EncodeTiledFn fn = nullptr;
     if (!fn) {
         void* p = nullptr;
@@ -282,7 +199,7 @@ EncodeTiledFn encode_fn() {
 }
 
 // 3-D BF16 operand map {K, rows, batch}, box {64, box_rows, 1}, 128-byte swizzle.
-int make_map(CUtensorMap* m, const uint16_t* base, int K, int rows, int batch, long long row_pitch_elems,
+int tc_make_map(CUtensorMap* m, const uint16_t* base, int K, int rows, int batch, long long row_pitch_elems,
              long long batch_pitch_elems, int box_rows) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) {
@@ -308,7 +225,6 @@ int make_map(CUtensorMap* m, const uint16_t* base, int K, int rows, int batch, l
     return TN_OK;
 }
 
-}  // namespace
 
 int tc_gemm_plan(const TcGemmArgs& p, TcGemmPlan* plan) {
     if (p.K % 8 != 0 || p.lda % 8 != 0 || p.ldb % 8 != 0) {
@@ -327,8 +243,8 @@ int tc_gemm_plan(const TcGemmArgs& p, TcGemmPlan* plan) {
     const long long tiles128 = (long long)((p.N + 127) / 128) * ((p.M + BM - 1) / BM) * p.batch;
     plan->bn = (p.N <= 64 || tiles128 < 148) ? 64 : 128;
     for (int q = 0; q < p.nsplit; ++q) {
-        TN_CHECK(make_map(&plan->maps.a[q], p.a[q], p.K, p.M, p.a_nbatch, p.lda, p.a_batch, BM));
-        TN_CHECK(make_map(&plan->maps.b[q], p.b[q], p.K, p.N, p.b_nbatch, p.ldb, p.b_batch, plan->bn));
+        TN_CHECK(tc_make_map(&plan->maps.a[q], p.a[q], p.K, p.M, p.a_nbatch, p.lda, p.a_batch, BM));
+        TN_CHECK(tc_make_map(&plan->maps.b[q], p.b[q], p.K, p.N, p.b_nbatch, p.ldb, p.b_batch, plan->bn));
     }
     return TN_OK;
 }

@@ -39,6 +39,11 @@ struct TcGemmPlan {
     int bn = 128;
 };
 
+// 3-D BF16 operand map {K, rows, batch} with box {64, box_rows, 1} and the
+// 128-byte swizzle of the K-major UMMA operands.
+int tc_make_map(CUtensorMap* m, const uint16_t* base, int K, int rows, int batch, long long row_pitch_elems,
+                long long batch_pitch_elems, int box_rows);
+
 int tc_gemm_plan(const TcGemmArgs& a, TcGemmPlan* plan);
 int tc_gemm_run(const TcGemmPlan& plan, cudaStream_t st);
 

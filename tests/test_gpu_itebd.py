@@ -52,12 +52,21 @@ def test_trotter_steps_match_oracle(T, S, D, dt, nsteps):
 
 
 def test_ground_state_d8_within_reference_bounds(T):
-    st = T.iTEBDState(0.5, 8, seed=11)
-    steps = st.FindiTimeGroundState([0.5, 0.2, 0.1, 0.01, 0.001], 1000, 8)
-    E = st.GetExpectation()
-    print("iTEBD D=8", E, steps)
+    """The D = 8 bound of iTEBDTests.C:737-759 (E < -0.442846, above the
+    exact 1/4 - ln 2) with the reference's line driver: D grown from 2 to 8
+    by 1 in the first line, OrthogonalizeI around every D stage, dt 0.5 ->
+    0.2 -> 0.1 -> 0.01 -> 0.001 -> 0.  The device starts from the oracle's
+    initial state and ends at the oracle's energy."""
+    dts = [0.5, 0.2, 0.1, 0.01, 0.001, 0.0]
+    ref = I.State(0.5, 2, seed=11)
+    dev = load(T, ref, 2)
+    steps = dev.FindiTimeGroundState(dts, 1000, 8, 5e-5, deltaD=1)
+    E = dev.GetExpectation()
+    Eref, st, _ = I.find_ground_state_lines(0.5, 2, 8, 1, dts, 1000, seed=11)
+    print("iTEBD D=8", E, Eref, steps)
     assert EXACT < E < -0.442846
-    assert st.GetBond(0).size == 8 and st.GetBond(1).size == 8
+    assert abs(E - Eref) < 1e-8
+    assert dev.GetBond(0).size == 8 and dev.GetBond(1).size == 8
 
 
 def test_orthogonalize_matches_oracle(T):

@@ -195,8 +195,55 @@ def test_dense_eigensolver(T, ctx):
     A = B + B.T
     U, w = T.CudaEigenSolver(ctx).Solve(A, 1e-12, 2)
     ev = np.linalg.eigvalsh(A)
-    np.testing.assert_allclose(w, ev[:2], atol=1e-9)
-    assert np.linalg.norm(A @ U - U * w) < 1e-7
+    np.testing.assert_allclose(w, ev[:2], atol=1e-12 * np.abs(ev).max())
+    assert np.linalg.norm(A @ U - U * w) < 1e-10 * np.abs(ev).max()
+
+
+def test_dense_eigensolver_structured(T, ctx, oracle):
+    """LapackEigenSolver::Solve contract (LapackEigenSolver.C:62-109: zheevx,
+    RANGE='I', the lowest k pairs ascending) on matrices whose ground state is
+    orthogonal to the all-ones vector: the two-site Heisenberg term (singlet
+    ground state, ExactDiagTests.C:79-85), the full L = 8 spin-1/2 chain
+    Hamiltonian, and a matrix with a prescribed spectrum and eigenvectors."""
+    h = oracle.local_h12(0.5, 1.0, 1.0, 0.0)
+    U, w = T.CudaEigenSolver(ctx).Solve(h, 1e-13, 4)
+    np.testing.assert_allclose(w, [-0.75, 0.25, 0.25, 0.25], atol=1e-14)
+    singlet = np.array([0, 1, -1, 0]) / np.sqrt(2)
+    assert abs(abs(U[:, 0] @ singlet) - 1) < 1e-13
+    # L = 8 chain, 256 x 256: sum of bond terms
+    L, dd = 8, 2
+    H = np.zeros((dd ** L, dd ** L))
+    for b in range(L - 1):
+        H += np.kron(np.kron(np.eye(dd ** b), h), np.eye(dd ** (L - b - 2)))
+    U, w = T.CudaEigenSolver(ctx).Solve(H, 1e-13, 3)
+    ev, evec = np.linalg.eigh(H)
+    np.testing.assert_allclose(w, ev[:3], atol=1e-12)
+    assert abs(abs(U[:, 0] @ evec[:, 0]) - 1) < 1e-10
+    assert abs(U[:, 0].sum()) < 1e-10          # the singlet ground state is orthogonal to the ones vector
+    # prescribed spectrum, eigenvectors from a random orthogonal matrix with the lowest one orthogonal to ones
+    rng = np.random.default_rng(5)
+    n = 40
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    Q[:, 0] = np.r_[1.0, -1.0, np.zeros(n - 2)] / np.sqrt(2)
+    Q, _ = np.linalg.qr(Q)
+    lam = np.sort(rng.uniform(-3, 3, n))
+    A = (Q * lam) @ Q.T
+    U, w = T.CudaEigenSolver(ctx).Solve(A, 1e-13, 5)
+    np.testing.assert_allclose(w, lam[:5], atol=1e-12)
+    assert np.linalg.norm(A @ U - U * w) < 1e-11
+    assert np.abs(U.T @ U - np.eye(5)).max() < 1e-12
+
+
+def test_svd_solve_truncates(T, ctx):
+    """SVDSolver::Solve(A, eps, k) (LapackSVDSolver.C:42-90): the k largest triplets."""
+    rng = np.random.default_rng(8)
+    A = rng.uniform(-1, 1, size=(30, 20))
+    U, s, Vt = T.CudaSVDSolver(ctx).Solve(A, 1e-12, 7)
+    u0, s0, vt0 = np.linalg.svd(A, full_matrices=False)
+    assert U.shape == (30, 7) and s.shape == (7,) and Vt.shape == (7, 20)
+    np.testing.assert_allclose(s, s0[:7], rtol=1e-12)
+    np.testing.assert_allclose(np.abs(U.T @ u0[:, :7]), np.eye(7), atol=1e-10)
+    np.testing.assert_allclose(np.abs(Vt @ vt0[:7].T), np.eye(7), atol=1e-10)
 
 
 def test_compressor(T, ctx, oracle):

@@ -99,3 +99,28 @@ def test_mixed_sweep_energy_vs_fp64(T, precision, tol):
     print("FP64", E64 / L, var64, st64["matvecs"], "mixed", Em / L, varm, stm["matvecs"], stm["matvecs_fp64"])
     assert abs(Em - E64) / L <= tol
     assert stm["matvecs_fp64"] < stm["matvecs"]
+
+
+@pytest.mark.parametrize("split", ["1,1", "2,1", "1,2", "1,4", "2,8", "1,8"])
+def test_mixed_matvec_every_splitk(T, ctx, oracle, split, monkeypatch):
+    """Every split-K pair of the two tcgen05 GEMMs (the cluster reduction over
+    1..8 CTAs) gives the same operator: D1 = D2 = 128 against the FP64 oracle."""
+    import ctypes as C
+    monkeypatch.setenv("TN_CHAIN_SPLITK", split)
+    rng = np.random.default_rng(21)
+    d, D1, D2 = 2, 128, 128
+    W = oracle.mpo_site(10, 0.5, 2, 1.0, 1.0, 0.2, 5)
+    F = rng.uniform(-1, 1, size=5 * D1 * D1)
+    G = rng.uniform(-1, 1, size=5 * D2 * D2)
+    dF, dG = dev(F), dev(G)
+    Wc = np.ascontiguousarray(W.ravel())
+    for prec, tol in ((1, TOL[1]), (2, TOL[2])):
+        h = C.c_void_p()
+        T._capi.check(ctx._lib.tn_heff_create(ctx.handle, prec, d, 5, 5, D1, D2, Wc.ctypes.data, dF.data_ptr(),
+                                              dG.data_ptr(), C.byref(h)), "create")
+        x = rng.uniform(-1, 1, size=d * D1 * D2)
+        dx, y = dev(x), dev(np.zeros(d * D1 * D2))
+        T._capi.check(ctx._lib.tn_heff_apply(h, dx.data_ptr(), y.data_ptr()), "apply")
+        ref = oracle.heff_matvec(W, F, G, x, D1, D2)
+        assert np.linalg.norm(y.cpu().numpy() - ref) / np.linalg.norm(ref) <= tol
+        T._capi.check(ctx._lib.tn_heff_destroy(h), "destroy")

@@ -25,9 +25,9 @@ def T():
     return T
 
 
-def run_gpu(T, L, S, D, sweeps, precision, seed):
+def run_gpu(T, L, S, D, sweeps, precision, seed, hz=0.0):
     f = T.Factory.GetFactory()
-    H = f.Make1D_NN_HeisenbergHamiltonian(L, S, T.RegularLower, 1.0, 1.0, 0.0)
+    H = f.Make1D_NN_HeisenbergHamiltonian(L, S, T.RegularLower, 1.0, 1.0, hz)
     psi = H.CreateMPS(D, 1e-12, 1e-12)
     psi.InitializeWith(T.Random, seed=seed)
     isched = T.IterationSchedule()
@@ -52,11 +52,17 @@ def test_mixed_sweep_D128_vs_oracle(T, oracle, precision):
 
 
 def test_mixed_sweep_spin1_vs_oracle(T, oracle):
-    """Spin 1 (d = 3), L = 24, D = 48 -- config 3's model at a size the oracle
-    runs in seconds -- on the split-precision path against the oracle."""
-    L, S, D, sw, seed = 24, 1.0, 48, 2, 77
-    E, var, st = run_gpu(T, L, S, D, sw, 2, seed)
-    r = oracle.find_ground_state(L, S, D, [(sw, D, 1, 1e-12, 1e-12, 1e-10)], seed=seed, eig_mode=1, gauge=1)
+    """Spin 1 (d = 3), config 3's model at a size the oracle runs in seconds:
+    L = 16, D = 32 (bulk sites 4..12 on the split-precision path), 16 sweeps
+    on both sides.  The open spin-1 chain has a near-fourfold ground state
+    (free spin-1/2 edge states split only by ~exp(-L/6)); a field hz = 0.1
+    polarises the edge spins and makes the ground state unique.  Early in the
+    optimisation the energy is first-order sensitive to where each site solve
+    stops (the state is far from stationary), so the comparison is made after
+    16 sweeps, where the trajectories have settled into the same optimum."""
+    L, S, D, sw, seed, hz = 16, 1.0, 32, 16, 77, 0.1
+    E, var, st = run_gpu(T, L, S, D, sw, 2, seed, hz=hz)
+    r = oracle.find_ground_state(L, S, D, [(sw, D, 1, 1e-12, 1e-12, 1e-10)], hz=hz, seed=seed, eig_mode=1, gauge=1)
     print("d3", E / L, r["energy"] / L, (E - r["energy"]) / L, st["matvecs"], st["matvecs_fp64"])
     assert abs(E - r["energy"]) / L <= TOL[2]
     assert st["total_sweeps"] == r["total_sweeps"]
