@@ -45,6 +45,9 @@ L_CHAIN, S_SPIN, D_FINAL = 100, 0.5, 256
 SCHEDULE = [(2, 16, 16), (2, 32, 16), (2, 64, 32), (2, 128, 64), (2, 256, 128)]
 EPS_EIGEN = 1e-10
 KRYLOV = 20
+# DRAM bytes (read + write) of one Heff application, summed over its kernels, from
+# the ncu capture of `bench.py --matvec-only --D 256` (profiles/heff_matvec_D256.md)
+TRAFFIC = {("mixed", 256): None, ("fp64", 256): 21.1e6}
 
 
 def parse():
@@ -57,9 +60,14 @@ def parse():
     p.add_argument("--no-fp64-compare", action="store_true",
                    help="skip the FP64 GPU sweep on the same schedule (speed-up and energy check)")
     p.add_argument("--L", type=int, default=L_CHAIN)
+    p.add_argument("--S", type=float, default=S_SPIN, help="spin (0.5: config 2; 1.0 with --L 128 --D 512: config 3)")
     p.add_argument("--D", type=int, default=D_FINAL)
     p.add_argument("--cpu-sites", type=int, default=4, help="bulk site updates in the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-learned", action="store_true",
+                   help="skip the Davidson arms (diagonal and learned correction) of the D step")
+    p.add_argument("--ref-half-sweep", type=int, default=1,
+                   help="reference arm: time one full half-sweep once to check the extrapolation (1) or not (0)")
     p.add_argument("--workload", choices=["sweep", "scan"], default="sweep",
                    help="scan: the XXZ parameter scan (independent chains, concurrent per-worker streams)")
     p.add_argument("--scan-n", type=int, default=64, help="scan instances (all ranks together)")
@@ -83,11 +91,12 @@ def max_over_ranks(x, dist, device):
 
 
 def unit_of(args):
-    return f"s per sweep pair (L={args.L}, D={args.D})"
+    return f"s per sweep pair (L={args.L}, D={args.D}{'' if args.S == 0.5 else f', S={args.S:g}'})"
 
 
 def workload_of(args):
-    return (f"Heisenberg S=1/2 L={args.L} open chain, d=2, Dw=5: the first sweep pair of the D={args.D} line "
+    d = int(round(2 * args.S + 1))
+    return (f"Heisenberg S={args.S:g} L={args.L} open chain, d={d}, Dw=5: the first sweep pair of the D={args.D} line "
             f"(state converged by the D 16->{args.D // 2} schedule lines, 2 sweeps/line, then grown to D={args.D} "
             f"by zero padding), Krylov 20, eig tol 1e-10")
 
@@ -207,16 +216,16 @@ def heff_flops(d, Dw1, Dw2, D1, D2):
     return 2.0 * d * Dw1 * D1 * D1 * D2 + 2.0 * d * Dw2 * D1 * D2 * D2 + 2.0 * d * d * Dw1 * Dw2 * D1 * D2
 
 
-def matvec_microbench(T, ctx, torch, D, precision, reps=50):
+def matvec_microbench(T, ctx, torch, D, precision, reps=50, S=0.5):
     """Average device time of one bulk Heff application at D x D (d=2, Dw=5) through
     the operator handle, on a torch stream that the library launches on, so that the
     torch events bracket exactly these launches."""
     import ctypes as C
     import numpy as np
     lib = ctx._lib
-    H = T.Factory(ctx).Make1D_NN_HeisenbergHamiltonian(10, 0.5, T.RegularLower, 1.0, 1.0, 0.0)
+    H = T.Factory(ctx).Make1D_NN_HeisenbergHamiltonian(10, S, T.RegularLower, 1.0, 1.0, 0.0)
     W = np.ascontiguousarray(H.GetW(5).ravel())
-    d, Dw = 2, 5
+    d, Dw = int(round(2 * S + 1)), 5
     g = torch.Generator(device="cuda").manual_seed(42)
     F = torch.rand(Dw * D * D, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
     G = torch.rand(Dw * D * D, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
@@ -265,6 +274,60 @@ def matvec_microbench(T, ctx, torch, D, precision, reps=50):
     return t, heff_flops(d, Dw, Dw, D, D)
 
 
+def lanczos_probe(T, ctx, D, peaks, d=2):
+    """Achieved HBM bandwidth of the Lanczos Krylov kernels (CGS2 projections, update,
+    next vector) at the bulk vector size N = 2 D^2, replayed from their CUDA graph on a
+    diagonal operator (tn_lanczos_probe), against the measured copy bandwidth."""
+    import ctypes as C
+    N = d * D * D
+    us, b = C.c_double(), C.c_double()
+    T._capi.check(ctx._lib.tn_lanczos_probe(ctx.handle, N, KRYLOV, C.byref(us), C.byref(b)), "tn_lanczos_probe")
+    gbs = b.value / (us.value * 1e-6) / 1e9
+    return {"N": N, "krylov": KRYLOV, "us_per_step": round(us.value, 2), "bytes_per_step": round(b.value),
+            "achieved_gbs": round(gbs, 1), "peak_gbs": peaks["hbm_gbs"], "frac": round(gbs / peaks["hbm_gbs"], 4),
+            "note": "algorithmic bytes (j+4)N doubles per step j plus the diagonal operator's 2N; "
+                    "device time from the graph replay (CUDA events)"}
+
+
+def learned_arms(args, T, ctx, run_path, t_step, E_after, fp64_cmp):
+    """Davidson on the same D step: diagonal correction, and the learned one (3-layer
+    MLP, width 64, BF16 weights) trained on the GPU on exact corrections recorded from
+    FP64 diagonal-Davidson sweeps of a small chain (L=16, D=32, 2 sweeps).  Diagonal
+    Davidson is the judge: the energies after the step are compared."""
+    f = T.Factory(ctx)
+    Hs = f.Make1D_NN_HeisenbergHamiltonian(16, args.S, T.RegularLower, 1.0, 1.0, 0.0)
+    t0 = time.perf_counter()
+    ds = T.TrainingSet(2_000_000, ctx)
+    psi = Hs.CreateMPS(32, 1e-12, 1e-12)
+    psi.InitializeWith(T.Random, seed=21)
+    psi.SetRecorder(ds)
+    sched = T.IterationSchedule()
+    eps = T.Epsilons(1e-12)
+    eps.itsEigenSolverEpsilon = EPS_EIGEN
+    sched.Insert(T.IterationScheduleLine(2, 32, 1, eps))
+    psi.FindVariationalGroundState(Hs, sched, T.SolverOptions(eigensolver=T.DAVIDSON, krylov=16))
+    psi.SetRecorder(None)
+    F, Tt = ds.device_arrays()
+    model = T.LearnedCorrection(seed=9, ctx=ctx)
+    _, l0 = model.gradient(F, Tt)
+    model.train(F, Tt, steps=1500, batch=4096, lr=2e-3, seed=3)
+    _, l1 = model.gradient(F, Tt)
+    train_s = time.perf_counter() - t0
+    diag = run_path(args.precision, False, davidson=True, finish=False)
+    lrn = run_path(args.precision, False, davidson=True, model=model, finish=False)
+    ref = fp64_cmp["value"] if fp64_cmp else None
+    return {"pairs": len(ds), "train_loss": [round(l0, 4), round(l1, 4)], "record_train_s": round(train_s, 2),
+            "diagonal": {"value": round(diag["t_step"], 6), "matvecs_per_step": diag["matvecs"] / args.steps,
+                         "dE_per_site_vs_lanczos": abs(diag["E_after"] - E_after) / args.L},
+            "learned": {"value": round(lrn["t_step"], 6), "matvecs_per_step": lrn["matvecs"] / args.steps,
+                        "dE_per_site_vs_diagonal": abs(lrn["E_after"] - diag["E_after"]) / args.L,
+                        "learned_steps": lrn["last"].get("learned_steps"),
+                        "fallbacks": lrn["last"].get("fallbacks")},
+            "gain_matvecs_learned_vs_diagonal": round(diag["matvecs"] / max(lrn["matvecs"], 1), 3),
+            "gain_time_learned_vs_diagonal": round(diag["t_step"] / lrn["t_step"], 3),
+            "speedup_learned_vs_fp64_gpu": round(ref / lrn["t_step"], 3) if ref else None}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -280,14 +343,14 @@ def run_ours(args, rank, world, local_rank):
     ctx = T.Context(local_rank)
     lib = ctx._lib
     f = T.Factory(ctx)
-    H = f.Make1D_NN_HeisenbergHamiltonian(args.L, S_SPIN, T.RegularLower, 1.0, 1.0, 0.0)
+    H = f.Make1D_NN_HeisenbergHamiltonian(args.L, args.S, T.RegularLower, 1.0, 1.0, 0.0)
     lines = schedule_for(args.D)
 
-    def run_path(precision, sample_clocks):
+    def run_path(precision, sample_clocks, fp64_tol_rel=0.0, davidson=False, model=None, finish=True):
         """Schedule up to the line before D, snapshot, then W warm-up and K timed steps;
         a step is the D line's first sweep pair from the grown snapshot."""
         prec = {"fp64": T.FP64, "mixed": T.MIXED, "mixed_hi": T.MIXED_HI}[precision]
-        opts = T.SolverOptions(precision=prec, krylov=KRYLOV, max_restarts=10)
+        opts = T.SolverOptions(precision=prec, krylov=KRYLOV, max_restarts=10, fp64_tol_rel=fp64_tol_rel)
         psi = H.CreateMPS(lines[0][1], 1e-12, 1e-12)
         psi.InitializeWith(T.Random, seed=1234)
 
@@ -304,6 +367,11 @@ def run_ours(args, rank, world, local_rank):
             psi.FindVariationalGroundState(H, make_sched(lines[:-1]), opts)
         pre_s = time.perf_counter() - t0
         grown = grow_sites([psi.GetSite(i) for i in range(1, args.L + 1)], args.D)
+        if davidson:
+            # the timed steps run Davidson (diagonal, or with the learned correction)
+            opts = T.SolverOptions(precision=prec, eigensolver=T.DAVIDSON, krylov=16, max_restarts=10,
+                                   use_learned=1 if model is not None else 0)
+            psi.SetLearnedCorrection(model)
 
         def step():
             for i, a in enumerate(grown, start=1):
@@ -336,17 +404,20 @@ def run_ours(args, rank, world, local_rank):
             clocks.stop()
         t_step = max_over_ranks(sum(step_ms) / len(step_ms) / 1e3, dist, "cuda")
         E_step = psi.GetExpectation(H)
-        # finish the schedule (the D line to convergence) from the grown snapshot
-        for i, a in enumerate(grown, start=1):
-            psi.SetSite(i, a)
-        t1 = time.perf_counter()
-        var = psi.FindVariationalGroundState(H, make_sched([lines[-1]]), opts)
-        schedule_s = pre_s + time.perf_counter() - t1
-        sched_stats = dict(psi.last_stats)
-        E_sched = psi.GetExpectation(H)
+        last = dict(psi.last_stats)
+        var = schedule_s = sched_stats = E_sched = None
+        if finish:
+            # finish the schedule (the D line to convergence) from the grown snapshot
+            for i, a in enumerate(grown, start=1):
+                psi.SetSite(i, a)
+            t1 = time.perf_counter()
+            var = psi.FindVariationalGroundState(H, make_sched([lines[-1]]), opts)
+            schedule_s = pre_s + time.perf_counter() - t1
+            sched_stats = dict(psi.last_stats)
+            E_sched = psi.GetExpectation(H)
         return dict(psi=psi, opts=opts, var=var, schedule_s=schedule_s, sched_stats=sched_stats, E_sched=E_sched,
                     t_step=t_step, step_ms=step_ms, matvecs=matvecs, flops=flops, launches=launches,
-                    clocks=clocks, E_after=E_step, grown=grown, step=step)
+                    clocks=clocks, E_after=E_step, grown=grown, step=step, last=last)
 
     main_run = run_path(args.precision, True)
     psi, opts, var = main_run["psi"], main_run["opts"], main_run["var"]
@@ -384,9 +455,25 @@ def run_ours(args, rank, world, local_rank):
                     "dE_per_site_after_steps": abs(E_after - ref64["E_after"]) / args.L,
                     "matvecs_per_step": ref64["matvecs"] / args.steps}
         del ref64
+        # the FP64 sweep stopped by the split-precision path's rule: residual relative
+        # to |T| (1e-7, 1e-9 for mixed_hi) with the stall test, so that the speed-up
+        # from precision is separated from the speed-up from the stop rule
+        tol_rel = 1e-9 if args.precision == "mixed_hi" else 1e-7
+        same = run_path("fp64", False, fp64_tol_rel=tol_rel, finish=False)
+        fp64_cmp["same_stop_rule"] = {
+            "value": round(same["t_step"], 6), "unit": unit_of(args), "fp64_tol_rel": tol_rel,
+            "speedup_of_split_precision": round(same["t_step"] / t_step, 3),
+            "speedup_over_fp64_tol_1e-10": round(fp64_cmp["value"] / same["t_step"], 3),
+            "dE_per_site_vs_split_precision": abs(E_after - same["E_after"]) / args.L,
+            "matvecs_per_step": same["matvecs"] / args.steps}
+        del same
+
+    learned = None
+    if not args.no_learned:
+        learned = learned_arms(args, T, ctx, run_path, t_step, E_after, fp64_cmp)
 
     # --- roofline of the dominant kernel (the bulk Heff contraction chain)
-    t_mv, F_mv = matvec_microbench(T, ctx, torch, args.D, args.precision)
+    t_mv, F_mv = matvec_microbench(T, ctx, torch, args.D, args.precision, S=args.S)
     peaks, peak_kind = measured_peaks()
     if args.precision == "fp64":
         peak = fp64_peak_tflops(torch)
@@ -398,10 +485,14 @@ def run_ours(args, rank, world, local_rank):
     achieved = F_mv / t_mv / 1e12
     # DRAM bytes per application from the ncu capture of the same command
     # (profiles/heff_matvec_D256.md); measured at D = 256 only
-    traffic = {("mixed", 256): 11.6e6, ("fp64", 256): 21.1e6}.get((args.precision, args.D))
+    traffic = TRAFFIC.get((args.precision, args.D))
     roofline = {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": "heff_matvec (3-stage chain)",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": "heff_matvec (x split + two segmented tcgen05 GEMMs)" if args.precision != "fp64"
+                else "heff_matvec (FP64 DMMA chain)",
                 "per_launch_us": round(t_mv * 1e6, 2), "flop_per_launch": F_mv, "peak_source": peak_src}
+
+    lanczos = lanczos_probe(T, ctx, args.D, peaks, d=int(round(2 * args.S + 1)))
 
     out = None
     if rank == 0:
@@ -438,6 +529,8 @@ def run_ours(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "lanczos_hbm": lanczos,
+            "davidson_learned": learned,
             "cpu_baseline": cpu,
             "clocks": clk,
         }
@@ -507,10 +600,10 @@ def cpu_baseline_same_state(args, sites, step_ms, psi):
     from oracle import oracle as O
     ncores = os.cpu_count() or 1
     first = args.L // 2 - args.cpu_sites // 2
-    sec, nmv = O.sweep_sample(args.L, S_SPIN, sites, first, args.cpu_sites, krylov=KRYLOV, max_restarts=10,
+    sec, nmv = O.sweep_sample(args.L, args.S, sites, first, args.cpu_sites, krylov=KRYLOV, max_restarts=10,
                               tol=EPS_EIGEN, nthreads=ncores)
     per_site = sec / args.cpu_sites
-    d, Dw = 2, 5
+    d, Dw = int(round(2 * args.S + 1)), 5
     bulk = heff_flops(d, Dw, Dw, args.D, args.D)
     w = 0.0
     for a in sites:
@@ -523,43 +616,90 @@ def cpu_baseline_same_state(args, sites, step_ms, psi):
                       f"matvecs); scaled by the Heff cost of all 2L site updates of a sweep pair"}
 
 
-def run_reference(args, rank, world):
-    """The reference's CPU algorithm for the path: the oracle restatement (the reference
-    itself cannot be built: its oml/LAPACK/ARPACK/PRIMME dependencies are absent), on
-    all host cores, on a bounded sample of the same workload."""
-    if rank != 0:
-        return None
+def reference_snapshot(args):
+    """The input of the timed step: the state the D <= D/2 schedule lines converge to
+    from seed 1234, grown to D by zero padding -- the same snapshot the GPU arm
+    starts from.  It is prepared (untimed) by the library's FP64 path when a GPU is
+    present; otherwise a random right-canonical MPS of the same shapes stands in."""
     import numpy as np
-    from oracle import oracle as O
-    O.build()
-    ncores = os.cpu_count() or 1
-    L, D, d = args.L, args.D, 2
-    # right-canonical random MPS of the final shapes (ramp min(d^k, D) from both ends)
-    dims = []
+    try:
+        import torch
+        gpu = torch.cuda.is_available()
+    except Exception:
+        gpu = False
+    if gpu:
+        import tensornetworks_b200 as T
+        ctx = T.Context(0)
+        H = T.Factory(ctx).Make1D_NN_HeisenbergHamiltonian(args.L, args.S, T.RegularLower, 1.0, 1.0, 0.0)
+        lines = schedule_for(args.D)
+        psi = H.CreateMPS(lines[0][1], 1e-12, 1e-12)
+        psi.InitializeWith(T.Random, seed=1234)
+        sched = T.IterationSchedule()
+        for (ms, Dm, dD) in lines[:-1]:
+            eps = T.Epsilons(1e-12)
+            eps.itsEigenSolverEpsilon = EPS_EIGEN
+            sched.Insert(T.IterationScheduleLine(ms, Dm, dD, eps))
+        if len(lines) > 1:
+            psi.FindVariationalGroundState(H, sched, T.SolverOptions(precision=T.FP64, krylov=KRYLOV))
+        sites = grow_sites([psi.GetSite(i) for i in range(1, args.L + 1)], args.D)
+        del psi, H
+        ctx.close()
+        return sites, True
+    L, D, d = args.L, args.D, int(round(2 * args.S + 1))
+    rng = np.random.default_rng(1234)
+    sites = []
     for i in range(L):
         l = 1 if i == 0 else min(D, d ** i, d ** (L - i))
         r = 1 if i == L - 1 else min(D, d ** (i + 1), d ** (L - i - 1))
-        dims.append((l, r))
-    rng = np.random.default_rng(1234)
-    sites = [rng.uniform(-1, 1, size=(d,) + dm) for dm in dims]
+        sites.append(rng.uniform(-1, 1, size=(d, l, r)))
+    return sites, False
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU algorithm for the path: the oracle restatement (the reference
+    itself cannot be built: its oml/LAPACK/ARPACK/PRIMME dependencies are absent), on
+    all host cores, on the same snapshot as the GPU arm.  A step is a bounded sample of
+    --cpu-sites bulk site updates, extrapolated to a sweep pair by the Heff cost of
+    every site; once per run a full half-sweep (all L-1 updates) is timed as well, as
+    the check of that extrapolation."""
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    O.build()
+    ncores = os.cpu_count() or 1
+    L, D, d = args.L, args.D, int(round(2 * args.S + 1))
+    sites, same = reference_snapshot(args)
     first = L // 2 - args.cpu_sites // 2
+    bulk = heff_flops(d, 5, 5, D, D)
+    w = sum(heff_flops(d, 5, 5, a.shape[1], a.shape[2]) / bulk for a in sites)
+    if args.warmup > 0:  # one untimed site update (page-in, thread start)
+        O.sweep_sample(L, args.S, sites, first, 1, krylov=KRYLOV, max_restarts=10, tol=EPS_EIGEN, nthreads=ncores)
     times = []
     for _ in range(max(1, args.steps)):
-        sec, nmv = O.sweep_sample(L, S_SPIN, sites, first, args.cpu_sites, krylov=KRYLOV, max_restarts=10,
+        sec, nmv = O.sweep_sample(L, args.S, sites, first, args.cpu_sites, krylov=KRYLOV, max_restarts=10,
                                   tol=EPS_EIGEN, nthreads=ncores)
         times.append(sec)
     per_site = sum(times) / len(times) / args.cpu_sites
-    bulk = heff_flops(d, 5, 5, D, D)
-    w = sum(heff_flops(d, 5, 5, a, b) / bulk for a, b in dims)
     value = per_site * 2.0 * w
+    check = None
+    if args.ref_half_sweep:
+        sec, nmv = O.sweep_sample(L, args.S, sites, 1, L - 1, krylov=KRYLOV, max_restarts=10, tol=EPS_EIGEN,
+                                  nthreads=ncores)
+        w_half = sum(heff_flops(d, 5, 5, a.shape[1], a.shape[2]) / bulk for a in sites[:L - 1])
+        check = {"half_sweep_measured_s": round(sec, 3), "half_sweep_extrapolated_s": round(per_site * w_half, 3),
+                 "ratio_measured_over_extrapolated": round(sec / (per_site * w_half), 3), "matvecs": nmv,
+                 "sweep_pair_from_measured_half_s": round(2.0 * sec, 3)}
     sample = (f"{args.cpu_sites} bulk D={D} site updates (Lanczos Krylov 20 tol 1e-10 + QR gauge + environment) "
-              f"of a random right-canonical L={L} MPS per step, scaled by the Heff cost of the 2L site updates "
-              f"of a sweep pair; oracle C++ restatement (reference not buildable here)")
+              f"of the {'same grown snapshot the GPU arm starts from (prepared untimed by the library FP64 path)' if same else 'random right-canonical MPS of the same shapes (no GPU to prepare the snapshot)'} "
+              f"per step, extrapolated to the 2L site updates of a sweep pair by their Heff cost; oracle C++ "
+              f"restatement (reference not buildable here)")
     out = {"metric": METRIC, "value": round(value, 3), "unit": unit_of(args),
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value * 1e3, 1),
            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic", "impl": "reference",
+           "data": "synthetic", "impl": "reference", "same_config": same,
+           "extrapolated_from_site_updates": args.cpu_sites,
            "config": {"workload": workload_of(args), "precision": "fp64 (CPU oracle restatement)"},
+           "half_sweep_check": check,
            "cpu_baseline": {"value": round(value, 3), "unit": unit_of(args), "cores": ncores, "kind": "port",
                             "sample": sample},
            "e2e": {"value": round(value, 3), "unit": unit_of(args), "h2d_bytes_per_step": 0,
@@ -583,7 +723,8 @@ def main():
         import torch
         import tensornetworks_b200 as T
         torch.cuda.set_device(local_rank)
-        t, flop = matvec_microbench(T, T.Context(local_rank), torch, args.D, args.precision, reps=max(1, args.steps))
+        t, flop = matvec_microbench(T, T.Context(local_rank), torch, args.D, args.precision, reps=max(1, args.steps),
+                                    S=args.S)
         print(json.dumps({"matvec_us": round(t * 1e6, 2), "flop": flop, "tflops": round(flop / t / 1e12, 3),
                           "D": args.D, "precision": args.precision}), flush=True)
     else:

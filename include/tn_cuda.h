@@ -182,6 +182,14 @@ int tn_mps_sweep(tn_mps psi, tn_hamiltonian H, int nsweeps, double eps_eigen,
                  const tn_solver_options* opt, tn_sweep_stats* stats);
 /* MPS::Normalize(DRight) followed by MPSImp::LoadHeffCaches (MPSImp_Variational.C:18-19). */
 int tn_mps_prepare_sweeps(tn_mps psi, tn_hamiltonian H);
+/* MPS::CalculateOneSiteDMs (MPS.H:63, MPSImp_ExpectationsAndDMs.C:59-71):
+ * L blocks of d x d, rho_host[(ia-1) d^2 + m d + n].  Right-normalises the
+ * state first and leaves it left-normalised, as the reference does. */
+int tn_mps_one_site_dms(tn_mps psi, double* rho_host);
+/* MPS::CalculateTwoSiteDMs (MPS.H:64, MPSImp_ExpectationsAndDMs.C:73-117): for
+ * the L(L-1)/2 pairs ia < ib in order (ia outer), d^4 values each,
+ * rho[((m d + m2) d + n) d + n2] with (m, n) on site ia and (m2, n2) on ib. */
+int tn_mps_two_site_dms(tn_mps psi, double* rho_host);
 /* Per-site Ritz energies of the last solves (MPSSite::itsEmin), L values. */
 int tn_mps_get_site_energies(tn_mps psi, double* E_host);
 
@@ -376,6 +384,14 @@ int tn_fullstate_get_amplitudes(tn_fullstate fs, double* host);
 /* FullStateImp::DoMatVecContraction (FullStateImp.C:207-217), the
  * SparseEigenSolverClient face: y = H x on device vectors of d^L. */
 int tn_fullstate_matvec(tn_fullstate fs, tn_hamiltonian h, const double* x, double* y);
+
+/* Measurement hook (no counterpart in the reference): device microseconds per
+ * step of the library's Lanczos Krylov kernels (CGS2 projections, update,
+ * next vector, tridiagonal decision), replayed from its CUDA graph on a
+ * diagonal operator of size N with a basis of m vectors; *bytes_per_step: the
+ * algorithmic HBM bytes of one step, (j + 4) N doubles averaged over the
+ * steps j plus the operator's read and write of 2 N doubles. */
+int tn_lanczos_probe(tn_ctx ctx, long long N, int m, double* us_per_step, double* bytes_per_step);
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,9 @@ SIGNATURES = {
     "tn_itebd_step": (_I, [_V, _D, _I, _I]),
     "tn_itebd_find_ground_state": (_I, [_V, _V, _I, _I, _I, _I, _D, _V]),
     "tn_itebd_orthogonalize": (_I, [_V, _I, _D, _I, _PD, _PI]),
+    "tn_mps_one_site_dms": (_I, [_V, _V]),
+    "tn_mps_two_site_dms": (_I, [_V, _V]),
+    "tn_lanczos_probe": (_I, [_V, C.c_longlong, _I, _PD, _PD]),
     "tn_fullstate_create": (_I, [_V, _ULL, _PV]),
     "tn_fullstate_destroy": (_I, [_V]),
     "tn_fullstate_get_size": (C.c_longlong, [_V]),

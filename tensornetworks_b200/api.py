@@ -311,6 +311,28 @@ class MPS:
         self.last_stats = st.as_dict()
         return self.last_stats
 
+    def CalculateOneSiteDMs(self) -> np.ndarray:
+        """MPS::CalculateOneSiteDMs: (L, d, d), rho[ia-1][m, n] (the state ends left-normalised)."""
+        d = self.H.Getd()
+        out = np.empty(self.L * d * d)
+        check(self._lib.tn_mps_one_site_dms(self.handle, out.ctypes.data), "tn_mps_one_site_dms")
+        return out.reshape(self.L, d, d)
+
+    def CalculateTwoSiteDMs(self) -> dict:
+        """MPS::CalculateTwoSiteDMs: {(ia, ib): rho (d, d, d, d)} for 1 <= ia < ib <= L,
+        indexed rho[m, m2, n, n2] as the reference's Matrix4 (m, n on ia; m2, n2 on ib)."""
+        d, L = self.H.Getd(), self.L
+        npairs = L * (L - 1) // 2
+        out = np.empty(npairs * d ** 4)
+        check(self._lib.tn_mps_two_site_dms(self.handle, out.ctypes.data), "tn_mps_two_site_dms")
+        out = out.reshape(npairs, d, d, d, d)
+        res, k = {}, 0
+        for ia in range(1, L):
+            for ib in range(ia + 1, L + 1):
+                res[(ia, ib)] = out[k]
+                k += 1
+        return res
+
     def SetLearnedCorrection(self, model: Optional["LearnedCorrection"]):
         """Attach (None: detach) the learned Davidson correction used when the
         options select eigensolver=DAVIDSON with use_learned=1."""

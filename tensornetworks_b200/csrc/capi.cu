@@ -365,6 +365,22 @@ int tn_mps_get_expectation_h2(tn_mps m, tn_hamiltonian h, double* E2) {
     return m->m.expectation(h->h.ops2, E2);
 }
 
+// MPSImp::CalculateOneSiteDMs (MPSImp_ExpectationsAndDMs.C:59-71): L blocks of d x d,
+// rho[(ia-1) d^2 + m d + n]; leaves the MPS left-normalised, as the reference.
+int tn_mps_one_site_dms(tn_mps m, double* rho_host) {
+    if (!m || !rho_host) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
+    return m->m.one_site_dms(rho_host);
+}
+
+// MPSImp::CalculateTwoSiteDMs (MPSImp_ExpectationsAndDMs.C:73-117): for every pair
+// ia < ib in order, d^4 values rho[((m d + m2) d + n) d + n2] (m, n on ia; m2, n2 on ib).
+int tn_mps_two_site_dms(tn_mps m, double* rho_host) {
+    if (!m || !rho_host) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
+    return m->m.two_site_dms(rho_host);
+}
+
 int tn_mps_find_variational_ground_state(tn_mps m, tn_hamiltonian h, const tn_sched_line* lines, int nlines,
                                          const tn_solver_options* opt, tn_sweep_stats* stats, double* variance) {
     if (!m || !h || !lines || nlines < 1 || h->h.L != m->m.L) return TN_BAD_ARG;
@@ -1095,6 +1111,70 @@ int tn_fullstate_matvec(tn_fullstate fs, tn_hamiltonian h, const double* x, doub
     TN_ON_DEVICE(fs->f.ctx->device);
     TN_CHECK(fs->f.set_hamiltonian(h->h.Jxy, h->h.Jz, h->h.hz));
     return fs->f.matvec(x, y, nullptr);
+}
+
+
+}  // extern "C"
+
+namespace {
+// y = (1 + i/n) x: a diagonal operator with distinct eigenvalues, so that the
+// Krylov space never closes early
+__global__ void diag_probe_kernel(const double* __restrict__ x, double* __restrict__ y, long long n, const int* skip) {
+    if (skip && *skip) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = (1.0 + (double)i / (double)n) * x[i];
+}
+}  // namespace
+
+extern "C" {
+
+// Device time per Lanczos step of the library's Krylov kernels (CGS2 dots and
+// updates, next vector, tridiagonal decision) on a diagonal operator, the
+// steps replayed from the CUDA graph as in a sweep.  A measurement hook with
+// no counterpart in the reference.
+int tn_lanczos_probe(tn_ctx c, long long N, int m, double* us_per_step, double* bytes_per_step) {
+    if (!c || N < 64 || m < 2 || !us_per_step) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
+    Ctx& cx = c->c;
+    DevBuf xb;
+    TN_CHECK(xb.ensure(sizeof(double) * (size_t)N));
+    const int g = (int)std::min<long long>((N + 255) / 256, (long long)cx.sm_count * 8);
+    MatvecFn mv = [&](const double* x, double* y, const int* skip) -> int {
+        diag_probe_kernel<<<g, 256, 0, cx.stream>>>(x, y, N, skip);
+        TN_LAUNCH_CHECK();
+        return (int)TN_OK;
+    };
+    const bool prof0 = cx.prof;
+    cx.prof = true;
+    unsigned long long key = hash_val(HASH_SEED, 0x70726f6265ULL);
+    key = hash_val(key, N);
+    key = hash_val(key, m);
+    int rc = TN_OK;
+    LzResult r{};
+    for (int pass = 0; pass < 2 && rc == TN_OK; ++pass) {  // pass 0 records the graph
+        cx.prof_ms[2] = 0;
+        cx.prof_steps = 0;
+        rc = fill(xb.as<double>(), N, 1.0, cx.stream);
+        if (rc == TN_OK) rc = lanczos_solve(cx, N, xb.as<double>(), m, 1, 1e-300, mv, &r, 0.0, key);
+    }
+    const double ms = cx.prof_ms[2];
+    const long long steps = cx.prof_steps;
+    cx.prof = prof0;
+    TN_CHECK(rc);
+    if (steps < 1) {
+        set_error("tn_lanczos_probe: no Krylov step was timed");
+        return TN_CUDA_ERROR;
+    }
+    *us_per_step = ms * 1e3 / (double)steps;
+    if (bytes_per_step) {
+        // (j + 4) N doubles per step j of the CGS2 step (basis reads for the two
+        // projection passes, the update and the next vector), plus the diagonal
+        // operator's read and write
+        double b = 0;
+        for (long long j = 1; j <= steps; ++j) b += (double)(j + 4) * N * 8.0;
+        *bytes_per_step = b / (double)steps + 2.0 * N * 8.0;
+    }
+    return TN_OK;
 }
 
 }  // extern "C"

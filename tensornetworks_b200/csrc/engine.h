@@ -97,6 +97,11 @@ struct MPSState {
     int sweep(bool left, double epsEigen);
     int increase_bond_dims(int D);
     int expectation(const std::vector<SiteMPO>& ops, double* E);
+    // reduced density matrices (dms.cu): L d x d blocks; for the pairs ia < ib in
+    // order, d^4 values rho[((m d + m2) d + n) d + n2]
+    int one_site_dms(double* out_host);
+    int two_site_dms(double* out_host);
+    int dm_scatter(const double* dots, double* rho);
     int find_ground_state(const tn_sched_line* lines, int nlines, const tn_solver_options* opt,
                           tn_sweep_stats* stats);
     int sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options* opt, tn_sweep_stats* stats);

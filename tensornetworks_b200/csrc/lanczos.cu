@@ -212,56 +212,6 @@ __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __res
     }
 }
 
-// lz_dots_kernel fused with the matvec's last stage: w[m][e] = sum_w2
-// Yp[(m*Dw2 + w2)][e] (FP32 partials summed in FP64, in order) is formed and
-// written by the first chunk's pass, which dots it with V at once.
-__global__ void lz_tail_dots_kernel(const float* __restrict__ Yp, int Dw2, long long blk,
-                                    const double* __restrict__ V, double* __restrict__ w, long long N,
-                                    double* partial, LzState* st) {
-    pdl_wait();
-    if (st->done) return;
-    __shared__ double sh[KCHUNK * 32];
-    __shared__ double res[KCHUNK];
-    __shared__ bool last;
-    const int j = st->j;
-    const int nk = j + 1;
-    for (int k0 = 0; k0 < nk; k0 += KCHUNK) {
-        double v[KCHUNK] = {0};
-        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
-             i += (long long)gridDim.x * blockDim.x) {
-            double wi;
-            if (k0 == 0) {
-                const long long m = i / blk, r = i - m * blk;
-                const float* src = Yp + (long long)m * Dw2 * blk + r;
-                wi = 0.0;
-                for (int q = 0; q < Dw2; ++q) wi += (double)src[(long long)q * blk];
-                w[i] = wi;
-            } else {
-                wi = w[i];
-            }
-#pragma unroll
-            for (int q = 0; q < KCHUNK; ++q)
-                if (k0 + q < nk) v[q] = fma(V[(long long)(k0 + q) * N + i], wi, v[q]);
-        }
-        block_sum_chunk(v, res, sh);
-        if (threadIdx.x < KCHUNK && k0 + threadIdx.x < nk)
-            partial[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned int prev = atomicAdd(&st->counter, 1u);
-        last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last) {
-        __shared__ double hsum[LZ_MAXK + KCHUNK];
-        reduce_partials(partial, gridDim.x, LZ_MAXK, nk, hsum, sh);
-        for (int k = threadIdx.x; k < nk; k += blockDim.x) st->h[k] = hsum[k];
-        if (threadIdx.x == 0) st->counter = 0;
-    }
-}
-
 // w' = w - V h;  h2 = V^T w';  nrm2 = |w'|^2.  The last block forms alpha_j and
 // beta_j; the tridiagonal eigenproblem and the decision to stop follow in
 // block 0 of lz_next_kernel, beside the other blocks' vector work.
@@ -512,24 +462,11 @@ inline int vec_grid(long long N, int sm) {
 
 }  // namespace
 
-// w = Heff xcur and h = V^T w: the matvec, then the dots; when the matvec leaves
-// its last stage to the caller, that stage and the dots are one kernel.
+// w = Heff xcur and h = V^T w: the matvec, then the dots.
 int step_matvec_dots(Ctx& c, const MatvecFn& mv, int grid, const double* V, double* w, const double* xcur,
                      long long N, double* partial, LzState* s) {
-    cudaStream_t st = c.stream;
-    MatvecTail tail;
-    c.take_tail = &tail;
-    const int rc = mv(xcur, w, &s->done);
-    c.take_tail = nullptr;
-    TN_CHECK(rc);
-    if (tail.deferred && (long long)tail.d * tail.blk == N)
-        return launch_pdl(lz_tail_dots_kernel, grid, LZ_THREADS, 0, st, tail.Yp, tail.Dw2, tail.blk, V, w, N, partial,
-                          s);
-    if (tail.deferred) {
-        set_error("lanczos: matvec tail of %lld elements for a vector of %lld", (long long)tail.d * tail.blk, N);
-        return TN_BAD_SHAPE;
-    }
-    return launch_pdl(lz_dots_kernel, grid, LZ_THREADS, 0, st, V, (const double*)w, N, partial, s);
+    TN_CHECK(mv(xcur, w, &s->done));
+    return launch_pdl(lz_dots_kernel, grid, LZ_THREADS, 0, c.stream, V, (const double*)w, N, partial, s);
 }
 
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,

@@ -2,7 +2,7 @@
 // (distributed shared memory) reduction; the two contractions of the fused
 // split-precision Heff matvec.  See tc_chain.cu.
 #pragma once
-#include "tc_gemm.h"
+#include "tma_maps.h"
 
 namespace tnb {
 

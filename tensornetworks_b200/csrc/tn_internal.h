@@ -160,16 +160,6 @@ struct LzGraph {
     unsigned long long kernels_per_iter = 0;
 };
 
-// The last stage of a split-precision matvec, y[m][e] = sum_w2 Yp[(m*Dw2 + w2)][e]
-// (FP32 partials -> FP64), left to the caller when it asks for it (so that the
-// Lanczos step can fuse it with the dot products of y).
-struct MatvecTail {
-    bool deferred = false;
-    const float* Yp = nullptr;
-    int d = 0, Dw2 = 0;
-    long long blk = 0;
-};
-
 // Execution context (one per tn_ctx handle).
 struct Ctx {
     int device = 0;
@@ -207,7 +197,6 @@ struct Ctx {
     DevBuf apiw[3];        // staging copies of the dense-solver entry points
     HostBuf pinned;
     int sm_count = 148;
-    MatvecTail* take_tail = nullptr;  // set around a matvec call that may leave its last stage
     bool use_persistent_qr = true;  // TN_NO_PERSISTENT_QR=1: the two-stream look-ahead QR instead
     long long qr_spin_limit = 1LL << 21;  // polls per wait in the persistent QR (TN_QR_SPIN_LIMIT)
     // cache of the last MPO term list uploaded through the C ABI
