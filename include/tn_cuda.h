@@ -89,7 +89,7 @@ typedef struct {
     int verbose;         /* 1: print the reference's per-sweep log line     */
     double mixed_tol;    /* residual target of the split-precision Krylov
                             phase relative to the norm of its tridiagonal
-                            matrix (0: 1e-7 for MIXED, 1e-9 for MIXED_HI);
+                            matrix (0: 2e-6 for MIXED, 1e-9 for MIXED_HI);
                             the phase also stops when its residual no
                             longer falls (the operator's noise floor)       */
     double refine_tol;   /* FP64 residual above which an FP64 Lanczos

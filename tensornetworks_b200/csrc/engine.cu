@@ -581,7 +581,7 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     int restarts = opt.max_restarts > 0 ? opt.max_restarts : 10;
     // residual target: the requested tolerance, but not below the split operator's
     // noise floor relative to |T| (BF16x3 ~ 2^-16, BF16x6 ~ FP32 accumulation)
-    const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-7);
+    const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 2e-6);
     // the operator: everything the recorded matvec launches depend on
     unsigned long long key = hash_val(HASH_SEED, 0x6d69786564ULL);
     key = hash_val(key, s);
@@ -775,7 +775,7 @@ int MPSState::refine_site_davidson(int ia, double epsEigen) {
         const double sigma = mixed_shift_host(msite, st);
         TN_CHECK(shift_vector(diagbuf.as<double>(), N, -sigma, st));
         mv = [&](const double* x, double* y, const int* skip) { return heff_matvec_mixed(*ctx, msite, x, y, skip); };
-        tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 1e-7);
+        tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 2e-6);
         key = hash_val(key, ns);
         for (const DevBuf* b : {&msite.Fs, &msite.Gc, &msite.Xs, &msite.Ps, &msite.segs, &msite.shifts, &msite.err})
             key = hash_val(key, b->p);

@@ -65,6 +65,29 @@ __device__ void reduce_partials(const double* partial, int nb, int stride, int n
     }
 }
 
+// acc + sgn * sum_{k < nk} c[k] V[k N + i] with the basis loads issued eight at
+// a time (independent, all in flight before their FMAs): a thread touches only a
+// few elements, so without this the loop is one load latency per basis vector.
+__device__ __forceinline__ double basis_combine(const double* __restrict__ V, long long N, long long i,
+                                                const double* c, int nk, double sgn, double acc) {
+    int k = 0;
+    for (; k + 8 <= nk; k += 8) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = __ldg(V + (long long)(k + q) * N + i);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc = fma(sgn * c[k + q], v[q], acc);
+    }
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (k + q < nk) v[q] = __ldg(V + (long long)(k + q) * N + i);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (k + q < nk) acc = fma(sgn * c[k + q], v[q], acc);
+    return acc;
+}
+
 // ---- kernels ---------------------------------------------------------------
 
 // A restart's reset (first: the whole solve's); with a step-loop handle it
@@ -229,7 +252,7 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
     __syncthreads();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         double wi = w[i];
-        for (int k = 0; k < nk; ++k) wi = fma(-hs[k], V[(long long)k * N + i], wi);
+        wi = basis_combine(V, N, i, hs, nk, -1.0, wi);
         w[i] = wi;
     }
     // second projection (h2) and the norm of w'
@@ -330,7 +353,7 @@ __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict_
     double* vn = V + (long long)(j + 1) * N;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         double wi = w[i];
-        for (int k = 0; k < nk; ++k) wi = fma(-hs[k], V[(long long)k * N + i], wi);
+        wi = basis_combine(V, N, i, hs, nk, -1.0, wi);
         wi *= inv;
         vn[i] = wi;
         xcur[i] = wi;
@@ -387,7 +410,7 @@ __global__ void lz_ritz_vector_kernel(const double* __restrict__ V, double* __re
     __syncthreads();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         double s = 0;
-        for (int k = 0; k < n; ++k) s = fma(ys[k], V[(long long)k * N + i], s);
+        s = basis_combine(V, N, i, ys, n, 1.0, s);
         x[i] = s;
     }
 }
