@@ -406,6 +406,15 @@ def run_ours(args, rank, world, local_rank):
         if clocks:
             clocks.stop()
         t_step = max_over_ranks(sum(step_ms) / len(step_ms) / 1e3, dist, "cuda")
+        # one more step, untimed, with CUDA events around every site's phases
+        opts.phase_timing = 1
+        ph = step()
+        opts.phase_timing = 0
+        phases = {"refine_ms": round(ph["refine_ms"], 3), "gauge_ms": round(ph["gauge_ms"], 3),
+                  "env_ms": round(ph["env_ms"], 3), "sweep_ms": round(ph["sweep_ms"], 3)}
+        if ph["sweep_ms"] > 0:
+            phases["gauge_share"] = round(ph["gauge_ms"] / ph["sweep_ms"], 4)
+            phases["refine_share"] = round(ph["refine_ms"] / ph["sweep_ms"], 4)
         E_step = psi.GetExpectation(H)
         last = dict(psi.last_stats)
         var = schedule_s = sched_stats = E_sched = None
@@ -420,7 +429,7 @@ def run_ours(args, rank, world, local_rank):
             E_sched = psi.GetExpectation(H)
         return dict(psi=psi, opts=opts, var=var, schedule_s=schedule_s, sched_stats=sched_stats, E_sched=E_sched,
                     t_step=t_step, step_ms=step_ms, matvecs=matvecs, flops=flops, launches=launches,
-                    clocks=clocks, E_after=E_step, grown=grown, step=step, last=last)
+                    clocks=clocks, E_after=E_step, grown=grown, step=step, last=last, phases=phases)
 
     main_run = run_path(args.precision, True)
     psi, opts, var = main_run["psi"], main_run["opts"], main_run["var"]
@@ -456,7 +465,8 @@ def run_ours(args, rank, world, local_rank):
                     "energy_per_bond": ref64["E_after"] / (args.L - 1),
                     "dE_per_site_schedule": abs(E_sched - ref64["E_sched"]) / args.L,
                     "dE_per_site_after_steps": abs(E_after - ref64["E_after"]) / args.L,
-                    "matvecs_per_step": ref64["matvecs"] / args.steps}
+                    "matvecs_per_step": ref64["matvecs"] / args.steps,
+                    "phases_device_ms": ref64["phases"]}
         del ref64
         # the FP64 sweep stopped by the split-precision path's rule: residual relative
         # to |T| (2e-6, 1e-9 for mixed_hi) with the stall test, so that the speed-up
@@ -468,7 +478,8 @@ def run_ours(args, rank, world, local_rank):
             "speedup_of_split_precision": round(same["t_step"] / t_step, 3),
             "speedup_over_fp64_tol_1e-10": round(fp64_cmp["value"] / same["t_step"], 3),
             "dE_per_site_vs_split_precision": abs(E_after - same["E_after"]) / args.L,
-            "matvecs_per_step": same["matvecs"] / args.steps}
+            "matvecs_per_step": same["matvecs"] / args.steps,
+            "phases_device_ms": same["phases"]}
         del same
 
     learned = None
@@ -522,6 +533,7 @@ def run_ours(args, rank, world, local_rank):
                        "l2": "inputs > L2 (site tensors + environments ~ 0.6 GB at D=256)"},
             "heff_tflops_sweep": round(flops / (sum(step_ms) / 1e3) / 1e12, 4),
             "matvecs_per_step": main_run["matvecs"] / args.steps,
+            "phases_device_ms": main_run["phases"],
             "fp64_gpu": fp64_cmp,
             "schedule_s": round(schedule_s, 3),
             "schedule_sweep_ms": round(sched_stats["sweep_ms"], 1),

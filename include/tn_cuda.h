@@ -101,6 +101,10 @@ typedef struct {
                             stop on a stalled residual as the split-precision
                             phase (0: the absolute eps_eigen only).  Lets the
                             FP64 sweep stop by the mixed path's rule.       */
+    int phase_timing;    /* 1: CUDA events on the library stream around each
+                            site's eigen-solve, gauge move and environment
+                            update; their device times go to the refine_ms,
+                            gauge_ms and env_ms statistics                  */
 } tn_solver_options;
 
 /* Per-run statistics, device-timed with CUDA events. */
@@ -122,6 +126,9 @@ typedef struct {
                                took over) plus FP64 refinements of the mixed
                                path                                          */
     long long learned_steps; /* Davidson corrections the learned MLP made    */
+    double refine_ms;       /* device time of the site eigen-solves, the     */
+    double gauge_ms;        /* gauge moves (QR/LQ and the neighbour product) */
+    double env_ms;          /* and the environment updates (phase_timing=1)  */
 } tn_sweep_stats;
 
 /* ---- context ------------------------------------------------------------- */
@@ -182,6 +189,28 @@ int tn_mps_sweep(tn_mps psi, tn_hamiltonian H, int nsweeps, double eps_eigen,
                  const tn_solver_options* opt, tn_sweep_stats* stats);
 /* MPS::Normalize(DRight) followed by MPSImp::LoadHeffCaches (MPSImp_Variational.C:18-19). */
 int tn_mps_prepare_sweeps(tn_mps psi, tn_hamiltonian H);
+/* One line of an imaginary-time schedule: the fields of IterationScheduleLine
+ * (IterationSchedule.H:27-35) and Epsilons (Epsilons.H:11-26) that
+ * MPSImp::FindiTimeGroundState reads. */
+typedef struct {
+    int    max_iter;         /* itsMaxGSSweepIterations                        */
+    int    Dmax;             /* itsDmax (the MPS compressor's Dmax)             */
+    int    max_opt_iter;     /* itsMaxOptimizeIterations                        */
+    int    order;            /* itsTrotterOrder: 1 (first) or 2 (second)        */
+    double dt;               /* itsdt                                           */
+    double eps_energy;       /* itsDelatEnergy1Epsilon                          */
+    double eps_lambda;       /* itsDeltaLambdaEpsilon                           */
+    double eps_norm;         /* itsDelatNormEpsilon (Optimize's stop)           */
+    double eps_mps_compress; /* itsMPSCompressEpsilon (0: Dmax only)            */
+} tn_itime_line;
+/* MPS::FindiTimeGroundState(H, schedule) (MPSImp_iTime.C:18-88): per line, the
+ * Trotter operator of exp(-dt H) (first or second order, the exact product of
+ * the gate layers), applied, SVD-compressed both ways and variationally
+ * optimised towards the uncompressed product, until |dE| and the bond-value
+ * change fall below the line's epsilons or the energy rises.  *variance:
+ * <H^2> - <H>^2 at the end; iters_out[line] (may be null): iterations run. */
+int tn_mps_find_itime_ground_state(tn_mps psi, tn_hamiltonian h, const tn_itime_line* lines, int nlines,
+                                   double* variance, int* iters_out);
 /* MPS::CalculateOneSiteDMs (MPS.H:63, MPSImp_ExpectationsAndDMs.C:59-71):
  * L blocks of d x d, rho_host[(ia-1) d^2 + m d + n].  Right-normalises the
  * state first and leaves it left-normalised, as the reference does. */

@@ -5,4 +5,4 @@ from ._capi import LIB_PATH, TNError, load  # noqa: F401
 from .api import (  # noqa: F401
     DAVIDSON, FP64, LANCZOS, MIXED, MIXED_HI, Context, CudaEigenSolver, CudaQRSolver, CudaSVDSolver, DLeft, DRight,
     Epsilons, Factory, Hamiltonian, IterationSchedule, IterationScheduleLine, LearnedCorrection, MPS, Random,
-    FullState, RegularLower, RegularUpper, SolverOptions, SVCompressor, TrainingSet, default_context, iTEBDState)
+    FirstOrder, FullState, RegularLower, SecondOrder, RegularUpper, SolverOptions, SVCompressor, TrainingSet, default_context, iTEBDState)

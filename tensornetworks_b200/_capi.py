@@ -37,10 +37,17 @@ class SchedLine(C.Structure):
                 ("eps_energy", C.c_double), ("eps_lambda", C.c_double), ("eps_eigen", C.c_double)]
 
 
+class ITimeLine(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("Dmax", C.c_int), ("max_opt_iter", C.c_int), ("order", C.c_int),
+                ("dt", C.c_double), ("eps_energy", C.c_double), ("eps_lambda", C.c_double),
+                ("eps_norm", C.c_double), ("eps_mps_compress", C.c_double)]
+
+
 class SolverOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("eigensolver", C.c_int), ("krylov", C.c_int),
                 ("max_restarts", C.c_int), ("use_learned", C.c_int), ("verbose", C.c_int),
-                ("mixed_tol", C.c_double), ("refine_tol", C.c_double), ("fp64_tol_rel", C.c_double)]
+                ("mixed_tol", C.c_double), ("refine_tol", C.c_double), ("fp64_tol_rel", C.c_double),
+                ("phase_timing", C.c_int)]
 
 
 class SweepStats(C.Structure):
@@ -48,7 +55,8 @@ class SweepStats(C.Structure):
                 ("total_sweeps", C.c_int), ("final_D", C.c_int), ("matvecs", C.c_longlong),
                 ("matvecs_fp64", C.c_longlong), ("heff_flop", C.c_double), ("heff_ms", C.c_double),
                 ("sweep_ms", C.c_double), ("last_dE", C.c_double), ("last_dlambda", C.c_double),
-                ("not_converged", C.c_int), ("fallbacks", C.c_int), ("learned_steps", C.c_longlong)]
+                ("not_converged", C.c_int), ("fallbacks", C.c_int), ("learned_steps", C.c_longlong),
+                ("refine_ms", C.c_double), ("gauge_ms", C.c_double), ("env_ms", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -98,6 +106,7 @@ SIGNATURES = {
     "tn_itebd_step": (_I, [_V, _D, _I, _I]),
     "tn_itebd_find_ground_state": (_I, [_V, _V, _I, _I, _I, _I, _D, _V]),
     "tn_itebd_orthogonalize": (_I, [_V, _I, _D, _I, _PD, _PI]),
+    "tn_mps_find_itime_ground_state": (_I, [_V, _V, _V, _I, _PD, _V]),
     "tn_mps_one_site_dms": (_I, [_V, _V]),
     "tn_mps_two_site_dms": (_I, [_V, _V]),
     "tn_lanczos_probe": (_I, [_V, C.c_longlong, _I, _PD, _PD]),

@@ -97,22 +97,44 @@ class Epsilons:
                 setattr(self, f, self.default_eps)
 
 
+FirstOrder, SecondOrder = 1, 2  # TrotterOrder (Enums.H:13)
+
+
 class IterationScheduleLine:
-    """IterationScheduleLine(maxiter, Dmax, [DeltaD,] eps) (IterationSchedule.C:9-36)."""
+    """IterationScheduleLine (IterationSchedule.H:13-35, IterationSchedule.C:9-100):
+    variational forms (maxiter, Dmax, [DeltaD,] eps) and imaginary-time forms
+    (maxiter, Dmax, [DeltaD,] dt, order, eps) and
+    (maxiter, Dmax, DeltaD, maxOptIter, dt, order, eps)."""
 
     def __init__(self, maxiter: int, Dmax: int, *args):
+        DeltaD, nopt, dt, order = 1, 1, 0.0, FirstOrder
         if len(args) == 1:
-            DeltaD, eps = 1, args[0]
+            eps = args[0]
         elif len(args) == 2:
             DeltaD, eps = args
+        elif len(args) == 3:
+            dt, order, eps = args
+        elif len(args) == 4:
+            DeltaD, dt, order, eps = args
+        elif len(args) == 5:
+            DeltaD, nopt, dt, order, eps = args
         else:
-            raise TypeError("IterationScheduleLine(maxiter, Dmax, [DeltaD,] eps)")
+            raise TypeError("IterationScheduleLine(maxiter, Dmax, [DeltaD, [maxOptIter,]] [dt, order,] eps)")
         if maxiter <= 0 or Dmax <= 0 or DeltaD <= 0:
             raise ValueError("maxiter, Dmax and DeltaD must be positive")
         self.itsMaxGSSweepIterations = int(maxiter)
         self.itsDmax = int(Dmax)
         self.itsDeltaD = int(DeltaD)
+        self.itsMaxOptimizeIterations = int(nopt)
+        self.itsdt = float(dt)
+        self.itsTrotterOrder = int(order)
         self.itsEps = eps
+
+    def to_itime(self) -> capi.ITimeLine:
+        e = self.itsEps
+        return capi.ITimeLine(self.itsMaxGSSweepIterations, self.itsDmax, self.itsMaxOptimizeIterations,
+                              self.itsTrotterOrder, self.itsdt, e.itsDelatEnergy1Epsilon, e.itsDeltaLambdaEpsilon,
+                              e.itsDelatNormEpsilon, e.itsMPSCompressEpsilon)
 
     def to_c(self) -> capi.SchedLine:
         e = self.itsEps
@@ -142,11 +164,12 @@ class SolverOptions:
     mixed_tol: float = 0.0
     refine_tol: float = 0.0
     fp64_tol_rel: float = 0.0
+    phase_timing: int = 0
 
     def to_c(self):
         return capi.SolverOptions(self.precision, self.eigensolver, self.krylov, self.max_restarts,
                                   self.use_learned, self.verbose, self.mixed_tol, self.refine_tol,
-                                  self.fp64_tol_rel)
+                                  self.fp64_tol_rel, self.phase_timing)
 
 
 # ---------------------------------------------------------------------------
@@ -310,6 +333,17 @@ class MPS:
                                      C.byref(st)), "tn_mps_sweep")
         self.last_stats = st.as_dict()
         return self.last_stats
+
+    def FindiTimeGroundState(self, H: Hamiltonian, schedule: IterationSchedule) -> float:
+        """MPS::FindiTimeGroundState (MPSImp_iTime.C:18-88): returns <H^2> - <H>^2;
+        the iterations of each line are kept in last_itime_iterations."""
+        lines = (capi.ITimeLine * len(schedule))(*[ln.to_itime() for ln in schedule.lines])
+        var = C.c_double()
+        iters = (C.c_int * len(schedule))()
+        check(self._lib.tn_mps_find_itime_ground_state(self.handle, H.handle, lines, len(schedule), C.byref(var),
+                                                       iters), "tn_mps_find_itime_ground_state")
+        self.last_itime_iterations = list(iters)
+        return var.value
 
     def CalculateOneSiteDMs(self) -> np.ndarray:
         """MPS::CalculateOneSiteDMs: (L, d, d), rho[ia-1][m, n] (the state ends left-normalised)."""

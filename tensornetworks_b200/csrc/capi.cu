@@ -158,7 +158,9 @@ int tn_ctx_create(int device, tn_ctx* out) {
     c->c.device = device;
     c->c.sm_count = prop.multiProcessorCount;
     if (const char* ng = std::getenv("TN_NO_GRAPHS")) c->c.use_graphs = !(ng[0] == '1');
+    if (const char* nf = std::getenv("TN_NO_FUSED_LZ")) c->c.use_fused_lz = !(nf[0] == '1');
     if (const char* np = std::getenv("TN_NO_PERSISTENT_QR")) c->c.use_persistent_qr = !(np[0] == '1');
+    if (const char* fq = std::getenv("TN_QR_FORWARD_Q")) c->c.qr_forward_q = (fq[0] != '0');
     if (const char* sl = std::getenv("TN_QR_SPIN_LIMIT")) c->c.qr_spin_limit = std::max(1LL, std::atoll(sl));
     TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.own_stream, cudaStreamNonBlocking));
     c->c.stream = c->c.own_stream;
@@ -363,6 +365,20 @@ int tn_mps_get_expectation_h2(tn_mps m, tn_hamiltonian h, double* E2) {
     if (!m || !h || !E2 || h->h.L != m->m.L) return TN_BAD_ARG;
     TN_ON_DEVICE(m->m.ctx->device);
     return m->m.expectation(h->h.ops2, E2);
+}
+
+int tn_mps_find_itime_ground_state(tn_mps m, tn_hamiltonian h, const tn_itime_line* lines, int nlines,
+                                   double* variance, int* iters_out) {
+    if (!m || !h || !lines || nlines < 1 || h->h.L != m->m.L) return TN_BAD_ARG;
+    TN_ON_DEVICE(m->m.ctx->device);
+    for (int i = 0; i < nlines; ++i)
+        if (lines[i].max_iter < 1 || lines[i].Dmax < 1 || (lines[i].order != 1 && lines[i].order != 2) ||
+            !(lines[i].dt > 0)) {
+            set_error("imaginary-time schedule line %d invalid", i);
+            return TN_BAD_ARG;
+        }
+    m->m.H = &h->h;
+    return m->m.itime_ground_state(lines, nlines, variance, iters_out);
 }
 
 // MPSImp::CalculateOneSiteDMs (MPSImp_ExpectationsAndDMs.C:59-71): L blocks of d x d,

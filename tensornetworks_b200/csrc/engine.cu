@@ -190,6 +190,7 @@ int Hamiltonian::build() {
 // MPS
 // ---------------------------------------------------------------------------
 MPSState::~MPSState() {
+    for (auto e : phase_ev) cudaEventDestroy(e);
     for (auto p : A) delete p;
     for (auto p : Lenv) delete p;
     for (auto p : Renv) delete p;
@@ -869,18 +870,28 @@ int MPSState::sweep(bool left, double epsEigen) {
     auto secs = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
         return std::chrono::duration<double>(b - a).count();
     };
+    const bool dev_phases = opt.phase_timing != 0;
+    if (dev_phases) TN_CHECK(phase_events_ensure((size_t)4 * L));
+    auto mark = [&](int step, int k) -> int {
+        if (dev_phases) TN_CUDA_CHECK(cudaEventRecord(phase_ev[(size_t)4 * step + k], ctx->stream));
+        return TN_OK;
+    };
     for (int step = 0; step < L; ++step) {
         const int ia = left ? 1 + step : L - step;
         auto t0 = now();
         const unsigned long long n0 = launch_count();
+        TN_CHECK(mark(step, 0));
         TN_CHECK(refine_site(ia, epsEigen));
+        TN_CHECK(mark(step, 1));
         auto t1 = now();
         const unsigned long long n1 = launch_count();
         TN_CHECK(normalize_site(ia, left));
+        TN_CHECK(mark(step, 2));
         auto t2 = now();
         const unsigned long long n2 = launch_count();
         if (left && ia < L) TN_CHECK(compute_left_env(ia));
         if (!left && ia > 1) TN_CHECK(compute_right_env(ia));
+        TN_CHECK(mark(step, 3));
         auto t3 = now();
         if (prof) {
             t_refine += secs(t0, t1);
@@ -896,7 +907,25 @@ int MPSState::sweep(bool left, double epsEigen) {
         }
     }
     TN_CHECK(rq_collect());
+    if (dev_phases) {
+        TN_CUDA_CHECK(cudaEventSynchronize(phase_ev[(size_t)4 * (L - 1) + 3]));
+        for (int step = 0; step < L; ++step)
+            for (int k = 0; k < 3; ++k) {
+                float ms = 0;
+                TN_CUDA_CHECK(cudaEventElapsedTime(&ms, phase_ev[(size_t)4 * step + k], phase_ev[(size_t)4 * step + k + 1]));
+                phase_ms[k] += ms;
+            }
+    }
     return check_device_error(*ctx);
+}
+
+int MPSState::phase_events_ensure(size_t n) {
+    while (phase_ev.size() < n) {
+        cudaEvent_t e = nullptr;
+        TN_CUDA_CHECK(cudaEventCreate(&e));
+        phase_ev.push_back(e);
+    }
+    return TN_OK;
 }
 
 // MPSImp::IncreaseBondDimensions (MPSImp.C:123-147) with Bond::NewBondDimension (Bond.C:60-84).
@@ -977,6 +1006,7 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
     not_converged = fallbacks = 0;
     learned_steps = learned_stalls = 0;
     t_refine = t_gauge = t_env = t_bond = 0;
+    phase_ms[0] = phase_ms[1] = phase_ms[2] = 0;
     n_refine = n_gauge = n_env = 0;
     ctx->prof = opt.verbose >= 4;
     for (double& v : ctx->prof_ms) v = 0;
@@ -1021,6 +1051,9 @@ int MPSState::sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options*
         stats->not_converged = not_converged;
         stats->fallbacks = fallbacks + (int)learned_stalls;
         stats->learned_steps = learned_steps;
+        stats->refine_ms = phase_ms[0];
+        stats->gauge_ms = phase_ms[1];
+        stats->env_ms = phase_ms[2];
     }
     return TN_OK;
 }
@@ -1042,6 +1075,7 @@ int MPSState::find_ground_state(const tn_sched_line* lines, int nlines, const tn
     heff_flop = 0;
     not_converged = fallbacks = 0;
     learned_steps = learned_stalls = 0;
+    phase_ms[0] = phase_ms[1] = phase_ms[2] = 0;
     TN_CHECK(normalize_all(false));
     TN_CHECK(load_heff_caches());
     double E1 = 0, E2 = 0, DE2 = 0, dE = 0, dl = 0;
@@ -1100,6 +1134,9 @@ int MPSState::find_ground_state(const tn_sched_line* lines, int nlines, const tn
         stats->not_converged = not_converged;
         stats->fallbacks = fallbacks + (int)learned_stalls;
         stats->learned_steps = learned_steps;
+        stats->refine_ms = phase_ms[0];
+        stats->gauge_ms = phase_ms[1];
+        stats->env_ms = phase_ms[2];
     }
     return TN_OK;
 }

@@ -30,6 +30,12 @@ struct Hamiltonian {
     int build();
 };
 
+// Site tensors of a second MPS (the imaginary-time target |psi2>), 1-based.
+struct SiteSet {
+    std::vector<DevBuf*> A;
+    std::vector<int> D1, D2;
+};
+
 struct MPSState {
     Ctx* ctx = nullptr;
     Hamiltonian* H = nullptr;
@@ -76,6 +82,11 @@ struct MPSState {
     // phase timing (verbose >= 2): seconds in refine / gauge / environment / bond values
     double t_refine = 0, t_gauge = 0, t_env = 0, t_bond = 0;
     unsigned long long n_refine = 0, n_gauge = 0, n_env = 0;  // launches per phase (verbose >= 2)
+    // device phase timing (opt.phase_timing): four events per site of a half-sweep,
+    // read after the half-sweep; milliseconds in refine / gauge / environment
+    std::vector<cudaEvent_t> phase_ev;
+    double phase_ms[3] = {0, 0, 0};
+    int phase_events_ensure(size_t n);
 
     ~MPSState();
     int init(Hamiltonian* h, int D);
@@ -102,6 +113,15 @@ struct MPSState {
     int one_site_dms(double* out_host);
     int two_site_dms(double* out_host);
     int dm_scatter(const double* dots, double* rho);
+    // imaginary-time evolution (itime.cu)
+    int site_reserve(int ia, size_t n);
+    int trotter_mpo(double dt, int order, std::vector<SiteMPO>& out) const;
+    int apply_mpo_inplace(const std::vector<SiteMPO>& W);
+    int svd_compress_sweep(bool left, int Dmax, double eps, std::vector<std::vector<double>>* svals);
+    int overlap_left(int ia, const SiteSet& P2, std::vector<DevBuf*>& Lo);
+    int overlap_right(int ia, const SiteSet& P2, std::vector<DevBuf*>& Ro);
+    int overlap_site(int ia, const SiteSet& P2, std::vector<DevBuf*>& Lo, std::vector<DevBuf*>& Ro);
+    int itime_ground_state(const tn_itime_line* lines, int nlines, double* variance, int* iters_out);
     int find_ground_state(const tn_sched_line* lines, int nlines, const tn_solver_options* opt,
                           tn_sweep_stats* stats);
     int sweep_pairs(int nsweeps, double epsEigen, const tn_solver_options* opt, tn_sweep_stats* stats);

@@ -346,142 +346,104 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // ---------------------------------------------------------------------------
-// Column-group panel (B = 32 columns, mp <= 32 + 8 RR rows, 256 threads).
-// Lane l of warp w has row group rg = l & 3 and column group cg = l >> 2: it
-// holds columns 4cg .. 4cg+3 on one top row, 4w + rg (the top 32 rows hold
-// the diagonal), and on RR/4 bulk rows, 32 + RR w + (RR/4) rg + 0 .. RR/4-1,
-// all in registers.  Step j needs v_j^T p_c for every column c.  Each warp's
-// share of column j sits in its four lanes of column group j/4, which copy it
-// to the warp's slice of shared memory as soon as step j-1 has updated it;
-// every lane reads its rows of it (broadcast), keeps them in registers for
-// both the dot and the update, and forms four column sums; two shuffle levels
-// leave lane l with the warp's sum for column l, and one block barrier per
-// step adds the eight warps' sums.  The reflector's scaling is deferred: the sums use
-// the unscaled column u_j (zeroed at rows <= j), so
-//     v_j^T p_c = p_c[j] + scal_j sum_{r>j} u_j[r] p_c[r],
-// and the same sum for c = j is the squared norm dlarfg needs, so no separate
-// norm reduction is made.  A finished column keeps u until the end, where it
-// is scaled and its diagonal set to beta; its Gram entry v_c^T v_j is scal_c
-// times the sum above.  Row j of every column (read by all warps) and the
-// partial sums are double-buffered by step parity in shared memory, which is
-// what lets one barrier per step suffice.  The panel moves between global and
-// shared memory with coalesced copies.  Reflectors follow dlarfg as above.
-// Shared memory of the column-group panel (one instance per kernel, whichever
-// row capacity RR the panel uses).
-struct PanelSmem {
-    double part[2][8][32];     // per-warp column sums
-    double2 vb[2][8][8][4];    // each warp's rows of u_j, row pairs by row group (RL / 2 <= 8)
-    double rowj[2][32];        // row j of every column
-    double Gs[32][33];         // Gs[l][jj] = v_l^T v_jj, l < jj
+// Warp-column panel (B = 32 columns, mp <= 32 RPL rows, 256 threads).
+// Warp w owns panel columns 4w .. 4w+3 whole: lane l holds rows l + 32 q
+// (q < RPL) of its four columns in registers, so every column sum is a warp
+// reduction (shuffles, no shared memory) and the only block barrier of a step
+// hands the next reflector to the other warps.  Step j: the warp owning column
+// j has published its rows below j (u_j, the unscaled reflector; zero at rows
+// <= j) and its row j (alpha) in shared memory; every warp reads u_j, forms
+// S_c = u_j . p_c for its four columns and |u_j|^2 (the same butterfly in every
+// warp, so every lane of every warp holds the same sums and the same dlarfg
+// values), then for c > j applies the reflector,
+//     v_j^T p_c = p_c[j] + scal_j S_c,   p_c -= tau_j (v_j^T p_c) v_j,
+// and for c < j (a finished column, which still holds u_c below its
+// diagonal) records the Gram entry v_c^T v_j = scal_c (u_c[j] + scal_j S_c) of
+// the T build.  The column-ownership test is warp-uniform, so finished
+// columns cost no update.  The warp owning column j+1 then publishes it (it
+// has just applied reflector j to it) into the other parity's buffer, and one
+// barrier ends the step.  Reflectors follow dlarfg (no reflection when the
+// sub-column is zero).  The panel comes from global memory by L2 loads
+// (ld.global.cg): in the persistent QR other CTAs write these columns during
+// the same launch.
+constexpr int PWC_MAXR = 512;  // rows of the warp-column panel
+struct PanelWcSmem {
+    double ub[2][PWC_MAXR];  // u_j by step parity
+    double alph[2];          // row j of column j
+    double Gs[32][33];       // Gs[l][jj] = v_l^T v_jj, l < jj
     double taus[32], scals[32], betas[32];
-    double Tsm[32][33];        // T(i, jj)
-    double Xs[32][33];         // products of the blocked T build
+    double Tsm[32][33];      // T(i, jj)
+    double Xs[32][33];       // products of the blocked T build
 };
 
-template <int RR>
-__device__ __forceinline__ void panel_col(double* __restrict__ W, int ldw, int m, int j0, int b,
-                                          double* __restrict__ V, int ldv, double* __restrict__ T, int ldt,
-                                          double* stage, PanelSmem& sm) {
-    constexpr int B = 32, NW = 8, RB = RR / 4, RL = RB + 1;
-    static_assert(RR % 4 == 0 && RL % 2 == 0 && RL / 2 <= 8, "bulk rows per lane must be odd, at most 15");
-    auto& part = sm.part;
-    auto& vb = sm.vb;
-    auto& rowj = sm.rowj;
-    auto& Gs = sm.Gs;
-    auto& taus = sm.taus;
-    auto& scals = sm.scals;
-    auto& betas = sm.betas;
+template <int RPL>
+__device__ __forceinline__ void panel_wc(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                         double* __restrict__ V, int ldv, double* __restrict__ T, int ldt,
+                                         PanelWcSmem& sm) {
+    constexpr int B = 32;
+    static_assert(32 * RPL <= PWC_MAXR, "panel rows");
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int rg = lane & 3, cg = lane >> 2;
     const int mp = m - j0;
-    const int ls = mp + 1;
-    constexpr int RT = (32 + 8 * RR + 255) / 256;  // rows of a column per thread in the copies
-    for (int e = tid; e < B * (B + 1); e += 256) (&Gs[0][0])[e] = 0.0;  // entries past b stay zero
-    // Asynchronous copies through L1 (all in flight at once).  In the persistent QR
-    // other CTAs write these columns during the same launch; this SM's L1 can
-    // hold no stale line of them, since it only ever cached panels already
-    // factored plus the first <= 15 rows of the column after a panel, and rows
-    // above the diagonal of a later panel are never staged.
-#pragma unroll 4
-    for (int c = 0; c < b; ++c) {
-#pragma unroll
-        for (int h = 0; h < RT; ++h) {
-            const int r = tid + 256 * h;
-            if (r < mp) cp_async8(stage + (size_t)c * ls + r, W + (size_t)(j0 + c) * ldw + j0 + r);
-        }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    auto row_of = [&](int ri) { return ri == 0 ? 4 * w + rg : 32 + RR * w + RB * rg + (ri - 1); };
-    double p[4][RL];
+    for (int e = tid; e < B * (B + 1); e += 256) (&sm.Gs[0][0])[e] = 0.0;  // entries past b stay zero
+    double p[4][RPL];
 #pragma unroll
     for (int ci = 0; ci < 4; ++ci) {
-        const int c = 4 * cg + ci;
+        const int c = 4 * w + ci;
 #pragma unroll
-        for (int ri = 0; ri < RL; ++ri) {
-            const int r = row_of(ri);
-            p[ci][ri] = (r < mp && c < b) ? stage[(size_t)c * ls + r] : 0.0;
+        for (int q = 0; q < RPL; ++q) {
+            const int ri = lane + 32 * q;
+            p[ci][q] = (c < b && ri < mp) ? __ldcg(W + (size_t)(j0 + c) * ldw + j0 + ri) : 0.0;
         }
     }
-    // this lane's rows of column slot `col` -> the warp's slice for step jn (zero at rows <= jn)
-    auto publish = [&](const double(&col)[RL], int jn) {
+    // column c (slot ci of warp c / 4) into the step buffer `par`
+    auto publish = [&](int c, int par) {
+        const int ci = c & 3;
 #pragma unroll
-        for (int ri = 0; ri < RL; ri += 2) {
-            double x0 = col[ri];
-            if (ri == 0 && 4 * w + rg <= jn) x0 = 0.0;  // top row at or above the diagonal
-            vb[jn & 1][w][ri / 2][rg] = make_double2(x0, col[ri + 1]);
+        for (int cc = 0; cc < 4; ++cc) {
+            if (cc != ci) continue;
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) {
+                const int ri = lane + 32 * q;
+                sm.ub[par][ri] = ri > c ? p[cc][q] : 0.0;
+            }
+            if (lane == c) sm.alph[par] = p[cc][0];
         }
     };
-    auto publish_slot = [&](int jn) {
-        const int sl = jn & 3;
-        if (sl == 0) publish(p[0], jn);
-        else if (sl == 1) publish(p[1], jn);
-        else if (sl == 2) publish(p[2], jn);
-        else publish(p[3], jn);
-    };
-    if (cg == 0) publish_slot(0);
-    auto tree8 = [](const double* x, int stride) {
-        return ((x[0] + x[stride]) + (x[2 * stride] + x[3 * stride])) +
-               ((x[4 * stride] + x[5 * stride]) + (x[6 * stride] + x[7 * stride]));
-    };
+    if (w == 0) publish(0, 0);
+    __syncthreads();
 #pragma unroll 1
     for (int j = 0; j < b; ++j) {
         const int par = j & 1;
-        const int jh = j >> 2, jl = j & 3;  // column j: group jh, slot jl; row j: warp jh, row group jl
-        if (w == jh && rg == jl) {
+        double u[RPL];
 #pragma unroll
-            for (int ci = 0; ci < 4; ++ci) rowj[par][4 * cg + ci] = p[ci][0];
-        }
-        __syncwarp();
-        double u[RL];
-#pragma unroll
-        for (int ri = 0; ri < RL; ri += 2) {
-            const double2 u2 = vb[par][w][ri / 2][rg];
-            u[ri] = u2.x;
-            u[ri + 1] = u2.y;
-        }
-        double acc[4][2];
+        for (int q = 0; q < RPL; ++q) u[q] = sm.ub[par][lane + 32 * q];
+        const double alpha = sm.alph[par];
+        double x[5];
 #pragma unroll
         for (int ci = 0; ci < 4; ++ci) {
-            acc[ci][0] = 0.0;
-            acc[ci][1] = 0.0;
+            double a0 = 0, a1 = 0;
 #pragma unroll
-            for (int ri = 0; ri < RL; ++ri) acc[ci][ri & 1] = fma(u[ri], p[ci][ri], acc[ci][ri & 1]);
+            for (int q = 0; q < RPL; q += 2) {
+                a0 = fma(u[q], p[ci][q], a0);
+                if (q + 1 < RPL) a1 = fma(u[q + 1], p[ci][q + 1], a1);
+            }
+            x[ci] = a0 + a1;
         }
-        // reduce-scatter over the row groups: lane l ends with column 4cg + rg = l
-        const bool hi = rg & 2, lo = rg & 1;
-        double k0 = hi ? acc[2][0] + acc[2][1] : acc[0][0] + acc[0][1];
-        double k1 = hi ? acc[3][0] + acc[3][1] : acc[1][0] + acc[1][1];
-        const double s0 = hi ? acc[0][0] + acc[0][1] : acc[2][0] + acc[2][1];
-        const double s1 = hi ? acc[1][0] + acc[1][1] : acc[3][0] + acc[3][1];
-        k0 += __shfl_xor_sync(0xffffffffu, s0, 2);
-        k1 += __shfl_xor_sync(0xffffffffu, s1, 2);
-        const double keep = lo ? k1 : k0, send = lo ? k0 : k1;
-        part[par][w][lane] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
-        __syncthreads();
-        static_assert(NW == 8, "eight warps");
-        const double S = tree8(&part[par][0][lane], B), xn2 = tree8(&part[par][0][j], B);
-        const double alpha = rowj[par][j];
+        {
+            double a0 = 0, a1 = 0;
+#pragma unroll
+            for (int q = 0; q < RPL; q += 2) {
+                a0 = fma(u[q], u[q], a0);
+                if (q + 1 < RPL) a1 = fma(u[q + 1], u[q + 1], a1);
+            }
+            x[4] = a0 + a1;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) x[v] += __shfl_xor_sync(0xffffffffu, x[v], o);
+        }
+        const double xn2 = x[4];
         double tau = 0, beta = alpha, scal = 1;
         if (xn2 > 0.0) {
             const double nrm = sqrt(alpha * alpha + xn2);
@@ -491,58 +453,44 @@ __device__ __forceinline__ void panel_col(double* __restrict__ W, int ldw, int m
             tau = -amb * amb * rinv;
             scal = beta * rinv;
         }
-        const double g = fma(scal, S, rowj[par][lane]);  // v_j^T p_lane
-        if (tau != 0.0) {
-            double tg[4];
 #pragma unroll
-            for (int ci = 0; ci < 4; ++ci) {
-                const double gc = __shfl_sync(0xffffffffu, g, (lane & ~3) | ci);
-                tg[ci] = (4 * cg + ci > j) ? tau * gc : 0.0;
-            }
+        for (int ci = 0; ci < 4; ++ci) {
+            const int c = 4 * w + ci;
+            const double pj = __shfl_sync(0xffffffffu, p[ci][0], j);  // row j of column c
+            const double g = fma(scal, x[ci], pj);                   // v_j^T p_c
+            if (c > j && c < b) {
+                if (tau != 0.0) {
+                    const double t = tau * g, cu = t * scal;
 #pragma unroll
-            for (int ci = 0; ci < 4; ++ci) {
-                const double cu = tg[ci] * scal;
-#pragma unroll
-                for (int ri = 0; ri < RL; ++ri) p[ci][ri] = fma(-cu, u[ri], p[ci][ri]);
-            }
-            if (w == jh && rg == jl) {
-#pragma unroll
-                for (int ci = 0; ci < 4; ++ci) p[ci][0] -= tg[ci];
+                    for (int q = 0; q < RPL; ++q) p[ci][q] = fma(-cu, u[q], p[ci][q]);
+                    if (lane == j) p[ci][0] -= t;
+                }
+            } else if (c < j && lane == 0) {
+                sm.Gs[c][j] = sm.scals[c] * g;
             }
         }
-        if (j + 1 < b && cg == ((j + 1) >> 2)) publish_slot(j + 1);
-        if (w == 0) {
-            if (lane < j) Gs[lane][j] = scals[lane] * g;
-            if (lane == j) {
-                taus[j] = tau;
-                scals[j] = scal;
-                betas[j] = beta;
-            }
+        if (w == (j >> 2) && lane == 0) {
+            sm.taus[j] = tau;
+            sm.scals[j] = scal;
+            sm.betas[j] = beta;
         }
+        if (j + 1 < b && w == ((j + 1) >> 2)) publish(j + 1, par ^ 1);
+        __syncthreads();
     }
-    __syncthreads();
+    // the factored panel: R above and on the diagonal, v below it
 #pragma unroll
     for (int ci = 0; ci < 4; ++ci) {
-        const int c = 4 * cg + ci;
+        const int c = 4 * w + ci;
         if (c < b) {
-            const double sc = scals[c], be = betas[c];
+            const double sc = sm.scals[c], be = sm.betas[c];
 #pragma unroll
-            for (int ri = 0; ri < RL; ++ri) {
-                const int r = row_of(ri);
-                if (r < mp) stage[(size_t)c * ls + r] = r < c ? p[ci][ri] : (r == c ? be : sc * p[ci][ri]);
-            }
-        }
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int c = 0; c < b; ++c) {
-#pragma unroll
-        for (int h = 0; h < RT; ++h) {
-            const int r = tid + 256 * h;
-            if (r < mp) {
-                const double val = stage[(size_t)c * ls + r];
-                W[(size_t)(j0 + c) * ldw + j0 + r] = val;
-                if (V) V[(size_t)c * ldv + r] = r < c ? 0.0 : (r == c ? 1.0 : val);
+            for (int q = 0; q < RPL; ++q) {
+                const int ri = lane + 32 * q;
+                if (ri < mp) {
+                    const double val = ri < c ? p[ci][q] : (ri == c ? be : sc * p[ci][q]);
+                    W[(size_t)(j0 + c) * ldw + j0 + ri] = val;
+                    if (V) V[(size_t)c * ldv + ri] = ri < c ? 0.0 : (ri == c ? 1.0 : val);
+                }
             }
         }
     }
@@ -553,6 +501,8 @@ __device__ __forceinline__ void panel_col(double* __restrict__ W, int ldw, int m
     // warp each, lane i builds row i), then the off-diagonal blocks at widths 8
     // and 16 as small products over the whole block.  Columns past b have
     // tau = 0 and zero Gram entries, so they come out zero.
+    auto& Gs = sm.Gs;
+    auto& taus = sm.taus;
     auto& Tsm = sm.Tsm;  // Tsm[i][jj] = T(i, jj)
     auto& Xs = sm.Xs;
     for (int e = tid; e < B * (B + 1); e += 256) (&Tsm[0][0])[e] = 0.0;
@@ -579,9 +529,9 @@ __device__ __forceinline__ void panel_col(double* __restrict__ W, int ldw, int m
         const int npair = B / (2 * h);
         for (int e = tid; e < npair * h * h; e += 256) {
             const int pr = e / (h * h), a = (e / h) % h, c = e % h, r0 = 2 * h * pr;
-            double x = 0;
-            for (int k = 0; k <= c; ++k) x = fma(Gs[r0 + a][r0 + h + k], Tsm[r0 + h + k][r0 + h + c], x);
-            Xs[r0 + a][r0 + h + c] = x;
+            double xx = 0;
+            for (int k = 0; k <= c; ++k) xx = fma(Gs[r0 + a][r0 + h + k], Tsm[r0 + h + k][r0 + h + c], xx);
+            Xs[r0 + a][r0 + h + c] = xx;
         }
         __syncthreads();
         for (int e = tid; e < npair * h * h; e += 256) {
@@ -598,37 +548,30 @@ __device__ __forceinline__ void panel_col(double* __restrict__ W, int ldw, int m
     }
 }
 
-template <int RR>
-__global__ void __launch_bounds__(256) qr_panel_col_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
-                                                           double* __restrict__ V, int ldv,
-                                                           double* __restrict__ T, int ldt) {
-    extern __shared__ double stage[];  // the panel, column-major, ld mp + 1
-    __shared__ PanelSmem sm;
-    panel_col<RR>(W, ldw, m, j0, b, V, ldv, T, ldt, stage, sm);
+// the panel by rows per lane
+__device__ __forceinline__ void panel_wc_any(double* W, int ldw, int m, int j0, int b, double* V, int ldv, double* T,
+                                             int ldt, PanelWcSmem& sm) {
+    const int mp = m - j0;
+    if (mp <= 64) panel_wc<2>(W, ldw, m, j0, b, V, ldv, T, ldt, sm);
+    else if (mp <= 128) panel_wc<4>(W, ldw, m, j0, b, V, ldv, T, ldt, sm);
+    else if (mp <= 256) panel_wc<8>(W, ldw, m, j0, b, V, ldv, T, ldt, sm);
+    else panel_wc<16>(W, ldw, m, j0, b, V, ldv, T, ldt, sm);
 }
 
-// Panel launch: the column-per-lane kernel for 32-wide panels, the row-per-thread
-// register kernel otherwise.
+__global__ void __launch_bounds__(256) qr_panel_wc_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                                         double* __restrict__ V, int ldv, double* __restrict__ T,
+                                                         int ldt) {
+    __shared__ PanelWcSmem sm;
+    panel_wc_any(W, ldw, m, j0, b, V, ldv, T, ldt, sm);
+}
+
+// Panel launch: the warp-column kernel for 32-wide panels of at most 512 rows,
+// the row-per-thread register kernel otherwise.
 template <int NT, int R, int B, int U>
 void launch_panel(cudaStream_t st, double* W, int ldw, int m, int j0, int b, double* V, int ldv, double* T, int ldt) {
     const int mp = m - j0;
-    if (B == 32 && mp <= 32 + 8 * 60) {
-        static thread_local int attr_dev = -1;
-        int dev = 0;
-        cudaGetDevice(&dev);
-        const size_t maxb = sizeof(double) * (size_t)(32 + 8 * 60 + 1) * 32;
-        if (attr_dev != dev) {
-            cudaFuncSetAttribute(qr_panel_col_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
-            cudaFuncSetAttribute(qr_panel_col_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
-            cudaFuncSetAttribute(qr_panel_col_kernel<28>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
-            cudaFuncSetAttribute(qr_panel_col_kernel<60>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb);
-            attr_dev = dev;
-        }
-        const size_t sm = sizeof(double) * (size_t)(mp + 1) * b;
-        if (mp <= 64) qr_panel_col_kernel<4><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
-        else if (mp <= 128) qr_panel_col_kernel<12><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
-        else if (mp <= 256) qr_panel_col_kernel<28><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
-        else qr_panel_col_kernel<60><<<1, 256, sm, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
+    if (B == 32 && mp <= PWC_MAXR) {
+        qr_panel_wc_kernel<<<1, 256, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
     } else {
         qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
     }
@@ -989,8 +932,8 @@ __global__ void __launch_bounds__(256, 1)
     qr_persistent_kernel(double* __restrict__ W, int m, int n, int k, double* __restrict__ Tall,
                          double* __restrict__ Qt, int* __restrict__ sync, int* __restrict__ derr,
                          long long spin_limit) {
-    extern __shared__ double dyn[];  // panel stage or the workers' V and C blocks, then their WySmem
-    __shared__ PanelSmem ps;
+    extern __shared__ double dyn[];  // the workers' V and C blocks, then their WySmem
+    __shared__ PanelWcSmem ps;
     __shared__ int task_sh, ok_sh;
     WySmem& ws = *reinterpret_cast<WySmem*>(dyn + (size_t)(m + 1) * 40);
     const int K = (k + 31) / 32;
@@ -1009,7 +952,7 @@ __global__ void __launch_bounds__(256, 1)
     };
     if (blockIdx.x == 0) {
         for (int kk = 0; kk < K; ++kk) {
-            const int j0 = 32 * kk, b = min(32, k - j0), mp = m - j0;
+            const int j0 = 32 * kk, b = min(32, k - j0);
             if (kk > 0) {
                 if (threadIdx.x == 0) ok_sh = 1;
                 __syncthreads();
@@ -1026,10 +969,7 @@ __global__ void __launch_bounds__(256, 1)
                 __threadfence();
             }
             double* Tk = Tall + (size_t)j0 * 32;
-            if (mp <= 64) panel_col<4>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
-            else if (mp <= 128) panel_col<12>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
-            else if (mp <= 256) panel_col<28>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
-            else panel_col<60>(W, m, m, j0, b, nullptr, 0, Tk, 32, dyn, ps);
+            panel_wc_any(W, m, m, j0, b, nullptr, 0, Tk, 32, ps);
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
@@ -1231,11 +1171,14 @@ int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double
         TN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_per_sm, qr_persistent_kernel, 256, smem));
         attr_dev = dev;
     }
-    const int nwb = (n + QRP_WB - 1) / QRP_WB, nqb = Qout ? (m + QRP_QB - 1) / QRP_QB : 0;
+    // Q forward inside the launch (Q^T accumulated m x m by the workers, beside
+    // the panels; the default, measured faster at 512 x 256) or backward after
+    // it (the dorgqr order on the thin m x k Q, one launch per reflector).
+    const bool fwdq = Qout && c.qr_forward_q;
+    const int nwb = (n + QRP_WB - 1) / QRP_WB, nqb = fwdq ? (m + QRP_QB - 1) / QRP_QB : 0;
     const int tasks = std::max(1, (n - 32 + QRP_WB - 1) / QRP_WB) + nqb;  // most tasks of one reflector
-    // 64 workers keep ahead of the panel chain (a reflector's ~180 tasks at
-    // m = 512 take them ~30 us of a ~50 us panel period) and leave SMs to other
-    // contexts sharing the device
+    // at most 64 workers: they keep ahead of the panel chain and leave SMs to
+    // other contexts sharing the device
     const int G = std::min(std::min(max_per_sm * c.sm_count, 1 + tasks), 65);
     if (G < 2) return QRP_UNAVAILABLE;
     const size_t words = 4 + (size_t)nwb + (size_t)nqb;
@@ -1245,7 +1188,7 @@ int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double
         TN_CUDA_CHECK(cudaMemset(c.derr.p, 0, sizeof(int)));
     }
     double* Qt = nullptr;
-    if (Qout) {
+    if (fwdq) {
         TN_CHECK(c.qaccum.ensure(sizeof(double) * (size_t)m * m));
         Qt = c.qaccum.as<double>();
         set_identity_kernel<<<g1d((long long)m * m), 256, 0, st>>>(Qt, m, m, m);
@@ -1267,10 +1210,23 @@ int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double
         extract_r_kernel<<<g1d((long long)k * n), 256, 0, st>>>(W, m, k, n, Rout, ldr);
         TN_LAUNCH_CHECK();
     }
-    if (Qout) {
+    if (fwdq) {
         dim3 grid((m + 31) / 32, (k + 31) / 32);
         transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(Qt, m, Qout, ldq, k, m);
         TN_LAUNCH_CHECK();
+    } else if (Qout) {
+        // Q = H_0 ... H_{K-1} [I; 0]: the last reflector first, each on the
+        // columns j0 .. k-1 and rows j0 .. m-1 it reaches (V read below the
+        // diagonal of the factored W)
+        set_identity_kernel<<<g1d((long long)m * k), 256, 0, st>>>(Qout, m, k, ldq);
+        TN_LAUNCH_CHECK();
+        for (int j0 = ((k - 1) / 32) * 32; j0 >= 0; j0 -= 32) {
+            const int b = std::min(32, k - j0), nq = k - j0;
+            wy_apply_kernel<32, false><<<(nq + WY_COLS - 1) / WY_COLS, WY_THREADS, wy_smem_bytes(m - j0, 32), st>>>(
+                W + (size_t)j0 * m + j0, m, Tall + (size_t)j0 * 32, 32, b, Qout + (size_t)j0 * ldq + j0, ldq, m - j0,
+                nq);
+            TN_LAUNCH_CHECK();
+        }
     }
     return TN_OK;
 }

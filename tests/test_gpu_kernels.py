@@ -117,6 +117,33 @@ def test_lanczos_heff(T, ctx, oracle, d, D1, D2, site):
     assert abs(th.value - tho) < 1e-10 * max(1, abs(tho))
 
 
+@pytest.mark.parametrize("fused", ["0", "1"])
+def test_lanczos_step_paths_agree(T, oracle, monkeypatch, fused):
+    """The one-launch cooperative step and the three-kernel step give the same
+    Lanczos (the oracle's Ritz value) on bulk sites with one, two and four
+    vector elements per thread of the one-launch step (N = 8192, 180 000,
+    307 200)."""
+    monkeypatch.setenv("TN_NO_FUSED_LZ", "0" if fused == "1" else "1")
+    c = T.Context(0)
+    for (d, D, site) in [(2, 64, 3), (2, 300, 3), (3, 320, 3)]:
+        W, A, F, G = envs(oracle, d, D, D, site)
+        Dw1, Dw2 = W.shape[:2]
+        D1, D2 = A.shape[1:]
+        x0 = oracle.site_flat(A)
+        dx = dev(x0)
+        th, res, nmv = C.c_double(), C.c_double(), C.c_int()
+        opt = T.SolverOptions(krylov=20, max_restarts=30).to_c()
+        Wc = np.ascontiguousarray(W.ravel())
+        dF, dG = dev(F), dev(G)
+        st = c._lib.tn_eigensolve_heff(c.handle, C.byref(opt), d, Dw1, Dw2, D1, D2, Wc.ctypes.data, dF.data_ptr(),
+                                       dG.data_ptr(), dx.data_ptr(), 1e-10, C.byref(th), C.byref(res), C.byref(nmv))
+        assert st == 0, T._capi.last_error()
+        tho, _, _, _ = oracle.lanczos_heff(W, F, G, x0, D1, D2, krylov=20, max_restarts=30, tol=1e-10)
+        assert abs(th.value - tho) < 1e-10 * max(1, abs(tho))
+        x = host(dx)
+        assert abs(np.linalg.norm(x) - 1) < 1e-12
+
+
 @pytest.mark.parametrize("m,n", [(7, 5), (5, 7), (64, 32), (32, 64), (512, 256), (130, 130), (1, 5), (9, 1),
                                  (700, 700), (1024, 300), (600, 40), (2000, 64)])
 def test_qr_lq(T, ctx, oracle, m, n):
@@ -154,6 +181,30 @@ def test_qr_rank_deficient_panels(T, ctx, oracle, m, n):
     Qo, Ro = oracle.qr(A)
     np.testing.assert_allclose(R, Ro, atol=1e-10)
     assert np.abs(Q @ R - A).max() < 1e-12
+
+
+@pytest.mark.parametrize("env", [{}, {"TN_QR_FORWARD_Q": "0"}, {"TN_NO_PERSISTENT_QR": "1"}])
+def test_qr_paths_gauge_shapes(T, oracle, monkeypatch, env):
+    """The persistent QR with the thin Q formed backwards (default) or Q^T
+    accumulated beside the panels, and the two-stream look-ahead QR, at the
+    gauge shapes of a bulk D = 256 site: same R as the oracle, orthonormal Q,
+    and zero-padded columns (a grown bond) completed to an orthonormal basis."""
+    for k_, v_ in env.items():
+        monkeypatch.setenv(k_, v_)
+    c = T.Context(0)
+    rng = np.random.default_rng(77)
+    for m, n in [(512, 256), (512, 512), (256, 512), (480, 200)]:
+        A = rng.uniform(-1, 1, size=(m, n))
+        Q, R = T.CudaQRSolver(c).SolveThinQR(A)
+        k = min(m, n)
+        assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-13
+        assert np.abs(Q @ R - A).max() < 1e-12
+        np.testing.assert_allclose(R, oracle.qr(A)[1], atol=1e-11)
+        Ap = A.copy()
+        Ap[:, n // 2 + 3:] = 0.0
+        Q, R = T.CudaQRSolver(c).SolveThinQR(Ap)
+        assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-13
+        assert np.abs(Q @ R - Ap).max() < 1e-12
 
 
 def test_qr_zero_columns_complete(T, ctx):
