@@ -150,6 +150,10 @@ int tn_hamiltonian_create_heisenberg(tn_ctx ctx, int L, double S, int form, doub
 int tn_hamiltonian_destroy(tn_hamiltonian H);
 /* SiteOperator::GetDws / Getd (TensorNetworks/SiteOperator.H:44-46). */
 int tn_hamiltonian_site_dims(tn_hamiltonian H, int site, int* Dw1, int* Dw2, int* d);
+/* Bond dimensions of site `site` of the H^2 MPO that <H^2> contracts
+ * (Hamiltonian::CreateH2Operator, Hamiltonian.C:8-16: the product H*H with its
+ * exactly dependent bond directions removed by SVD sweeps). */
+int tn_hamiltonian_h2_dims(tn_hamiltonian H, int site, int* Dw1, int* Dw2);
 /* SiteOperator::GetW (SiteOperator.H:52): copies W of a site into host memory. */
 int tn_hamiltonian_get_w(tn_hamiltonian H, int site, double* W_host);
 

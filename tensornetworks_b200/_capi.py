@@ -77,6 +77,7 @@ SIGNATURES = {
     "tn_hamiltonian_create_heisenberg": (_I, [_V, _I, _D, _I, _D, _D, _D, _PV]),
     "tn_hamiltonian_destroy": (_I, [_V]),
     "tn_hamiltonian_site_dims": (_I, [_V, _I, _PI, _PI, _PI]),
+    "tn_hamiltonian_h2_dims": (_I, [_V, _I, _PI, _PI]),
     "tn_hamiltonian_get_w": (_I, [_V, _I, _V]),
     "tn_mps_create": (_I, [_V, _I, _D, _D, _PV]),
     "tn_mps_destroy": (_I, [_V]),

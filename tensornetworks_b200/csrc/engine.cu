@@ -24,6 +24,7 @@
 #include <random>
 
 #include "engine.h"
+#include "host_linalg.h"
 
 namespace tnb {
 
@@ -146,6 +147,95 @@ inline int g1d(long long n) {
 // ---------------------------------------------------------------------------
 // Hamiltonian
 // ---------------------------------------------------------------------------
+// Bond singular values of an MPO, one left-to-right and one right-to-left SVD
+// sweep (SiteOperatorImp::CompressStd, SiteOperatorImpCompress.C:35-72, applied
+// bond by bond as MPO::Compress does): every bond keeps the singular values
+// above rel_eps times its largest, the rest are the exact linear dependencies
+// of a product MPO (Hamiltonian::CreateH2Operator compresses H*H the same way,
+// Hamiltonian.C:8-16, to 1e-13).  Host work on matrices of at most Dw d^2 rows.
+void compress_mpo(std::vector<SiteMPO>& ops, int L, int d, double rel_eps) {
+    const int dd = d * d;
+    auto kept = [&](const std::vector<double>& sv, std::vector<int>& order) {
+        order.resize(sv.size());
+        for (size_t i = 0; i < sv.size(); ++i) order[i] = (int)i;
+        std::sort(order.begin(), order.end(), [&](int a, int b) { return sv[a] > sv[b]; });
+        const double smax = sv[order[0]];
+        int k = 0;
+        while (k < (int)order.size() && sv[order[k]] > rel_eps * smax) ++k;
+        return std::max(k, 1);
+    };
+    std::vector<double> U, sv, V;
+    std::vector<int> order;
+    for (int ia = 1; ia < L; ++ia) {  // W_ia as M[(w1, m, n), w2]: keep U, pass s V^T on
+        SiteMPO& A = ops[ia];
+        SiteMPO& B = ops[ia + 1];
+        const int rows = A.Dw1 * dd, cols = A.Dw2;
+        std::vector<double> M((size_t)rows * cols);
+        for (int w1 = 0; w1 < A.Dw1; ++w1)
+            for (int w2 = 0; w2 < A.Dw2; ++w2)
+                for (int mn = 0; mn < dd; ++mn)
+                    M[(size_t)(w1 * dd + mn) + (size_t)w2 * rows] = A.W[((size_t)w1 * A.Dw2 + w2) * dd + mn];
+        host_svd_thin(M, rows, cols, U, sv, V);
+        const int k = kept(sv, order);
+        SiteMPO An;
+        An.Dw1 = A.Dw1;
+        An.Dw2 = k;
+        An.W.assign((size_t)An.Dw1 * k * dd, 0.0);
+        for (int w1 = 0; w1 < A.Dw1; ++w1)
+            for (int c = 0; c < k; ++c)
+                for (int mn = 0; mn < dd; ++mn)
+                    An.W[((size_t)w1 * k + c) * dd + mn] = U[(size_t)order[c] * rows + w1 * dd + mn];
+        SiteMPO Bn;
+        Bn.Dw1 = k;
+        Bn.Dw2 = B.Dw2;
+        Bn.W.assign((size_t)k * B.Dw2 * dd, 0.0);
+        for (int c = 0; c < k; ++c)
+            for (int w2 = 0; w2 < A.Dw2; ++w2) {
+                const double t = sv[order[c]] * V[(size_t)order[c] * cols + w2];
+                if (t == 0.0) continue;
+                for (int v2 = 0; v2 < B.Dw2; ++v2)
+                    for (int mn = 0; mn < dd; ++mn)
+                        Bn.W[((size_t)c * B.Dw2 + v2) * dd + mn] += t * B.W[((size_t)w2 * B.Dw2 + v2) * dd + mn];
+            }
+        A = std::move(An);
+        B = std::move(Bn);
+    }
+    for (int ia = L; ia > 1; --ia) {  // W_ia^T as M[(w2, m, n), w1]: keep U^T, pass V s back
+        SiteMPO& A = ops[ia];
+        SiteMPO& P = ops[ia - 1];
+        const int rows = A.Dw2 * dd, cols = A.Dw1;
+        std::vector<double> M((size_t)rows * cols);
+        for (int w1 = 0; w1 < A.Dw1; ++w1)
+            for (int w2 = 0; w2 < A.Dw2; ++w2)
+                for (int mn = 0; mn < dd; ++mn)
+                    M[(size_t)(w2 * dd + mn) + (size_t)w1 * rows] = A.W[((size_t)w1 * A.Dw2 + w2) * dd + mn];
+        host_svd_thin(M, rows, cols, U, sv, V);
+        const int k = kept(sv, order);
+        SiteMPO An;
+        An.Dw1 = k;
+        An.Dw2 = A.Dw2;
+        An.W.assign((size_t)k * A.Dw2 * dd, 0.0);
+        for (int c = 0; c < k; ++c)
+            for (int w2 = 0; w2 < A.Dw2; ++w2)
+                for (int mn = 0; mn < dd; ++mn)
+                    An.W[((size_t)c * A.Dw2 + w2) * dd + mn] = U[(size_t)order[c] * rows + w2 * dd + mn];
+        SiteMPO Pn;
+        Pn.Dw1 = P.Dw1;
+        Pn.Dw2 = k;
+        Pn.W.assign((size_t)P.Dw1 * k * dd, 0.0);
+        for (int v1 = 0; v1 < P.Dw1; ++v1)
+            for (int w1 = 0; w1 < A.Dw1; ++w1)
+                for (int c = 0; c < k; ++c) {
+                    const double t = V[(size_t)order[c] * cols + w1] * sv[order[c]];
+                    if (t == 0.0) continue;
+                    for (int mn = 0; mn < dd; ++mn)
+                        Pn.W[((size_t)v1 * k + c) * dd + mn] += P.W[((size_t)v1 * P.Dw2 + w1) * dd + mn] * t;
+                }
+        A = std::move(An);
+        P = std::move(Pn);
+    }
+}
+
 int Hamiltonian::build() {
     ops.assign(L + 1, SiteMPO());
     ops2.assign(L + 1, SiteMPO());
@@ -153,6 +243,7 @@ int Hamiltonian::build() {
         ops[ia] = site_mpo(L, S, d, form, Jxy, Jz, hz, ia);
         ops2[ia] = product_mpo(ops[ia], ops[ia], d);
     }
+    if (L > 1) compress_mpo(ops2, L, d, 1e-13);
     std::vector<WTermDev> all;
     std::vector<double> allW;
     std::vector<const SiteMPO*> done;
@@ -569,6 +660,9 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     // channels carrying the completed block energy (lower form: left 0, right Dw-1)
     const int wF = H->form == TN_FORM_REGULAR_LOWER ? 0 : op.Dw1 - 1;
     const int wG = H->form == TN_FORM_REGULAR_LOWER ? op.Dw2 - 1 : 0;
+    // residual target: the requested tolerance, but not below the split operator's
+    // noise floor relative to |T| (BF16x3 ~ 2^-16, BF16x6 ~ FP32 accumulation)
+    const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 2e-6);
     if (ctx->prof) {
         TN_CHECK(ctx->prof_events());
         TN_CUDA_CHECK(cudaEventRecord(ctx->pev[0], st));
@@ -580,9 +674,6 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     };
     int krylov = opt.krylov > 0 ? opt.krylov : 20;
     int restarts = opt.max_restarts > 0 ? opt.max_restarts : 10;
-    // residual target: the requested tolerance, but not below the split operator's
-    // noise floor relative to |T| (BF16x3 ~ 2^-16, BF16x6 ~ FP32 accumulation)
-    const double tol_rel = opt.mixed_tol > 0 ? opt.mixed_tol : (ns == 3 ? 1e-9 : 2e-6);
     // the operator: everything the recorded matvec launches depend on
     unsigned long long key = hash_val(HASH_SEED, 0x6d69786564ULL);
     key = hash_val(key, s);
@@ -668,6 +759,7 @@ int MPSState::rq_slots() {
     if ((int)rq_pending.size() != L + 2) {
         rq_pending.assign(L + 2, 0);
         rq_lz.assign(L + 2, 0);
+        rq_exact.assign(L + 2, 0);
         rq_dtheta.assign(L + 2, 0.0);
         rq_flop.assign(L + 2, 0.0);
     }
@@ -704,16 +796,25 @@ void MPSState::rq_order() {
 int MPSState::rq_collect() {
     if (!rq_inflight) return TN_OK;
     TN_CUDA_CHECK(cudaEventSynchronize(ctx->ev_y[1]));
+    TN_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));  // the summaries of device-driven solves
     rq_inflight = false;
     int bad = 0, nan = 0;
     for (int ia = 1; ia <= L; ++ia) {
         if (!rq_pending[ia]) continue;
         rq_pending[ia] = 0;
         const double* slot = reinterpret_cast<double*>(rqhost.p) + RQ_SLOT * (size_t)ia;
+        const bool exact = rq_exact[ia] != 0;  // an FP64 solve: its Ritz value is the energy, no check ran
+        rq_exact[ia] = 0;
         int err = 0;
-        std::memcpy(&err, slot + 3, sizeof(int));
+        if (!exact) std::memcpy(&err, slot + 3, sizeof(int));
         bad |= err;
-        const double theta = slot[0];
+        double theta = slot[0];
+        if (exact) {
+            LzSummary sm;
+            std::memcpy(&sm, slot + 4, sizeof(sm));
+            theta = sm.theta;
+            matvecs_fp64 += sm.matvecs;
+        }
         iterDE[ia] = theta - Emin[ia];
         Emin[ia] = theta;
         gapE[ia] = rq_dtheta[ia];
@@ -848,8 +949,25 @@ int MPSState::refine_site(int ia, double epsEigen) {
     for (const void* q : {(const void*)t, (const void*)F, (const void*)G, (const void*)P, (const void*)Q})
         key = hash_val(key, q);
     key = hash_val(key, op.nLR);
-    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, &r,
-                           opt.fp64_tol_rel > 0 ? opt.fp64_tol_rel : 0.0, key));
+    const double tol_rel = opt.fp64_tol_rel > 0 ? opt.fp64_tol_rel : 0.0;
+    if (opt.verbose < 3 && ctx->aux2) {
+        // device-driven restarts, nothing waits for the host: the solve's summary
+        // (its FP64 Ritz value is the site energy) is read once per half-sweep
+        TN_CHECK(rq_slots());
+        LzSummary* slot = reinterpret_cast<LzSummary*>(reinterpret_cast<double*>(rqhost.p) + RQ_SLOT * (size_t)ia + 4);
+        const int rc = lanczos_solve_async(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, tol_rel, key,
+                                           slot);
+        if (rc == TN_OK) {
+            rq_lz[ia] = 1;
+            rq_exact[ia] = 1;
+            rq_pending[ia] = 1;
+            rq_inflight = true;
+            rq_flop[ia] = heff_flops(s);
+            return TN_OK;
+        }
+        if (rc != LZ_ASYNC_UNAVAILABLE) return rc;
+    }
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mv, &r, tol_rel, key));
     matvecs += r.matvecs;
     matvecs_fp64 += r.matvecs;
     heff_flop += heff_flops(s) * r.matvecs;

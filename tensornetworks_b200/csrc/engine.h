@@ -68,7 +68,7 @@ struct MPSState {
     static constexpr int RQ_SLOT = 12;  // doubles per site
     DevBuf rqP, rqQ, rqbuf;
     HostBuf rqhost;
-    std::vector<char> rq_pending, rq_lz;
+    std::vector<char> rq_pending, rq_lz, rq_exact;  // rq_exact: an FP64 solve, no separate check
     std::vector<double> rq_dtheta, rq_flop;
     bool rq_inflight = false;
     MixedSite msite;

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "host_linalg.h"
 
 namespace tnb {
 
@@ -34,50 +35,6 @@ namespace {
 double sz_of(int m, double S) { return m - S; }
 double sp_el(int m, int n, double S) {  // <m|S+|n>
     return (m == n + 1) ? std::sqrt(S * (S + 1.0) - sz_of(m, S) * sz_of(n, S)) : 0.0;
-}
-
-// host one-sided Jacobi SVD of an m x n column-major matrix (m >= n): A = U diag(s) V^T
-void host_svd(std::vector<double> A, int m, int n, std::vector<double>& U, std::vector<double>& s,
-              std::vector<double>& V) {
-    V.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
-    for (int sweep = 0; sweep < 80; ++sweep) {
-        bool rot = false;
-        for (int p = 0; p < n; ++p)
-            for (int q = p + 1; q < n; ++q) {
-                double a = 0, b = 0, g = 0;
-                for (int i = 0; i < m; ++i) {
-                    const double x = A[(size_t)p * m + i], y = A[(size_t)q * m + i];
-                    a += x * x;
-                    b += y * y;
-                    g += x * y;
-                }
-                if (g == 0.0 || std::fabs(g) <= 1e-15 * std::sqrt(a * b)) continue;
-                rot = true;
-                const double zeta = (b - a) / (2 * g);
-                const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
-                const double c = 1 / std::sqrt(1 + t * t), sn = c * t;
-                for (int i = 0; i < m; ++i) {
-                    const double x = A[(size_t)p * m + i], y = A[(size_t)q * m + i];
-                    A[(size_t)p * m + i] = c * x - sn * y;
-                    A[(size_t)q * m + i] = sn * x + c * y;
-                }
-                for (int i = 0; i < n; ++i) {
-                    const double x = V[(size_t)p * n + i], y = V[(size_t)q * n + i];
-                    V[(size_t)p * n + i] = c * x - sn * y;
-                    V[(size_t)q * n + i] = sn * x + c * y;
-                }
-            }
-        if (!rot) break;
-    }
-    s.assign(n, 0.0);
-    U.assign((size_t)m * n, 0.0);
-    for (int j = 0; j < n; ++j) {
-        double nr = 0;
-        for (int i = 0; i < m; ++i) nr += A[(size_t)j * m + i] * A[(size_t)j * m + i];
-        s[j] = std::sqrt(nr);
-        for (int i = 0; i < m; ++i) U[(size_t)j * m + i] = s[j] > 0 ? A[(size_t)j * m + i] / s[j] : 0.0;
-    }
 }
 
 // Gate exp(-tau h) of one bond (h with the field weights ca, cb of its two sites)

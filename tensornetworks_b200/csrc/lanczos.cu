@@ -21,7 +21,7 @@ namespace tnb {
 
 namespace {
 
-constexpr int LZ_THREADS = 256;
+constexpr int LZ_THREADS = 512;  // with one block per SM (vec_grid): few partials for the last-block sums
 constexpr int KCHUNK = 8;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -234,14 +234,19 @@ __global__ void lz_scale_kernel(const double* x, double* v0, long long N, const 
     }
 }
 
-// h_k = V_k . w for k = 0..j  (partials per block, last block reduces).
+// The three kernels of a step hand their sums on as per-block partials: the
+// next kernel's every block adds the previous kernel's partials itself, in
+// the same fixed order (so every block holds bitwise the same sums), instead
+// of a last block reducing them at the end of the previous kernel while the
+// other SMs idle.
+
+// Partials of h_k = V_k . w, k = 0..j, into partA.
 __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __restrict__ w, long long N,
-                               double* partial, LzState* st) {
+                               double* partA, LzState* st) {
     pdl_wait();
     if (st->done) return;
     __shared__ double sh[KCHUNK * 32];
     __shared__ double res[KCHUNK];
-    __shared__ bool last;
     const int j = st->j;
     const int nk = j + 1;
     for (int k0 = 0; k0 < nk; k0 += KCHUNK) {
@@ -255,44 +260,29 @@ __global__ void lz_dots_kernel(const double* __restrict__ V, const double* __res
         }
         block_sum_chunk(v, res, sh);
         if (threadIdx.x < KCHUNK && k0 + threadIdx.x < nk)
-            partial[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned int prev = atomicAdd(&st->counter, 1u);
-        last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last) {
-        __shared__ double hsum[LZ_MAXK + KCHUNK];
-        reduce_partials(partial, gridDim.x, LZ_MAXK, nk, hsum, sh);
-        for (int k = threadIdx.x; k < nk; k += blockDim.x) st->h[k] = hsum[k];
-        if (threadIdx.x == 0) st->counter = 0;
+            partA[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
     }
 }
 
-// w' = w - V h;  h2 = V^T w';  nrm2 = |w'|^2.  The last block forms alpha_j and
-// beta_j; the tridiagonal eigenproblem and the decision to stop follow in
-// block 0 of lz_next_kernel, beside the other blocks' vector work.
+// h from partA; w' = w - V h; partials of h2 = V^T w' and |w'|^2 into partB.
+// Block 0 keeps h in the state (alpha_j = h_j + h2_j is formed next).
 __global__ void lz_update_kernel(const double* __restrict__ V, double* __restrict__ w, long long N,
-                                 double* partial, LzState* st) {
+                                 const double* partA, double* partB, LzState* st) {
     pdl_wait();
     if (st->done) return;
     __shared__ double sh[KCHUNK * 32];
     __shared__ double res[KCHUNK];
-    __shared__ double hs[LZ_MAXK];
-    __shared__ bool last;
+    __shared__ double hs[LZ_MAXK + KCHUNK];
     const int j = st->j;
     const int nk = j + 1;
-    for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h[k];
-    __syncthreads();
+    reduce_partials(partA, gridDim.x, LZ_MAXK, nk, hs, sh);
+    if (blockIdx.x == 0)
+        for (int k = threadIdx.x; k < nk; k += blockDim.x) st->h[k] = hs[k];
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         double wi = w[i];
         wi = basis_combine(V, N, i, hs, nk, -1.0, wi);
         w[i] = wi;
     }
-    // second projection (h2) and the norm of w'
     for (int k0 = 0; k0 < nk + 1; k0 += KCHUNK) {
         double v[KCHUNK] = {0};
         for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
@@ -307,64 +297,54 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
         }
         block_sum_chunk(v, res, sh);
         if (threadIdx.x < KCHUNK && k0 + (int)threadIdx.x <= nk)
-            partial[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned int prev = atomicAdd(&st->counter, 1u);
-        last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __shared__ double h2s[LZ_MAXK + KCHUNK];
-    reduce_partials(partial, gridDim.x, LZ_MAXK, nk + 1, h2s, sh);
-    if (threadIdx.x == 0) {
-        double ss = 0;
-        for (int k = 0; k < nk; ++k) { st->h2[k] = h2s[k]; ss += h2s[k] * h2s[k]; }
-        double nrm2 = h2s[nk];
-        st->alpha[j] = hs[j] + h2s[j];
-        st->beta[j] = sqrt(fmax(nrm2 - ss, 0.0));
-        st->counter = 0;
-        st->matvecs += 1;
-        st->jn = j + 1;
+            partB[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
     }
 }
 
-// V_{j+1} = (w' - V h2) / beta_j, also into the matvec input xcur; the last
-// block advances the step index (the other blocks read only jn).  Block 0
-// first solves the tridiagonal problem of step j, sets the convergence flag
-// and, inside a graph loop (cond != 0), whether the loop runs another step:
-// every step reaches it, and it ends the loop at the latest when the basis
-// limit is reached, so the loop always terminates.  Blocks that start after
-// block 0 has set the flag return at once; the loop then ends, so the step's
-// vector (and the half-counted ticket, which the next reset clears) is unused.
-__global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N, LzState* st,
-                               double* __restrict__ xcur, cudaGraphConditionalHandle cond = 0) {
+// h2 and |w'|^2 from partB, beta_j; V_{j+1} = (w' - V h2) / beta_j, also into
+// the matvec input xcur.  Block 0 records alpha_j and beta_j, then solves the
+// tridiagonal problem of step j and decides whether the restart ends (and,
+// inside a graph loop, whether the loop runs another step), after its share
+// of the vector.  The last block to finish advances the step index.  Blocks
+// that start after block 0 has ended the restart return at once; the step's
+// vector is then unused (and the half-counted ticket is cleared by the next
+// reset).
+__global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N,
+                               const double* partB, LzState* st, double* __restrict__ xcur,
+                               cudaGraphConditionalHandle cond = 0) {
     pdl_wait();
     if (st->done) {
         if (cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
         return;
     }
-    __shared__ double hs[LZ_MAXK];
-    __shared__ double inv;
+    __shared__ double sh[KCHUNK * 32];
+    __shared__ double h2s[LZ_MAXK + KCHUNK];
     __shared__ bool last;
-    const int j = st->jn - 1;
+    const int j = st->j;
     const int nk = j + 1;
-    if (blockIdx.x == 0) lz_decide_step(st, j, cond);
-    for (int k = threadIdx.x; k < nk; k += blockDim.x) hs[k] = st->h2[k];
-    if (threadIdx.x == 0) {
-        const double bj = st->beta[j];
-        inv = bj > 0 ? 1.0 / bj : 0.0;
-    }
-    __syncthreads();
+    reduce_partials(partB, gridDim.x, LZ_MAXK, nk + 1, h2s, sh);
+    double ss = 0;
+    for (int k = 0; k < nk; ++k) ss = fma(h2s[k], h2s[k], ss);
+    const double beta = sqrt(fmax(h2s[nk] - ss, 0.0));
+    const double inv = beta > 0 ? 1.0 / beta : 0.0;
     double* vn = V + (long long)(j + 1) * N;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         double wi = w[i];
-        wi = basis_combine(V, N, i, hs, nk, -1.0, wi);
+        wi = basis_combine(V, N, i, h2s, nk, -1.0, wi);
         wi *= inv;
         vn[i] = wi;
         xcur[i] = wi;
+    }
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < nk; ++k) st->h2[k] = h2s[k];
+            st->alpha[j] = st->h[j] + h2s[j];
+            st->beta[j] = beta;
+            st->matvecs += 1;
+            st->jn = j + 1;
+        }
+        __syncthreads();
+        lz_decide_step(st, j, cond);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -391,8 +371,8 @@ __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict_
 // Block 0 writes the state and makes the decision after its share of the
 // vector.  Grid barriers poll with a limit; on expiry the kernel raises the
 // context's error word and returns (the host reads it as TN_CUDA_ERROR).
-constexpr int LZF_THREADS = 256;
-constexpr int LZF_BLOCKS_PER_SM = 4;  // 32 warps per SM keep enough basis loads in flight
+constexpr int LZF_THREADS = 1024;    // 32 warps per SM keep enough basis loads in flight
+constexpr int LZF_BLOCKS_PER_SM = 1;  // one block per SM: the redundant reductions read G x nk partials
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
     unsigned int v;
@@ -644,7 +624,7 @@ __global__ void rq_resid_kernel(const double* __restrict__ x, const double* __re
 
 inline int vec_grid(long long N, int sm) {
     long long b = (N + LZ_THREADS - 1) / LZ_THREADS;
-    long long cap = (long long)sm * 2;
+    long long cap = (long long)sm;
     if (b > cap) b = cap;
     if (b < 1) b = 1;
     return (int)b;
@@ -662,7 +642,7 @@ constexpr int LZF_MAXR = 4;  // elements per thread the fused step keeps in regi
 // Per-block partial sums the solves need: the three-kernel step's, then the
 // fused step's two sets.
 inline size_t partial_doubles(long long N, int sm) {
-    return ((size_t)vec_grid(N, sm) + 2 * (size_t)fused_grid(N, sm)) * LZ_MAXK;
+    return (2 * (size_t)vec_grid(N, sm) + 2 * (size_t)fused_grid(N, sm)) * LZ_MAXK;
 }
 
 }  // namespace
@@ -687,7 +667,7 @@ static int launch_fused_step(Ctx& c, long long N, double* V, const double* w, do
     const int G = fused_grid(N, c.sm_count);
     const long long per = (long long)G * LZF_THREADS;
     const long long R = (N + per - 1) / per;
-    double* partA = partial + (size_t)vec_grid(N, c.sm_count) * LZ_MAXK;
+    double* partA = partial + 2 * (size_t)vec_grid(N, c.sm_count) * LZ_MAXK;
     double* partB = partA + (size_t)G * LZ_MAXK;
     int* err = c.derr.as<int>();
     long long limit = c.lz_spin_limit;
@@ -725,9 +705,12 @@ static int enqueue_lz_step(Ctx& c, const MatvecFn& mv, bool fused, int grid, dou
         TN_CHECK(mv(xcur, w, &s->done));
         return launch_fused_step(c, N, V, w, partial, s, xcur, cond);
     }
+    double* partB = partial + (size_t)grid * LZ_MAXK;
     TN_CHECK(step_matvec_dots(c, mv, grid, V, w, xcur, N, partial, s));
-    TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, c.stream, (const double*)V, w, N, partial, s));
-    return launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, c.stream, V, (const double*)w, N, s, xcur, cond);
+    TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, c.stream, (const double*)V, w, N,
+                        (const double*)partial, partB, s));
+    return launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, c.stream, V, (const double*)w, N, (const double*)partB, s,
+                      xcur, cond);
 }
 
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,

@@ -346,14 +346,14 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // ---------------------------------------------------------------------------
-// Warp-column panel (B = 32 columns, mp <= 32 RPL rows, 256 threads).
-// Warp w owns panel columns 4w .. 4w+3 whole: lane l holds rows l + 32 q
-// (q < RPL) of its four columns in registers, so every column sum is a warp
+// Warp-column panel (B = 32 columns, mp <= 32 RPL rows, 512 threads).
+// Warp w owns panel columns 2w, 2w+1 whole: lane l holds rows l + 32 q
+// (q < RPL) of its two columns in registers, so every column sum is a warp
 // reduction (shuffles, no shared memory) and the only block barrier of a step
 // hands the next reflector to the other warps.  Step j: the warp owning column
 // j has published its rows below j (u_j, the unscaled reflector; zero at rows
 // <= j) and its row j (alpha) in shared memory; every warp reads u_j, forms
-// S_c = u_j . p_c for its four columns and |u_j|^2 (the same butterfly in every
+// S_c = u_j . p_c for its two columns and |u_j|^2 (the same butterfly in every
 // warp, so every lane of every warp holds the same sums and the same dlarfg
 // values), then for c > j applies the reflector,
 //     v_j^T p_c = p_c[j] + scal_j S_c,   p_c -= tau_j (v_j^T p_c) v_j,
@@ -366,7 +366,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // sub-column is zero).  The panel comes from global memory by L2 loads
 // (ld.global.cg): in the persistent QR other CTAs write these columns during
 // the same launch.
-constexpr int PWC_MAXR = 512;  // rows of the warp-column panel
+constexpr int PWC_MAXR = 512;   // rows of the warp-column panel
+constexpr int PWC_WARPS = 16;   // two columns per warp: four warps per scheduler hide the step's latencies
+constexpr int PWC_THREADS = 32 * PWC_WARPS;
 struct PanelWcSmem {
     double ub[2][PWC_MAXR];  // u_j by step parity
     double alph[2];          // row j of column j
@@ -376,124 +378,12 @@ struct PanelWcSmem {
     double Xs[32][33];       // products of the blocked T build
 };
 
-template <int RPL>
-__device__ __forceinline__ void panel_wc(double* __restrict__ W, int ldw, int m, int j0, int b,
-                                         double* __restrict__ V, int ldv, double* __restrict__ T, int ldt,
-                                         PanelWcSmem& sm) {
+// T of the compact WY form from the reflectors' taus and Gram entries, by the
+// whole block (at least 128 threads).
+__device__ void build_t(const double (&Gs)[32][33], const double* taus, double (&Tsm)[32][33], double (&Xs)[32][33],
+                        int b, double* __restrict__ T, int ldt) {
     constexpr int B = 32;
-    static_assert(32 * RPL <= PWC_MAXR, "panel rows");
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int mp = m - j0;
-    for (int e = tid; e < B * (B + 1); e += 256) (&sm.Gs[0][0])[e] = 0.0;  // entries past b stay zero
-    double p[4][RPL];
-#pragma unroll
-    for (int ci = 0; ci < 4; ++ci) {
-        const int c = 4 * w + ci;
-#pragma unroll
-        for (int q = 0; q < RPL; ++q) {
-            const int ri = lane + 32 * q;
-            p[ci][q] = (c < b && ri < mp) ? __ldcg(W + (size_t)(j0 + c) * ldw + j0 + ri) : 0.0;
-        }
-    }
-    // column c (slot ci of warp c / 4) into the step buffer `par`
-    auto publish = [&](int c, int par) {
-        const int ci = c & 3;
-#pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-            if (cc != ci) continue;
-#pragma unroll
-            for (int q = 0; q < RPL; ++q) {
-                const int ri = lane + 32 * q;
-                sm.ub[par][ri] = ri > c ? p[cc][q] : 0.0;
-            }
-            if (lane == c) sm.alph[par] = p[cc][0];
-        }
-    };
-    if (w == 0) publish(0, 0);
-    __syncthreads();
-#pragma unroll 1
-    for (int j = 0; j < b; ++j) {
-        const int par = j & 1;
-        double u[RPL];
-#pragma unroll
-        for (int q = 0; q < RPL; ++q) u[q] = sm.ub[par][lane + 32 * q];
-        const double alpha = sm.alph[par];
-        double x[5];
-#pragma unroll
-        for (int ci = 0; ci < 4; ++ci) {
-            double a0 = 0, a1 = 0;
-#pragma unroll
-            for (int q = 0; q < RPL; q += 2) {
-                a0 = fma(u[q], p[ci][q], a0);
-                if (q + 1 < RPL) a1 = fma(u[q + 1], p[ci][q + 1], a1);
-            }
-            x[ci] = a0 + a1;
-        }
-        {
-            double a0 = 0, a1 = 0;
-#pragma unroll
-            for (int q = 0; q < RPL; q += 2) {
-                a0 = fma(u[q], u[q], a0);
-                if (q + 1 < RPL) a1 = fma(u[q + 1], u[q + 1], a1);
-            }
-            x[4] = a0 + a1;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) x[v] += __shfl_xor_sync(0xffffffffu, x[v], o);
-        }
-        const double xn2 = x[4];
-        double tau = 0, beta = alpha, scal = 1;
-        if (xn2 > 0.0) {
-            const double nrm = sqrt(alpha * alpha + xn2);
-            beta = alpha >= 0 ? -nrm : nrm;
-            const double amb = alpha - beta;
-            const double rinv = 1.0 / (beta * amb);  // tau = -amb / beta, scal = 1 / amb
-            tau = -amb * amb * rinv;
-            scal = beta * rinv;
-        }
-#pragma unroll
-        for (int ci = 0; ci < 4; ++ci) {
-            const int c = 4 * w + ci;
-            const double pj = __shfl_sync(0xffffffffu, p[ci][0], j);  // row j of column c
-            const double g = fma(scal, x[ci], pj);                   // v_j^T p_c
-            if (c > j && c < b) {
-                if (tau != 0.0) {
-                    const double t = tau * g, cu = t * scal;
-#pragma unroll
-                    for (int q = 0; q < RPL; ++q) p[ci][q] = fma(-cu, u[q], p[ci][q]);
-                    if (lane == j) p[ci][0] -= t;
-                }
-            } else if (c < j && lane == 0) {
-                sm.Gs[c][j] = sm.scals[c] * g;
-            }
-        }
-        if (w == (j >> 2) && lane == 0) {
-            sm.taus[j] = tau;
-            sm.scals[j] = scal;
-            sm.betas[j] = beta;
-        }
-        if (j + 1 < b && w == ((j + 1) >> 2)) publish(j + 1, par ^ 1);
-        __syncthreads();
-    }
-    // the factored panel: R above and on the diagonal, v below it
-#pragma unroll
-    for (int ci = 0; ci < 4; ++ci) {
-        const int c = 4 * w + ci;
-        if (c < b) {
-            const double sc = sm.scals[c], be = sm.betas[c];
-#pragma unroll
-            for (int q = 0; q < RPL; ++q) {
-                const int ri = lane + 32 * q;
-                if (ri < mp) {
-                    const double val = ri < c ? p[ci][q] : (ri == c ? be : sc * p[ci][q]);
-                    W[(size_t)(j0 + c) * ldw + j0 + ri] = val;
-                    if (V) V[(size_t)c * ldv + ri] = ri < c ? 0.0 : (ri == c ? 1.0 : val);
-                }
-            }
-        }
-    }
     // T (dlarft, forward, columnwise) blockwise.  For reflectors split into two
     // groups, I - V T V^T = (I - V1 T11 V1^T)(I - V2 T22 V2^T) gives
     // T = [T11, -T11 (V1^T V2) T22; 0, T22]: the four 8 x 8 diagonal blocks by
@@ -501,11 +391,7 @@ __device__ __forceinline__ void panel_wc(double* __restrict__ W, int ldw, int m,
     // warp each, lane i builds row i), then the off-diagonal blocks at widths 8
     // and 16 as small products over the whole block.  Columns past b have
     // tau = 0 and zero Gram entries, so they come out zero.
-    auto& Gs = sm.Gs;
-    auto& taus = sm.taus;
-    auto& Tsm = sm.Tsm;  // Tsm[i][jj] = T(i, jj)
-    auto& Xs = sm.Xs;
-    for (int e = tid; e < B * (B + 1); e += 256) (&Tsm[0][0])[e] = 0.0;
+    for (int e = tid; e < B * (B + 1); e += (int)blockDim.x) (&Tsm[0][0])[e] = 0.0;
     __syncthreads();
     if (w < 4 && lane < 8) {
         const int q0 = 8 * w, i = lane;
@@ -527,14 +413,14 @@ __device__ __forceinline__ void panel_wc(double* __restrict__ W, int ldw, int m,
     for (int h = 8; h < B; h *= 2) {
         // pairs of h x h blocks at r0 = 0, 2h, ...: X = G12 T22, then T12 = -T11 X
         const int npair = B / (2 * h);
-        for (int e = tid; e < npair * h * h; e += 256) {
+        for (int e = tid; e < npair * h * h; e += (int)blockDim.x) {
             const int pr = e / (h * h), a = (e / h) % h, c = e % h, r0 = 2 * h * pr;
             double xx = 0;
             for (int k = 0; k <= c; ++k) xx = fma(Gs[r0 + a][r0 + h + k], Tsm[r0 + h + k][r0 + h + c], xx);
             Xs[r0 + a][r0 + h + c] = xx;
         }
         __syncthreads();
-        for (int e = tid; e < npair * h * h; e += 256) {
+        for (int e = tid; e < npair * h * h; e += (int)blockDim.x) {
             const int pr = e / (h * h), a = (e / h) % h, c = e % h, r0 = 2 * h * pr;
             double t = 0;
             for (int k = a; k < h; ++k) t = fma(Tsm[r0 + a][r0 + k], Xs[r0 + k][r0 + h + c], t);
@@ -542,10 +428,131 @@ __device__ __forceinline__ void panel_wc(double* __restrict__ W, int ldw, int m,
         }
         __syncthreads();
     }
-    for (int e = tid; e < b * b; e += 256) {
+    for (int e = tid; e < b * b; e += (int)blockDim.x) {
         const int i = e % b, jj = e / b;
         T[(size_t)jj * ldt + i] = Tsm[i][jj];
     }
+}
+
+template <int RPL>
+__device__ __forceinline__ void panel_wc(double* __restrict__ W, int ldw, int m, int j0, int b,
+                                         double* __restrict__ V, int ldv, double* __restrict__ T, int ldt,
+                                         PanelWcSmem& sm) {
+    constexpr int B = 32, CPW = 32 / PWC_WARPS;  // columns per warp
+    static_assert(32 * RPL <= PWC_MAXR && CPW * PWC_WARPS == B, "panel shape");
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int mp = m - j0;
+    for (int e = tid; e < B * (B + 1); e += PWC_THREADS) (&sm.Gs[0][0])[e] = 0.0;  // entries past b stay zero
+    double p[CPW][RPL];
+#pragma unroll
+    for (int ci = 0; ci < CPW; ++ci) {
+        const int c = CPW * w + ci;
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            const int ri = lane + 32 * q;
+            p[ci][q] = (c < b && ri < mp) ? __ldcg(W + (size_t)(j0 + c) * ldw + j0 + ri) : 0.0;
+        }
+    }
+    // column c (slot c % CPW of warp c / CPW) into the step buffer `par`
+    auto publish = [&](int c, int par) {
+        const int ci = c % CPW;
+#pragma unroll
+        for (int cc = 0; cc < CPW; ++cc) {
+            if (cc != ci) continue;
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) {
+                const int ri = lane + 32 * q;
+                sm.ub[par][ri] = ri > c ? p[cc][q] : 0.0;
+            }
+            if (lane == c) sm.alph[par] = p[cc][0];
+        }
+    };
+    if (w == 0) publish(0, 0);
+    __syncthreads();
+#pragma unroll 1
+    for (int j = 0; j < b; ++j) {
+        const int par = j & 1;
+        double u[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) u[q] = sm.ub[par][lane + 32 * q];
+        const double alpha = sm.alph[par];
+        double x[CPW + 1];
+#pragma unroll
+        for (int ci = 0; ci < CPW; ++ci) {
+            double a0 = 0, a1 = 0;
+#pragma unroll
+            for (int q = 0; q < RPL; q += 2) {
+                a0 = fma(u[q], p[ci][q], a0);
+                if (q + 1 < RPL) a1 = fma(u[q + 1], p[ci][q + 1], a1);
+            }
+            x[ci] = a0 + a1;
+        }
+        {
+            double a0 = 0, a1 = 0;
+#pragma unroll
+            for (int q = 0; q < RPL; q += 2) {
+                a0 = fma(u[q], u[q], a0);
+                if (q + 1 < RPL) a1 = fma(u[q + 1], u[q + 1], a1);
+            }
+            x[CPW] = a0 + a1;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int v = 0; v <= CPW; ++v) x[v] += __shfl_xor_sync(0xffffffffu, x[v], o);
+        }
+        const double xn2 = x[CPW];
+        double tau = 0, beta = alpha, scal = 1;
+        if (xn2 > 0.0) {
+            const double nrm = sqrt(alpha * alpha + xn2);
+            beta = alpha >= 0 ? -nrm : nrm;
+            const double amb = alpha - beta;
+            const double rinv = 1.0 / (beta * amb);  // tau = -amb / beta, scal = 1 / amb
+            tau = -amb * amb * rinv;
+            scal = beta * rinv;
+        }
+#pragma unroll
+        for (int ci = 0; ci < CPW; ++ci) {
+            const int c = CPW * w + ci;
+            const double pj = __shfl_sync(0xffffffffu, p[ci][0], j);  // row j of column c
+            const double g = fma(scal, x[ci], pj);                   // v_j^T p_c
+            if (c > j && c < b) {
+                if (tau != 0.0) {
+                    const double t = tau * g, cu = t * scal;
+#pragma unroll
+                    for (int q = 0; q < RPL; ++q) p[ci][q] = fma(-cu, u[q], p[ci][q]);
+                    if (lane == j) p[ci][0] -= t;
+                }
+            } else if (c < j && lane == 0) {
+                sm.Gs[c][j] = sm.scals[c] * g;
+            }
+        }
+        if (w == j / CPW && lane == 0) {
+            sm.taus[j] = tau;
+            sm.scals[j] = scal;
+            sm.betas[j] = beta;
+        }
+        if (j + 1 < b && w == (j + 1) / CPW) publish(j + 1, par ^ 1);
+        __syncthreads();
+    }
+    // the factored panel: R above and on the diagonal, v below it
+#pragma unroll
+    for (int ci = 0; ci < CPW; ++ci) {
+        const int c = CPW * w + ci;
+        if (c < b) {
+            const double sc = sm.scals[c], be = sm.betas[c];
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) {
+                const int ri = lane + 32 * q;
+                if (ri < mp) {
+                    const double val = ri < c ? p[ci][q] : (ri == c ? be : sc * p[ci][q]);
+                    W[(size_t)(j0 + c) * ldw + j0 + ri] = val;
+                    if (V) V[(size_t)c * ldv + ri] = ri < c ? 0.0 : (ri == c ? 1.0 : val);
+                }
+            }
+        }
+    }
+    build_t(sm.Gs, sm.taus, sm.Tsm, sm.Xs, b, T, ldt);
 }
 
 // the panel by rows per lane
@@ -558,7 +565,7 @@ __device__ __forceinline__ void panel_wc_any(double* W, int ldw, int m, int j0, 
     else panel_wc<16>(W, ldw, m, j0, b, V, ldv, T, ldt, sm);
 }
 
-__global__ void __launch_bounds__(256) qr_panel_wc_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
+__global__ void __launch_bounds__(PWC_THREADS) qr_panel_wc_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
                                                          double* __restrict__ V, int ldv, double* __restrict__ T,
                                                          int ldt) {
     __shared__ PanelWcSmem sm;
@@ -571,7 +578,7 @@ template <int NT, int R, int B, int U>
 void launch_panel(cudaStream_t st, double* W, int ldw, int m, int j0, int b, double* V, int ldv, double* T, int ldt) {
     const int mp = m - j0;
     if (B == 32 && mp <= PWC_MAXR) {
-        qr_panel_wc_kernel<<<1, 256, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
+        qr_panel_wc_kernel<<<1, PWC_THREADS, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
     } else {
         qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
     }
@@ -827,7 +834,7 @@ __device__ bool wait_geq(const int* flag, int target, const int* err, long long 
 }
 
 struct WySmem {
-    double Zp[256];     // partial V^T C, [part][l][q]
+    double Zp[512];     // partial V^T C, [part][l][q] (one per thread)
     double Z2[32][8];
     double Ts[32][33];  // Ts[c][r] = T(r, c)
 };
@@ -842,8 +849,8 @@ struct WySmem {
 template <int NC>
 __device__ void wy_task(const double* __restrict__ V, int ldv, const double* __restrict__ T, int ldt, int b,
                         double* __restrict__ C, int ldc, int mp, int ncol, double* dyn, WySmem& ws) {
-    constexpr int B = 32, RT = 2, NPART = 256 / (B * NC);  // mp <= 512 rows: two per thread
-    static_assert(NPART * B * NC == 256, "one thread per (partition, l, q)");
+    constexpr int TH = PWC_THREADS, B = 32, RT = (512 + TH - 1) / TH, NPART = TH / (B * NC);  // mp <= 512 rows
+    static_assert(NPART * B * NC == TH, "one thread per (partition, l, q)");
     const int ld = mp + 1, tid = threadIdx.x;
     double* Vs = dyn;
     double* Cs = Vs + (size_t)ld * B;
@@ -851,7 +858,7 @@ __device__ void wy_task(const double* __restrict__ V, int ldv, const double* __r
     for (int col = 0; col < B; ++col) {
 #pragma unroll
         for (int h = 0; h < RT; ++h) {
-            const int r = tid + 256 * h;
+            const int r = tid + TH * h;
             if (r < mp) {
                 if (col < b && r > col) cp_async8(Vs + (size_t)col * ld + r, V + (size_t)col * ldv + r);
                 else Vs[(size_t)col * ld + r] = (col < b && r == col) ? 1.0 : 0.0;
@@ -862,11 +869,11 @@ __device__ void wy_task(const double* __restrict__ V, int ldv, const double* __r
     for (int col = 0; col < NC; ++col) {
 #pragma unroll
         for (int h = 0; h < RT; ++h) {
-            const int r = tid + 256 * h;
+            const int r = tid + TH * h;
             if (r < mp) Cs[(size_t)col * ld + r] = col < ncol ? __ldcg(C + (size_t)col * ldc + r) : 0.0;
         }
     }
-    for (int e = tid; e < B * B; e += 256) {
+    for (int e = tid; e < B * B; e += TH) {
         const int r = e & (B - 1), col = e / B;
         ws.Ts[col][r] = (r < b && col < b) ? __ldcg(T + (size_t)col * ldt + r) : 0.0;
     }
@@ -901,7 +908,7 @@ __device__ void wy_task(const double* __restrict__ V, int ldv, const double* __r
         ws.Z2[bb][q] = s;
     }
     __syncthreads();
-    for (int r = tid; r < mp; r += 256) {
+    for (int r = tid; r < mp; r += TH) {
         double acc[NC];
 #pragma unroll
         for (int q = 0; q < NC; ++q) acc[q] = Cs[(size_t)q * ld + r];
@@ -928,7 +935,7 @@ constexpr int QRP_MAXM = 512;
 constexpr int QRP_WB = 2;  // columns of W per task (the next panel's 32 columns make 16 tasks)
 constexpr int QRP_QB = 8;  // columns of Qt per task
 constexpr int QRP_UNAVAILABLE = -1;  // the persistent QR cannot be launched: take the look-ahead path
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(PWC_THREADS, 1)
     qr_persistent_kernel(double* __restrict__ W, int m, int n, int k, double* __restrict__ Tall,
                          double* __restrict__ Qt, int* __restrict__ sync, int* __restrict__ derr,
                          long long spin_limit) {
@@ -1167,8 +1174,9 @@ int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double
     TN_CUDA_CHECK(cudaGetDevice(&dev));
     const size_t smem = qrp_smem_bytes(QRP_MAXM);
     if (attr_dev != dev) {
-        TN_CUDA_CHECK(cudaFuncSetAttribute(qr_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        TN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_per_sm, qr_persistent_kernel, 256, smem));
+        TN_CUDA_CHECK(cudaFuncSetAttribute(qr_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        TN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_per_sm, qr_persistent_kernel, PWC_THREADS, smem));
         attr_dev = dev;
     }
     // Q forward inside the launch (Q^T accumulated m x m by the workers, beside
@@ -1198,11 +1206,14 @@ int qr_persistent(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double
     int* sync = c.qrsync.as<int>();
     int* derr = c.derr.as<int>();
     long long spin_limit = c.qr_spin_limit;
-    void* args[] = {&W, &m, &n, (void*)&k, &Tall, &Qt, &sync, &derr, &spin_limit};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr_persistent_kernel, dim3(G), dim3(256), args, smem, st);
-    if (e == cudaErrorCooperativeLaunchTooLarge) {
-        cudaGetLastError();
-        return QRP_UNAVAILABLE;
+    cudaError_t e;
+    {
+        void* args[] = {&W, &m, &n, (void*)&k, &Tall, &Qt, &sync, &derr, &spin_limit};
+        e = cudaLaunchCooperativeKernel((const void*)qr_persistent_kernel, dim3(G), dim3(PWC_THREADS), args, smem, st);
+        if (e == cudaErrorCooperativeLaunchTooLarge) {
+            cudaGetLastError();
+            return QRP_UNAVAILABLE;
+        }
     }
     TN_CUDA_CHECK(e);
     count_launch();

@@ -123,7 +123,7 @@ def test_lanczos_step_paths_agree(T, oracle, monkeypatch, fused):
     Lanczos (the oracle's Ritz value) on bulk sites with one, two and four
     vector elements per thread of the one-launch step (N = 8192, 180 000,
     307 200)."""
-    monkeypatch.setenv("TN_NO_FUSED_LZ", "0" if fused == "1" else "1")
+    monkeypatch.setenv("TN_FUSED_LZ", fused)
     c = T.Context(0)
     for (d, D, site) in [(2, 64, 3), (2, 300, 3), (3, 320, 3)]:
         W, A, F, G = envs(oracle, d, D, D, site)
@@ -185,10 +185,11 @@ def test_qr_rank_deficient_panels(T, ctx, oracle, m, n):
 
 @pytest.mark.parametrize("env", [{}, {"TN_QR_FORWARD_Q": "0"}, {"TN_NO_PERSISTENT_QR": "1"}])
 def test_qr_paths_gauge_shapes(T, oracle, monkeypatch, env):
-    """The persistent QR with the thin Q formed backwards (default) or Q^T
-    accumulated beside the panels, and the two-stream look-ahead QR, at the
-    gauge shapes of a bulk D = 256 site: same R as the oracle, orthonormal Q,
-    and zero-padded columns (a grown bond) completed to an orthonormal basis."""
+    """The persistent QR -- Q^T accumulated beside the panels (default) or the
+    thin Q formed after them -- and the two-stream look-ahead QR, at the gauge
+    shapes of a bulk
+    D = 256 site: same R as the oracle, orthonormal Q, and zero-padded columns
+    (a grown bond) completed to an orthonormal basis."""
     for k_, v_ in env.items():
         monkeypatch.setenv(k_, v_)
     c = T.Context(0)

@@ -90,6 +90,31 @@ def test_L2_h2(T):
     assert abs(E2 - E * E) < 1e-12
 
 
+@pytest.mark.parametrize("S,hz,bulk", [(0.5, 0.0, 9), (1.0, 0.1, 14)])
+def test_h2_mpo_compressed(T, S, hz, bulk):
+    """<H^2> contracts the product MPO H*H with its dependent bond directions
+    removed (Hamiltonian.C:8-16): bulk bonds well below Dw^2 = 25, boundary
+    bonds 1, and <H^2> on a random state unchanged against the exact product
+    (the trajectory tests compare the variance with the oracle's exact H*H)."""
+    import ctypes as C
+    ctx = T.Context(0)
+    L = 12
+    H = T.Factory(ctx).Make1D_NN_HeisenbergHamiltonian(L, S, T.RegularLower, 1.0, 1.0, hz)
+    dims = []
+    for site in range(1, L + 1):
+        a, b = C.c_int(), C.c_int()
+        assert ctx._lib.tn_hamiltonian_h2_dims(H.handle, site, C.byref(a), C.byref(b)) == 0
+        dims.append((a.value, b.value))
+    assert dims[0][0] == 1 and dims[-1][1] == 1
+    assert all(dims[i][1] == dims[i + 1][0] for i in range(L - 1))
+    assert max(b for _, b in dims) == bulk  # 25 uncompressed
+    psi = H.CreateMPS(6)
+    psi.InitializeWith(T.Random, seed=3)
+    psi.Normalize(T.DLeft)
+    E, E2 = psi.GetExpectation(H), psi.GetExpectationH2(H)
+    assert E2 >= E * E - 1e-9 * max(1.0, E2)
+
+
 @pytest.mark.parametrize("L,S,Dstart,lines,hz", [
     (10, 0.5, 8, [(3, 8, 1, E12, E12, 1e-10)], 0.0),                       # config 1 shape
     (24, 0.5, 16, [(2, 16, 1, E12, E12, 1e-10)], 0.0),
