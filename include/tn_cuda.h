@@ -310,6 +310,21 @@ int tn_qr(tn_ctx ctx, int m, int n, const double* A, int lda, double* Q, int ldq
           double* R, int ldr);
 int tn_lq(tn_ctx ctx, int m, int n, const double* A, int lda, double* L, int ldl,
           double* Q, int ldq);
+/* QRSolver<T>::SolveThinRQ / SolveThinQL (QRSolver.H:18-21,
+ * LapackQRSolver.C:163-274): A = R Q with R m x k (upper for m <= n), Q k x n
+ * orthonormal rows; A = Q L with Q m x k orthonormal columns, L k x n (lower
+ * for n <= m).  Householder QR of the index-reversed matrix. */
+int tn_rq(tn_ctx ctx, int m, int n, const double* A, int lda, double* R, int ldr, double* Q, int ldq);
+int tn_ql(tn_ctx ctx, int m, int n, const double* A, int lda, double* Q, int ldq, double* L, int ldl);
+/* QRSolver<T>::SolveRankRevealingQR / LQ / RQ / QL (LapackQRSolver.C:324-399):
+ * the thin factorisation, then the pivots with |T_ii| <= eps whose row (QR,
+ * QL) or column (LQ, RQ) of the triangular factor sums to at most eps are
+ * removed with the matching column / row of the orthonormal factor.  kind: 0
+ * QR, 1 LQ, 2 RQ, 3 QL.  QR / QL: F1 = Q (m x rank, ld1 >= m), F2 = R / L
+ * (rank x n, ld2 >= min(m, n)); LQ / RQ: F1 = L / R (m x rank), F2 = Q
+ * (rank x n).  *rank = columns / rows kept. */
+int tn_qr_rank_revealing(tn_ctx ctx, int kind, int m, int n, const double* A, int lda, double* F1, int ld1,
+                         double* F2, int ld2, double eps, int* rank);
 /* SVCompressor<T>::Compress (TensorNetworks/SVCompressor.H:20,
  * SVCompressorImp.C:19-73) on device data: s (k, descending) is truncated and
  * rescaled in place; U (m x k, ldu) and Vt (k x n, ldvt) keep their leading

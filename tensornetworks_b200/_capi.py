@@ -148,6 +148,9 @@ SIGNATURES = {
     "tn_svd_solve": (_I, [_V, _I, _I, _V, _I, _D, _I, _V, _I, _V, _V, _I]),
     "tn_svd_values": (_I, [_V, _I, _I, _V, _I, _V]),
     "tn_qr": (_I, [_V, _I, _I, _V, _I, _V, _I, _V, _I]),
+    "tn_rq": (_I, [_V, _I, _I, _V, _I, _V, _I, _V, _I]),
+    "tn_ql": (_I, [_V, _I, _I, _V, _I, _V, _I, _V, _I]),
+    "tn_qr_rank_revealing": (_I, [_V, _I, _I, _I, _V, _I, _V, _I, _V, _I, _D, _PI]),
     "tn_lq": (_I, [_V, _I, _I, _V, _I, _V, _I, _V, _I]),
     "tn_compress": (_I, [_V, _I, _D, _I, _V, _PI, _PD]),
 }

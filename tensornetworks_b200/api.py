@@ -702,6 +702,61 @@ class CudaQRSolver:
               "tn_lq")
         return _host(Lm, m, k), _host(Q, k, n)
 
+    def SolveThinRQ(self, A):
+        """A = R Q (LapackQRSolver.C:163-226): R m x k, Q k x n."""
+        torch = _torch()
+        m, n = np.shape(A)
+        k = min(m, n)
+        dA = _dev(A)
+        R = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        Q = torch.empty(k * n, dtype=torch.float64, device="cuda")
+        check(self.ctx._lib.tn_rq(self.ctx.handle, m, n, dA.data_ptr(), m, R.data_ptr(), m, Q.data_ptr(), k),
+              "tn_rq")
+        return _host(R, m, k), _host(Q, k, n)
+
+    def SolveThinQL(self, A):
+        """A = Q L (LapackQRSolver.C:229-274): Q m x k, L k x n."""
+        torch = _torch()
+        m, n = np.shape(A)
+        k = min(m, n)
+        dA = _dev(A)
+        Q = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        Lm = torch.empty(k * n, dtype=torch.float64, device="cuda")
+        check(self.ctx._lib.tn_ql(self.ctx.handle, m, n, dA.data_ptr(), m, Q.data_ptr(), m, Lm.data_ptr(), k),
+              "tn_ql")
+        return _host(Q, m, k), _host(Lm, k, n)
+
+    def _rank_revealing(self, kind, A, eps):
+        torch = _torch()
+        m, n = np.shape(A)
+        k = min(m, n)
+        dA = _dev(A)
+        F1 = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        F2 = torch.empty(k * n, dtype=torch.float64, device="cuda")
+        r = C.c_int(0)
+        check(self.ctx._lib.tn_qr_rank_revealing(self.ctx.handle, kind, m, n, dA.data_ptr(), m, F1.data_ptr(), m,
+                                                 F2.data_ptr(), k, float(eps), C.byref(r)), "tn_qr_rank_revealing")
+        rank = r.value
+        f1 = F1[: m * rank].cpu().numpy().reshape((rank, m)).T
+        f2 = F2.cpu().numpy()[: k * n].reshape((n, k)).T[:rank, :]
+        return f1, f2
+
+    def SolveRankRevealingQR(self, A, eps: float):
+        """(Q, R) with the zero rows of R and matching columns of Q removed (LapackQRSolver.C:367-373)."""
+        return self._rank_revealing(0, A, eps)
+
+    def SolveRankRevealingLQ(self, A, eps: float):
+        """(L, Q) with the zero columns of L and matching rows of Q removed (LapackQRSolver.C:393-399)."""
+        return self._rank_revealing(1, A, eps)
+
+    def SolveRankRevealingRQ(self, A, eps: float):
+        """(R, Q) with the zero columns of R and matching rows of Q removed (LapackQRSolver.C:374-380)."""
+        return self._rank_revealing(2, A, eps)
+
+    def SolveRankRevealingQL(self, A, eps: float):
+        """(Q, L) with the zero rows of L and matching columns of Q removed (LapackQRSolver.C:384-390)."""
+        return self._rank_revealing(3, A, eps)
+
 
 class CudaEigenSolver:
     """EigenSolver<double>::Solve (EigenSolver.H:31): lowest eigenpairs of a dense symmetric matrix."""

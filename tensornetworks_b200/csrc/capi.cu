@@ -779,6 +779,158 @@ int tn_lq(tn_ctx c, int m, int n, const double* A, int lda, double* L, int ldl, 
     return check_device_error(cx);
 }
 
+namespace {
+
+// Row / column abs sums of a column-major k x n matrix (rows: flag 0; columns: 1).
+__global__ void abs_sums_kernel(const double* __restrict__ M, int k, int n, int ld, int by_col,
+                                double* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cnt = by_col ? n : k;
+    if (t >= cnt) return;
+    double s = 0.0;
+    if (by_col)
+        for (int i = 0; i < k; ++i) s += fabs(M[(size_t)t * ld + i]);
+    else
+        for (int c = 0; c < n; ++c) s += fabs(M[(size_t)c * ld + t]);
+    out[t] = s;
+}
+
+// dst(r, c) = src(rows[r] or r, cols[c] or c): gather of kept rows / columns.
+__global__ void gather2d_kernel(int rows, int cols, const double* __restrict__ src, int lds, const int* ridx,
+                                const int* cidx, double* __restrict__ dst, int ldd) {
+    const long long total = (long long)rows * cols;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e % rows), c = (int)(e / rows);
+        const int sr = ridx ? ridx[r] : r, sc = cidx ? cidx[c] : c;
+        dst[(size_t)c * ldd + r] = src[(size_t)sc * lds + sr];
+    }
+}
+
+// The reference's ShrinkQR / ShrinkRQ (LapackQRSolver.C:324-365): the pivots of
+// the triangular factor T (k x n for rows, m x k for columns) with |T_ii| <= eps
+// whose whole row (column) sums to at most eps are dropped, with the matching
+// column (row) of the orthonormal factor O.  Outputs are written compacted.
+int shrink_factors(Ctx& cx, int k, const double* T, int ldt, int tr, int tc, bool rows, const double* O, int ldo,
+                   int orows, int ocols, double eps, double* Tout, int ldto, double* Oout, int ldoo, int* rank) {
+    cudaStream_t st = cx.stream;
+    DevBuf& sums = cx.apiw[2];
+    TN_CHECK(sums.ensure(sizeof(double) * (size_t)k + sizeof(int) * (size_t)k));
+    abs_sums_kernel<<<(k + 127) / 128, 128, 0, st>>>(T, tr, tc, ldt, rows ? 0 : 1, sums.as<double>());
+    TN_LAUNCH_CHECK();
+    std::vector<double> hs(k), diag(k);
+    TN_CUDA_CHECK(cudaMemcpyAsync(hs.data(), sums.p, sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+    for (int i = 0; i < k; ++i)
+        TN_CUDA_CHECK(cudaMemcpyAsync(&diag[i], T + (size_t)i * ldt + i, sizeof(double), cudaMemcpyDeviceToHost, st));
+    TN_CUDA_CHECK(cudaStreamSynchronize(st));
+    std::vector<int> keep;
+    for (int i = 0; i < k; ++i)
+        if (!(std::fabs(diag[i]) <= eps && hs[i] <= eps)) keep.push_back(i);
+    const int r = (int)keep.size();
+    *rank = r;
+    if (r == 0) return TN_OK;
+    int* dk = reinterpret_cast<int*>(sums.as<double>() + k);
+    TN_CUDA_CHECK(cudaMemcpyAsync(dk, keep.data(), sizeof(int) * r, cudaMemcpyHostToDevice, st));
+    const long long nt = rows ? (long long)r * tc : (long long)tr * r;
+    const long long no = rows ? (long long)orows * r : (long long)r * ocols;
+    auto grid = [](long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 4096)); };
+    if (rows) {  // T's kept rows, O's kept columns
+        gather2d_kernel<<<grid(nt), 256, 0, st>>>(r, tc, T, ldt, dk, nullptr, Tout, ldto);
+        TN_LAUNCH_CHECK();
+        gather2d_kernel<<<grid(no), 256, 0, st>>>(orows, r, O, ldo, nullptr, dk, Oout, ldoo);
+    } else {     // T's kept columns, O's kept rows
+        gather2d_kernel<<<grid(nt), 256, 0, st>>>(tr, r, T, ldt, nullptr, dk, Tout, ldto);
+        TN_LAUNCH_CHECK();
+        gather2d_kernel<<<grid(no), 256, 0, st>>>(r, ocols, O, ldo, dk, nullptr, Oout, ldoo);
+    }
+    TN_LAUNCH_CHECK();
+    TN_CUDA_CHECK(cudaStreamSynchronize(st));
+    return TN_OK;
+}
+
+}  // namespace
+
+// QRSolver::SolveThinRQ (LapackQRSolver.C:163-226): A = R Q with R m x k (upper
+// for m <= n) and Q k x n with orthonormal rows -- the QR of B = P_n A^T P_m
+// (P: index reversal), then R = P_m Rb^T P_k and Q = P_k Qb^T P_n.
+int tn_rq(tn_ctx c, int m, int n, const double* A, int lda, double* R, int ldr, double* Q, int ldq) {
+    if (!c || !A || !Q || !R || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
+    const int k = std::min(m, n);
+    if (ldr < m || ldq < k) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    DevBuf &W = cx.apiw[0], &Qb = cx.apiw[1], &Rb = cx.cqr;
+    TN_CHECK(W.ensure(sizeof(double) * (size_t)m * n));
+    TN_CHECK(Qb.ensure(sizeof(double) * (size_t)n * k));
+    TN_CHECK(Rb.ensure(sizeof(double) * (size_t)k * m));
+    // W (n x m, ld n): W(i, j) = A(m-1-j, n-1-i)
+    TN_CHECK(copy2d(n, m, A + (size_t)(n - 1) * lda + (m - 1), idx(-(long long)lda), idx(-1), W.as<double>(), idx(1),
+                    idx(n), 1.0, cx.stream));
+    TN_CHECK(qr_dense(cx, n, m, W.as<double>(), Qb.as<double>(), n, Rb.as<double>(), k));
+    // R(i, j) = Rb(k-1-j, m-1-i);  Q(i, j) = Qb(n-1-j, k-1-i)
+    TN_CHECK(copy2d(m, k, Rb.as<double>() + (size_t)(m - 1) * k + (k - 1), idx(-(long long)k), idx(-1), R, idx(1),
+                    idx(ldr), 1.0, cx.stream));
+    TN_CHECK(copy2d(k, n, Qb.as<double>() + (size_t)(k - 1) * n + (n - 1), idx(-(long long)n), idx(-1), Q, idx(1),
+                    idx(ldq), 1.0, cx.stream));
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return check_device_error(cx);
+}
+
+// QRSolver::SolveThinQL (LapackQRSolver.C:229-274): A = Q L with Q m x k
+// (orthonormal columns) and L k x n (lower for n <= m) -- the QR of
+// B = P_m A P_n, then Q = P_m Qb P_k and L = P_k Rb P_n.
+int tn_ql(tn_ctx c, int m, int n, const double* A, int lda, double* Q, int ldq, double* L, int ldl) {
+    if (!c || !A || !Q || !L || m < 1 || n < 1 || lda < m) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
+    const int k = std::min(m, n);
+    if (ldq < m || ldl < k) return TN_BAD_ARG;
+    Ctx& cx = c->c;
+    DevBuf &W = cx.apiw[0], &Qb = cx.apiw[1], &Rb = cx.cqr;
+    TN_CHECK(W.ensure(sizeof(double) * (size_t)m * n));
+    TN_CHECK(Qb.ensure(sizeof(double) * (size_t)m * k));
+    TN_CHECK(Rb.ensure(sizeof(double) * (size_t)k * n));
+    TN_CHECK(copy2d(m, n, A + (size_t)(n - 1) * lda + (m - 1), idx(-1), idx(-(long long)lda), W.as<double>(), idx(1),
+                    idx(m), 1.0, cx.stream));
+    TN_CHECK(qr_dense(cx, m, n, W.as<double>(), Qb.as<double>(), m, Rb.as<double>(), k));
+    TN_CHECK(copy2d(m, k, Qb.as<double>() + (size_t)(k - 1) * m + (m - 1), idx(-1), idx(-(long long)m), Q, idx(1),
+                    idx(ldq), 1.0, cx.stream));
+    TN_CHECK(copy2d(k, n, Rb.as<double>() + (size_t)(n - 1) * k + (k - 1), idx(-1), idx(-(long long)k), L, idx(1),
+                    idx(ldl), 1.0, cx.stream));
+    TN_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+    return check_device_error(cx);
+}
+
+// QRSolver::SolveRankRevealingQR / RQ / QL / LQ (LapackQRSolver.C:367-399): the
+// thin factorisation, then ShrinkQR / ShrinkRQ with eps.  kind: 0 QR (A = Q R),
+// 1 LQ (A = L Q), 2 RQ (A = R Q), 3 QL (A = Q L).  The outputs hold the kept
+// factors: QR / QL: F1 = Q m x rank, F2 = R / L rank x n;  LQ / RQ:
+// F1 = L / R m x rank, F2 = Q rank x n.  *rank = the number kept.
+int tn_qr_rank_revealing(tn_ctx c, int kind, int m, int n, const double* A, int lda, double* F1, int ld1,
+                         double* F2, int ld2, double eps, int* rank) {
+    if (!c || !A || !F1 || !F2 || !rank || m < 1 || n < 1 || lda < m || kind < 0 || kind > 3 || !(eps >= 0))
+        return TN_BAD_ARG;
+    const int k = std::min(m, n);
+    const bool col_first = (kind == 0 || kind == 3);  // Q first (m x k), triangle second (k x n)
+    if (ld1 < m || ld2 < k) return TN_BAD_ARG;
+    TN_ON_DEVICE(c->c.device);
+    Ctx& cx = c->c;
+    DevBuf &T1 = cx.rr1, &T2 = cx.rr2;
+    TN_CHECK(T1.ensure(sizeof(double) * (size_t)m * k));
+    TN_CHECK(T2.ensure(sizeof(double) * (size_t)k * n));
+    int st = TN_OK;
+    if (kind == 0) st = tn_qr(c, m, n, A, lda, T1.as<double>(), m, T2.as<double>(), k);
+    else if (kind == 1) st = tn_lq(c, m, n, A, lda, T1.as<double>(), m, T2.as<double>(), k);
+    else if (kind == 2) st = tn_rq(c, m, n, A, lda, T1.as<double>(), m, T2.as<double>(), k);
+    else st = tn_ql(c, m, n, A, lda, T1.as<double>(), m, T2.as<double>(), k);
+    TN_CHECK(st);
+    if (col_first)  // triangle T2 (k x n): rows dropped, with Q's columns
+        return shrink_factors(cx, k, T2.as<double>(), k, k, n, true, T1.as<double>(), m, m, k, eps, F2, ld2, F1, ld1,
+                              rank);
+    // triangle T1 (m x k): columns dropped, with Q's rows
+    return shrink_factors(cx, k, T1.as<double>(), m, m, k, false, T2.as<double>(), k, k, n, eps, F1, ld1, F2, ld2,
+                          rank);
+}
+
 // SVCompressorImp<T>::Compress (SVCompressorImp.C:19-73) on a device s vector.
 int tn_compress(tn_ctx c, int Dmax, double eps, int k, double* s, int* D_out, double* discarded) {
     if (!c || !s || k < 1 || !D_out) return TN_BAD_ARG;

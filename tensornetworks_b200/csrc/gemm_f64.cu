@@ -133,47 +133,61 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-template <bool A_MCONTIG, bool B_KCONTIG>
+// WM: rows of a warp's tile (32: CTA tile 64 x 64; 16: 32 x 64, twice the
+// CTAs for grids that would leave SMs idle or run one latency-bound CTA each).
+template <int WM, bool A_MCONTIG, bool B_KCONTIG>
 __global__ void __launch_bounds__(TNT) gemm_f64_dmma_kernel(LinGemm g) {
+    constexpr int BMT = 2 * WM, LDA = BMT + 4, RA = BMT * TBK / TNT, MI = WM / 8;
     if (g.skip && *g.skip) return;
-    __shared__ double As[TBK][TLD];
+    __shared__ double As[TBK][LDA];
     __shared__ double Bs[TBK][TLD];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int gid = lane >> 2, tig = lane & 3;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
+    const int wm = (warp >> 1) * WM, wn = (warp & 1) * 32;
+    const int m0 = blockIdx.y * BMT, n0 = blockIdx.x * TBN;
     const int b = blockIdx.z;
     const int b0 = b / g.nb1, b1 = b - b0 * g.nb1;
     const double* Ab = g.A + b0 * g.sA0 + b1 * g.sA1;
     const double* Bb = g.B + b0 * g.sB0 + b1 * g.sB1;
-    // tile slots: 8 per thread for A (TBK x TBM) and 8 for B (TBK x TBN)
-    double ra[8], rb[8];
+    // tile slots: RA per thread for A (TBK x BMT), 8 for B (TBK x TBN)
+    double ra[RA], rb[8];
     auto load = [&](int k0) {
+#pragma unroll
+        for (int r = 0; r < RA; ++r) {
+            const int e = t + TNT * r;
+            int am, ak;
+            if (A_MCONTIG) { am = e % BMT; ak = e / BMT; } else { ak = e % TBK; am = e / TBK; }
+            const int gm = m0 + am, gk = k0 + ak;
+            ra[r] = (gm < g.M && gk < g.K) ? __ldg(Ab + gm * g.sAm + gk * g.sAk) : 0.0;
+        }
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int e = t + TNT * r;
-            int am, ak, bk, bn;
-            if (A_MCONTIG) { am = e % TBM; ak = e / TBM; } else { ak = e % TBK; am = e / TBK; }
+            int bk, bn;
             if (B_KCONTIG) { bk = e % TBK; bn = e / TBK; } else { bn = e % TBN; bk = e / TBN; }
-            const int gm = m0 + am, gk = k0 + ak, hk = k0 + bk, gn = n0 + bn;
-            ra[r] = (gm < g.M && gk < g.K) ? __ldg(Ab + gm * g.sAm + gk * g.sAk) : 0.0;
+            const int hk = k0 + bk, gn = n0 + bn;
             rb[r] = (gn < g.N && hk < g.K) ? __ldg(Bb + hk * g.sBk + gn * g.sBn) : 0.0;
         }
     };
     auto store = [&]() {
 #pragma unroll
+        for (int r = 0; r < RA; ++r) {
+            const int e = t + TNT * r;
+            int am, ak;
+            if (A_MCONTIG) { am = e % BMT; ak = e / BMT; } else { ak = e % TBK; am = e / TBK; }
+            As[ak][am] = ra[r];
+        }
+#pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int e = t + TNT * r;
-            int am, ak, bk, bn;
-            if (A_MCONTIG) { am = e % TBM; ak = e / TBM; } else { ak = e % TBK; am = e / TBK; }
+            int bk, bn;
             if (B_KCONTIG) { bk = e % TBK; bn = e / TBK; } else { bn = e % TBN; bk = e / TBN; }
-            As[ak][am] = ra[r];
             Bs[bk][bn] = rb[r];
         }
     };
-    double acc[4][4][2];
+    double acc[MI][4][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     load(0);
@@ -183,13 +197,13 @@ __global__ void __launch_bounds__(TNT) gemm_f64_dmma_kernel(LinGemm g) {
         if (k0 + TBK < g.K) load(k0 + TBK);
 #pragma unroll
         for (int ks = 0; ks < TBK; ks += 4) {
-            double af[4], bf[4];
+            double af[MI], bf[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) af[i] = As[ks + tig][wm + i * 8 + gid];  // A(row gid, col tig)
+            for (int i = 0; i < MI; ++i) af[i] = As[ks + tig][wm + i * 8 + gid];  // A(row gid, col tig)
 #pragma unroll
             for (int j = 0; j < 4; ++j) bf[j] = Bs[ks + tig][wn + j * 8 + gid];  // B(row tig, col gid)
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < MI; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) dmma(acc[i][j], af[i], bf[j]);
         }
@@ -197,7 +211,7 @@ __global__ void __launch_bounds__(TNT) gemm_f64_dmma_kernel(LinGemm g) {
     }
     double* Cb = g.C + b0 * g.sC0 + b1 * g.sC1;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < MI; ++i) {
         const int gm = m0 + wm + i * 8 + gid;
         if (gm >= g.M) continue;
 #pragma unroll
@@ -241,11 +255,27 @@ int gemm_f64(const GemmArgs& g, cudaStream_t st) {
         l.sAm = g.A.mn.s; l.sAk = g.A.k.s; l.sBk = g.B.k.s; l.sBn = g.B.mn.s; l.sCm = g.C.m.s; l.sCn = g.C.n.s;
         l.sA0 = g.A.sb0; l.sA1 = g.A.sb1; l.sB0 = g.B.sb0; l.sB1 = g.B.sb1; l.sC0 = g.C.sb0; l.sC1 = g.C.sb1;
         l.A = g.A.ptr; l.B = g.B.ptr; l.C = g.C.ptr; l.alpha = g.alpha; l.beta = g.beta; l.skip = g.skip;
-        dim3 tg((g.N + TBN - 1) / TBN, (g.M + TBM - 1) / TBM, g.nb0 * g.nb1);
-        if (amc && bkc) gemm_f64_dmma_kernel<true, true><<<tg, TNT, 0, st>>>(l);
-        else if (amc && !bkc) gemm_f64_dmma_kernel<true, false><<<tg, TNT, 0, st>>>(l);
-        else if (!amc && bkc) gemm_f64_dmma_kernel<false, true><<<tg, TNT, 0, st>>>(l);
-        else gemm_f64_dmma_kernel<false, false><<<tg, TNT, 0, st>>>(l);
+        // 64 x 64 CTA tiles, or 32 x 64 when that grid would not fill two CTAs per SM
+        static int sms = 0;
+        if (sms == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+        }
+        const long long tiles64 = (long long)((g.N + TBN - 1) / TBN) * ((g.M + TBM - 1) / TBM) * g.nb0 * g.nb1;
+        if (tiles64 < 2LL * sms) {
+            dim3 tg((g.N + TBN - 1) / TBN, (g.M + 31) / 32, g.nb0 * g.nb1);
+            if (amc && bkc) gemm_f64_dmma_kernel<16, true, true><<<tg, TNT, 0, st>>>(l);
+            else if (amc && !bkc) gemm_f64_dmma_kernel<16, true, false><<<tg, TNT, 0, st>>>(l);
+            else if (!amc && bkc) gemm_f64_dmma_kernel<16, false, true><<<tg, TNT, 0, st>>>(l);
+            else gemm_f64_dmma_kernel<16, false, false><<<tg, TNT, 0, st>>>(l);
+        } else {
+            dim3 tg((g.N + TBN - 1) / TBN, (g.M + TBM - 1) / TBM, g.nb0 * g.nb1);
+            if (amc && bkc) gemm_f64_dmma_kernel<32, true, true><<<tg, TNT, 0, st>>>(l);
+            else if (amc && !bkc) gemm_f64_dmma_kernel<32, true, false><<<tg, TNT, 0, st>>>(l);
+            else if (!amc && bkc) gemm_f64_dmma_kernel<32, false, true><<<tg, TNT, 0, st>>>(l);
+            else gemm_f64_dmma_kernel<32, false, false><<<tg, TNT, 0, st>>>(l);
+        }
         TN_LAUNCH_CHECK();
         return TN_OK;
     }

@@ -97,9 +97,14 @@ __device__ __forceinline__ double basis_combine(const double* __restrict__ V, lo
 // step reaches it, so the loop ends at the latest at the basis limit.
 __device__ void lz_decide_step(LzState* st, int j, cudaGraphConditionalHandle cond) {
     const int nk = j + 1;
-    const double* a = st->alpha;
-    const double* b = st->beta;
-    const double th = block_eig_k(nk, a, b, 0);
+    __shared__ double a[LZ_MAXK], b[LZ_MAXK];
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+        a[i] = st->alpha[i];
+        b[i] = st->beta[i];
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;  // warp 0 decides (the callers' next barrier waits for it)
+    const double th = warp_eig_k(nk, a, b, 0);
     if (threadIdx.x == 0) {
         const double yl = last_component(nk, a, b, th);
         const double bj = b[j];
@@ -185,8 +190,8 @@ __global__ void lz_summary_kernel(const LzState* st, LzSummary* out, int kernels
     out->converged = st->converged;
     out->steps = st->steps;
     // first reset, per restart (reset, norm, scale, Ritz coefficients and vector,
-    // decision), this kernel, final reset, norm and scale
-    out->launches = 1 + 6LL * st->restarts + (long long)kernels_per_step * st->steps + 4;
+    // decision), this kernel
+    out->launches = 1 + 6LL * st->restarts + (long long)kernels_per_step * st->steps + 1;
 }
 
 // ||x||^2 -> st->xnorm (last block).
@@ -522,19 +527,32 @@ __global__ void __launch_bounds__(LZF_THREADS, LZF_BLOCKS_PER_SM) lz_step_kernel
 __global__ void lz_ritz_coeffs_kernel(LzState* st) {
     const int n = st->nb;
     if (n <= 0) return;
-    double th = block_eig_k(n, st->alpha, st->beta, 0);
-    double th2 = n > 1 ? block_eig_k(n, st->alpha, st->beta, 1) : th;
+    __shared__ double a[LZ_MAXK], b[LZ_MAXK];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a[i] = st->alpha[i];
+        b[i] = st->beta[i];
+    }
+    __syncthreads();
+    // warp 0 the lowest eigenvalue, warp 1 the next (the gap, for the statistics)
+    __shared__ double ths[2];
+    const int wv = threadIdx.x >> 5;
+    if (wv < 2) {
+        const double e = (wv == 0 || n > 1) ? warp_eig_k(n, a, b, wv) : 0.0;
+        if ((threadIdx.x & 31) == 0) ths[wv] = e;
+    }
+    __syncthreads();
+    const double th = ths[0], th2 = n > 1 ? ths[1] : th;
     if (threadIdx.x != 0) return;
     st->theta = th;
     st->theta2 = th2;
     __shared__ double y[LZ_MAXK], dl[LZ_MAXK], dd[LZ_MAXK], du[LZ_MAXK], du2[LZ_MAXK];
     __shared__ int piv[LZ_MAXK];
     double scale = 0;
-    for (int i = 0; i < n; ++i) scale = fmax(scale, fabs(st->alpha[i]) + (i < n - 1 ? fabs(st->beta[i]) : 0.0));
+    for (int i = 0; i < n; ++i) scale = fmax(scale, fabs(a[i]) + (i < n - 1 ? fabs(b[i]) : 0.0));
     scale = fmax(scale, 1e-300);
     for (int i = 0; i < n; ++i) y[i] = 1.0 + 0.1 * ((i * 7919) % 97) / 97.0;
     for (int it = 0; it < 3; ++it) {
-        tri_solve(n, st->alpha, st->beta, th + 4e-15 * scale, 2.2e-16 * scale, y, dl, dd, du, du2, piv);
+        tri_solve(n, a, b, th + 4e-15 * scale, 2.2e-16 * scale, y, dl, dd, du, du2, piv);
         double mx = 0;
         for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(y[i]));
         if (mx > 0) for (int i = 0; i < n; ++i) y[i] /= mx;
@@ -836,13 +854,7 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
             prev_resid = hs->resid;
         }
     }
-    // final normalisation of the Ritz vector
-    lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0, mm);
-    TN_LAUNCH_CHECK();
-    lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
-    TN_LAUNCH_CHECK();
-    lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, x, N, s, 0, nullptr);
-    TN_LAUNCH_CHECK();
+    // the Ritz vector V y is a unit vector already (orthonormal V, unit y)
     if (out) {
         out->theta = hs->theta;
         out->theta2 = hs->theta2;
@@ -982,12 +994,9 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
             return cudaGetLastError() == cudaSuccess ? TN_OK : TN_CUDA_ERROR;
         }, nullptr);
         if (rc != TN_OK) return fail(rc);
-        // the summary, then the final normalisation of the Ritz vector
+        // the summary (the Ritz vector V y is a unit vector already)
         rc = capture_into(st, g.graph, {n_out}, [&]() -> int {
             lz_summary_kernel<<<1, 32, 0, st>>>(s, sum, (int)kpi);
-            lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0, mm);
-            lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, N, partial, s);
-            lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, xw, N, s, 0, nullptr);
             return cudaGetLastError() == cudaSuccess ? TN_OK : TN_CUDA_ERROR;
         }, nullptr);
         if (rc != TN_OK) return fail(rc);

@@ -195,6 +195,7 @@ struct Ctx {
     DevBuf wterms;         // MPO term lists
     DevBuf misc;
     DevBuf apiw[3];        // staging copies of the dense-solver entry points
+    DevBuf cqr, rr1, rr2;  // RQ / QL factor staging; rank-revealing factorisations' full factors
     HostBuf pinned;
     int sm_count = 148;
     bool use_persistent_qr = true;  // TN_NO_PERSISTENT_QR=1: the two-stream look-ahead QR instead

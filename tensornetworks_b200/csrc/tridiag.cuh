@@ -71,6 +71,37 @@ __device__ double block_eig_k(int n, const double* a, const double* b, int k) {
     return 0.5 * (lo + hi);
 }
 
+// k-th smallest eigenvalue by multisection in ONE warp (every lane of the
+// calling warp must call it; a, b may be in shared or global memory): 32 Sturm
+// counts per round shrink the bracket 33-fold, so ~11 rounds reach rounding
+// level from the Gershgorin interval.  The block version spends 16 warps of
+// one SM on the same ~300-instruction counts per round; one warp costs a
+// sixteenth of the issue slots for one more round.
+__device__ double warp_eig_k(int n, const double* a, const double* b, int k) {
+    const int lane = threadIdx.x & 31;
+    double lo = a[0], hi = a[0];
+    for (int i = 0; i < n; ++i) {
+        const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i < n - 1 ? fabs(b[i]) : 0.0);
+        lo = fmin(lo, a[i] - r);
+        hi = fmax(hi, a[i] + r);
+    }
+    const double scale = fmax(fabs(lo), fabs(hi));
+    lo -= 1e-14 * scale + 1e-300;
+    hi += 1e-14 * scale + 1e-300;
+    const double inv = 1.0 / 33.0, frac = (double)(lane + 1) * inv;
+    for (int round = 0; round < 24; ++round) {
+        const double x = lo + (hi - lo) * frac;
+        const int ok = sturm_count(n, a, b, x) <= k;
+        const int cnt = __popc(__ballot_sync(0xffffffffu, ok));  // trial points with at most k eigenvalues below
+        const double nlo = cnt > 0 ? lo + (hi - lo) * ((double)cnt * inv) : lo;
+        const double nhi = cnt < 32 ? lo + (hi - lo) * ((double)(cnt + 1) * inv) : hi;
+        lo = nlo;
+        hi = nhi;
+        if (hi - lo <= 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300) break;
+    }
+    return 0.5 * (lo + hi);
+}
+
 // |last component| of the normalised eigenvector of T for eigenvalue th:
 // y_n^2 = p_{n-1}(th) / p_n'(th) with the monic characteristic polynomials of
 // the leading blocks (scaled recurrences; the ratio is scale-free).

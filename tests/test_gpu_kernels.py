@@ -208,6 +208,65 @@ def test_qr_paths_gauge_shapes(T, oracle, monkeypatch, env):
         assert np.abs(Q @ R - Ap).max() < 1e-12
 
 
+@pytest.mark.parametrize("m,n", [(7, 5), (5, 7), (64, 32), (32, 64), (256, 512), (512, 256), (130, 130)])
+def test_rq_ql(T, ctx, m, n):
+    """SolveThinRQ / SolveThinQL (LapackQRSolver.C:163-274): A = R Q with R upper
+    (m <= n) and orthonormal rows of Q; A = Q L with L lower (n <= m) and
+    orthonormal columns of Q."""
+    rng = np.random.default_rng(3 * m + n)
+    A = rng.uniform(-1, 1, size=(m, n))
+    k = min(m, n)
+    s = T.CudaQRSolver(ctx)
+    R, Q = s.SolveThinRQ(A)
+    assert np.abs(Q @ Q.T - np.eye(k)).max() < 1e-13
+    assert np.abs(R @ Q - A).max() < 1e-12
+    if m <= n:
+        assert np.allclose(np.triu(R), R)
+    Q2, L = s.SolveThinQL(A)
+    assert np.abs(Q2.T @ Q2 - np.eye(k)).max() < 1e-13
+    assert np.abs(Q2 @ L - A).max() < 1e-12
+    if n <= m:
+        assert np.allclose(np.tril(L), L)
+
+
+@pytest.mark.parametrize("kind", ["QR", "LQ", "RQ", "QL"])
+def test_rank_revealing(T, ctx, kind):
+    """SolveRankRevealingQR / LQ / RQ / QL (LapackQRSolver.C:324-399): four
+    columns (rows for the row forms) that depend on the others, placed where
+    the factorisation meets them last, leave four zero rows (columns) of the
+    triangular factor; those are removed with the matching part of Q and the
+    kept factors still give A."""
+    rng = np.random.default_rng(11)
+    m, n = (40, 24) if kind in ("QR", "QL") else (24, 40)
+    A = rng.uniform(-1, 1, size=(m, n))
+    M = rng.uniform(-1, 1, size=(4, 4))
+    if kind == "QR":
+        A[:, -4:] = A[:, :4] @ M
+    elif kind == "QL":
+        A[:, :4] = A[:, -4:] @ M
+    elif kind == "LQ":
+        A[-4:, :] = M @ A[:4, :]
+    else:
+        A[:4, :] = M @ A[-4:, :]
+    s = T.CudaQRSolver(ctx)
+    F1, F2 = getattr(s, "SolveRankRevealing" + kind)(A, 1e-10)
+    k = min(m, n)
+    if kind in ("QR", "QL"):
+        Q, Tr = F1, F2
+        assert Q.shape[1] == Tr.shape[0] == k - 4
+        assert np.abs(Q.T @ Q - np.eye(Q.shape[1])).max() < 1e-13
+        assert np.abs(Q @ Tr - A).max() < 1e-12
+    else:
+        Tr, Q = F1, F2
+        assert Tr.shape[1] == Q.shape[0] == k - 4
+        assert np.abs(Q @ Q.T - np.eye(Q.shape[0])).max() < 1e-13
+        assert np.abs(Tr @ Q - A).max() < 1e-12
+    # a full-rank matrix keeps everything
+    B = rng.uniform(-1, 1, size=(m, n))
+    G1, G2 = getattr(s, "SolveRankRevealing" + kind)(B, 1e-10)
+    assert (G1.shape[1] if kind in ("QR", "QL") else G2.shape[0]) == k
+
+
 def test_qr_zero_columns_complete(T, ctx):
     rng = np.random.default_rng(1)
     A = np.zeros((40, 16))
