@@ -139,7 +139,6 @@ __global__ void lz_reset_kernel(LzState* st, double tol, double tol_rel, int fir
         st->done = 0;
         st->nb = 0;
         st->counter = 0;
-        st->bar_count = 0;
         st->j = 0;
         st->jn = 0;
         st->mmax = mmax;
@@ -364,165 +363,6 @@ __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict_
     }
 }
 
-// ---- the fused step ----------------------------------------------------------
-//
-// lz_step_kernel<R> does the vector work of one step -- h = V^T w, w' = w - V h,
-// h2 = V^T w', |w'|, alpha and beta, the tridiagonal decision, and
-// v_{j+1} = (w' - V h2) / beta -- in ONE cooperative launch instead of the
-// three kernels above: the two global reductions are separated by grid-wide
-// barriers instead of kernel boundaries, w stays in registers (R elements per
-// thread, grid-strided), and every block reduces the per-block partials itself
-// in the same fixed order, so all blocks hold bitwise the same h, h2 and beta.
-// Block 0 writes the state and makes the decision after its share of the
-// vector.  Grid barriers poll with a limit; on expiry the kernel raises the
-// context's error word and returns (the host reads it as TN_CUDA_ERROR).
-constexpr int LZF_THREADS = 1024;    // 32 warps per SM keep enough basis loads in flight
-constexpr int LZF_BLOCKS_PER_SM = 1;  // one block per SM: the redundant reductions read G x nk partials
-
-__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ int ld_acquire_i32(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Grid-wide barrier over the blocks of a cooperative launch (all resident).
-// false when the wait ran out or another block raised the error word.
-__device__ bool lz_grid_sync(LzState* st, int* err, long long limit) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        const unsigned int g = ld_acquire_u32(&st->bar_gen);
-        __threadfence();
-        const unsigned int prev = atomicAdd(&st->bar_count, 1u);
-        if (prev == gridDim.x - 1) {
-            st->bar_count = 0;  // before the release: no block arrives again before it sees the new generation
-            __threadfence();
-            atomicAdd(&st->bar_gen, 1u);
-        } else {
-            for (long long it = 0; ld_acquire_u32(&st->bar_gen) == g; ++it) {
-                if (it >= limit || ((it & 255) == 255 && ld_acquire_i32(err))) {
-                    atomicExch(err, 1);
-                    ok = 0;
-                    break;
-                }
-                if (it > 4096) __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
-template <int R>
-__global__ void __launch_bounds__(LZF_THREADS, LZF_BLOCKS_PER_SM) lz_step_kernel(double* __restrict__ V, const double* __restrict__ w,
-                                                             long long N, double* partA, double* partB, LzState* st,
-                                                             double* __restrict__ xcur, int* err, long long limit,
-                                                             cudaGraphConditionalHandle cond) {
-    pdl_wait();
-    // every block reads done before the first barrier; block 0 writes it after the second
-    if (st->done) {
-        if (cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
-        return;
-    }
-    __shared__ double sh[KCHUNK * 32];
-    __shared__ double res[KCHUNK];
-    __shared__ double hs[LZ_MAXK + KCHUNK];
-    __shared__ double h2s[LZ_MAXK + KCHUNK];
-    const int j = st->j;
-    const int nk = j + 1;
-    const long long T = (long long)gridDim.x * blockDim.x;
-    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    double wr[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const long long i = t0 + r * T;
-        wr[r] = i < N ? w[i] : 0.0;
-    }
-    // h = V^T w
-    for (int k0 = 0; k0 < nk; k0 += KCHUNK) {
-        double v[KCHUNK] = {0};
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const long long i = t0 + r * T;
-            if (i < N) {
-                double x[KCHUNK];
-#pragma unroll
-                for (int q = 0; q < KCHUNK; ++q) x[q] = (k0 + q < nk) ? __ldg(V + (long long)(k0 + q) * N + i) : 0.0;
-#pragma unroll
-                for (int q = 0; q < KCHUNK; ++q) v[q] = fma(x[q], wr[r], v[q]);
-            }
-        }
-        block_sum_chunk(v, res, sh);
-        if (threadIdx.x < KCHUNK && k0 + (int)threadIdx.x < nk)
-            partA[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
-    }
-    if (!lz_grid_sync(st, err, limit)) return;
-    reduce_partials(partA, gridDim.x, LZ_MAXK, nk, hs, sh);
-    // w' = w - V h, then h2 = V^T w' and |w'|^2
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const long long i = t0 + r * T;
-        if (i < N) wr[r] = basis_combine(V, N, i, hs, nk, -1.0, wr[r]);
-    }
-    for (int k0 = 0; k0 < nk + 1; k0 += KCHUNK) {
-        double v[KCHUNK] = {0};
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const long long i = t0 + r * T;
-            if (i < N) {
-                double x[KCHUNK];
-#pragma unroll
-                for (int q = 0; q < KCHUNK; ++q) {
-                    const int k = k0 + q;
-                    x[q] = k < nk ? __ldg(V + (long long)k * N + i) : (k == nk ? wr[r] : 0.0);
-                }
-#pragma unroll
-                for (int q = 0; q < KCHUNK; ++q) v[q] = fma(x[q], wr[r], v[q]);
-            }
-        }
-        block_sum_chunk(v, res, sh);
-        if (threadIdx.x < KCHUNK && k0 + (int)threadIdx.x <= nk)
-            partB[(long long)blockIdx.x * LZ_MAXK + k0 + threadIdx.x] = res[threadIdx.x];
-    }
-    if (!lz_grid_sync(st, err, limit)) return;
-    reduce_partials(partB, gridDim.x, LZ_MAXK, nk + 1, h2s, sh);
-    double ss = 0;
-    for (int k = 0; k < nk; ++k) ss = fma(h2s[k], h2s[k], ss);
-    const double beta = sqrt(fmax(h2s[nk] - ss, 0.0));
-    const double inv = beta > 0 ? 1.0 / beta : 0.0;
-    double* vn = V + (long long)(j + 1) * N;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const long long i = t0 + r * T;
-        if (i < N) {
-            const double x = basis_combine(V, N, i, h2s, nk, -1.0, wr[r]) * inv;
-            vn[i] = x;
-            xcur[i] = x;
-        }
-    }
-    if (blockIdx.x != 0) return;
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < nk; ++k) {
-            st->h[k] = hs[k];
-            st->h2[k] = h2s[k];
-        }
-        st->alpha[j] = hs[j] + h2s[j];
-        st->beta[j] = beta;
-        st->matvecs += 1;
-        st->jn = j + 1;
-        st->j = j + 1;
-    }
-    __syncthreads();
-    lz_decide_step(st, j, cond);
-}
-
 // Ritz coefficients y of the lowest eigenpair of T_nb (inverse iteration), and theta2.
 __global__ void lz_ritz_coeffs_kernel(LzState* st) {
     const int n = st->nb;
@@ -648,20 +488,8 @@ inline int vec_grid(long long N, int sm) {
     return (int)b;
 }
 
-// Blocks of the fused step: LZF_BLOCKS_PER_SM per SM at most, fewer for short vectors.
-inline int fused_grid(long long N, int sm) {
-    long long b = (N + LZF_THREADS - 1) / LZF_THREADS;
-    if (b > (long long)sm * LZF_BLOCKS_PER_SM) b = (long long)sm * LZF_BLOCKS_PER_SM;
-    if (b < 1) b = 1;
-    return (int)b;
-}
-constexpr int LZF_MAXR = 4;  // elements per thread the fused step keeps in registers
-
-// Per-block partial sums the solves need: the three-kernel step's, then the
-// fused step's two sets.
-inline size_t partial_doubles(long long N, int sm) {
-    return (2 * (size_t)vec_grid(N, sm) + 2 * (size_t)fused_grid(N, sm)) * LZ_MAXK;
-}
+// Per-block partial sums a step needs: the dots', then the update's.
+inline size_t partial_doubles(long long N, int sm) { return 2 * (size_t)vec_grid(N, sm) * LZ_MAXK; }
 
 }  // namespace
 
@@ -672,57 +500,9 @@ int step_matvec_dots(Ctx& c, const MatvecFn& mv, int grid, const double* V, doub
     return launch_pdl(lz_dots_kernel, grid, LZ_THREADS, 0, c.stream, V, (const double*)w, N, partial, s);
 }
 
-// Whether the fused step serves a vector of N elements on this context.
-static bool fused_step_ok(const Ctx& c, long long N) {
-    const long long per = (long long)fused_grid(N, c.sm_count) * LZF_THREADS;
-    return c.use_fused_lz && (N + per - 1) / per <= LZF_MAXR;
-}
-
-// The vector work of one step as one cooperative launch (lz_step_kernel); the
-// partials after the three-kernel step's (partial + vec_grid * LZ_MAXK).
-static int launch_fused_step(Ctx& c, long long N, double* V, const double* w, double* partial, LzState* s,
-                             double* xcur, cudaGraphConditionalHandle cond) {
-    const int G = fused_grid(N, c.sm_count);
-    const long long per = (long long)G * LZF_THREADS;
-    const long long R = (N + per - 1) / per;
-    double* partA = partial + 2 * (size_t)vec_grid(N, c.sm_count) * LZ_MAXK;
-    double* partB = partA + (size_t)G * LZ_MAXK;
-    int* err = c.derr.as<int>();
-    long long limit = c.lz_spin_limit;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(G);
-    cfg.blockDim = dim3(LZF_THREADS);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = c.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaError_t e;
-    if (R <= 1) e = cudaLaunchKernelEx(&cfg, lz_step_kernel<1>, V, w, N, partA, partB, s, xcur, err, limit, cond);
-    else if (R <= 2) e = cudaLaunchKernelEx(&cfg, lz_step_kernel<2>, V, w, N, partA, partB, s, xcur, err, limit, cond);
-    else e = cudaLaunchKernelEx(&cfg, lz_step_kernel<LZF_MAXR>, V, w, N, partA, partB, s, xcur, err, limit, cond);
-    TN_CUDA_CHECK(e);
-    count_launch();
-    return TN_OK;
-}
-
-static int ensure_error_word(Ctx& c) {
-    if (!c.derr.p) {
-        TN_CHECK(c.derr.ensure(sizeof(int)));
-        TN_CUDA_CHECK(cudaMemset(c.derr.p, 0, sizeof(int)));
-    }
-    return TN_OK;
-}
-
-// One Lanczos step: the matvec, then the vector work (fused or three kernels).
-static int enqueue_lz_step(Ctx& c, const MatvecFn& mv, bool fused, int grid, double* V, double* w, double* xcur,
-                           long long N, double* partial, LzState* s, cudaGraphConditionalHandle cond) {
-    if (fused) {
-        TN_CHECK(mv(xcur, w, &s->done));
-        return launch_fused_step(c, N, V, w, partial, s, xcur, cond);
-    }
+// One Lanczos step: the matvec, then the vector work as three kernels.
+static int enqueue_lz_step(Ctx& c, const MatvecFn& mv, int grid, double* V, double* w, double* xcur, long long N,
+                           double* partial, LzState* s, cudaGraphConditionalHandle cond) {
     double* partB = partial + (size_t)grid * LZ_MAXK;
     TN_CHECK(step_matvec_dots(c, mv, grid, V, w, xcur, N, partial, s));
     TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, c.stream, (const double*)V, w, N,
@@ -740,8 +520,6 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
     if ((long long)mm > N) mm = (int)N;
     if (mm < 1) mm = 1;
     const int grid = vec_grid(N, c.sm_count);
-    const bool fused = fused_step_ok(c, N);
-    if (fused) TN_CHECK(ensure_error_word(c));
     // workspace: V (mm+1 vectors), w, xcur, partials
     size_t need = sizeof(double) * ((size_t)(mm + 3) * N + partial_doubles(N, c.sm_count) + 64);
     TN_CHECK(c.lz.ensure(need));
@@ -756,7 +534,7 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
 
     // one Lanczos step; cond != 0 inside the graph body
     auto enqueue_step = [&](cudaGraphConditionalHandle cond) -> int {
-        return enqueue_lz_step(c, mv, fused, grid, V, w, xcur, N, partial, s, cond);
+        return enqueue_lz_step(c, mv, grid, V, w, xcur, N, partial, s, cond);
     };
 
     LzGraph* gr = nullptr;
@@ -765,7 +543,6 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         key = hash_val(key, N);
         key = hash_val(key, mm);
         key = hash_val(key, grid);
-        key = hash_val(key, fused);
         key = hash_val(key, (const void*)V);
         key = hash_val(key, (const void*)s);
         key = hash_val(key, st);
@@ -863,7 +640,6 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         out->restarts = restarts;
         out->converged = converged ? 1 : 0;
     }
-    if (fused) TN_CHECK(check_device_error(c));  // a grid barrier of the fused step that ran out
     if (!std::isfinite(hs->theta)) {
         set_error("lanczos: non-finite Ritz value");
         return TN_NAN_DETECTED;
@@ -917,8 +693,6 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
     if (mm < 1) mm = 1;
     const int maxR = maxRestarts > 0 ? maxRestarts : 1;
     const int grid = vec_grid(N, c.sm_count);
-    const bool fused = fused_step_ok(c, N);
-    if (fused) TN_CHECK(ensure_error_word(c));
     // workspace: V (mm+1 vectors), w, xcur, the solve's copy of x, partials
     size_t need = sizeof(double) * ((size_t)(mm + 4) * N + partial_doubles(N, c.sm_count) + 64);
     TN_CHECK(c.lz.ensure(need));
@@ -933,7 +707,7 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
     LzSummary* sum = c.lzsum.as<LzSummary>();
     unsigned long long key = hash_val(graph_key, 0x6e65737465644c5aULL);
     for (unsigned long long v : {(unsigned long long)N, (unsigned long long)mm, (unsigned long long)maxR,
-                                 (unsigned long long)grid, (unsigned long long)fused, alloc_generation()})
+                                 (unsigned long long)grid, alloc_generation()})
         key = hash_val(key, v);
     key = hash_val(key, tol);
     key = hash_val(key, tol_rel);
@@ -983,7 +757,7 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
         }
         const unsigned long long n0 = launch_count();
         rc = capture_into(st, b_in, {}, [&]() -> int {
-            return enqueue_lz_step(c, mv, fused, grid, V, w, xcur, N, partial, s, h_in);
+            return enqueue_lz_step(c, mv, grid, V, w, xcur, N, partial, s, h_in);
         }, nullptr);
         const unsigned long long kpi = launch_count() - n0;
         if (rc != TN_OK) return fail(rc);

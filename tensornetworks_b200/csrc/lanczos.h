@@ -27,9 +27,6 @@ struct LzState {
     // and the residual of the previous restart
     int restarts, steps;
     double prev_resid;
-    // grid barrier of the fused step kernel: arrivals, and the generation the
-    // last arrival advances (waiters poll it)
-    unsigned int bar_count, bar_gen;
 };
 
 struct LzResult {

@@ -201,10 +201,6 @@ struct Ctx {
     bool use_persistent_qr = true;  // TN_NO_PERSISTENT_QR=1: the two-stream look-ahead QR instead
     bool qr_forward_q = true;       // TN_QR_FORWARD_Q=0: the persistent QR forms the thin Q after the panels
     long long qr_spin_limit = 1LL << 21;  // polls per wait in the persistent QR (TN_QR_SPIN_LIMIT)
-    // one cooperative kernel per Lanczos step for the vector work instead of
-    // three kernels (TN_FUSED_LZ=1); polls per wait of its grid barriers
-    bool use_fused_lz = false;
-    long long lz_spin_limit = 1LL << 21;
     // cache of the last MPO term list uploaded through the C ABI
     std::vector<double> wcache_W;
     int wcache_key[4] = {0, 0, 0, 0};

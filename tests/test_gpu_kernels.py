@@ -117,13 +117,10 @@ def test_lanczos_heff(T, ctx, oracle, d, D1, D2, site):
     assert abs(th.value - tho) < 1e-10 * max(1, abs(tho))
 
 
-@pytest.mark.parametrize("fused", ["0", "1"])
-def test_lanczos_step_paths_agree(T, oracle, monkeypatch, fused):
-    """The one-launch cooperative step and the three-kernel step give the same
-    Lanczos (the oracle's Ritz value) on bulk sites with one, two and four
-    vector elements per thread of the one-launch step (N = 8192, 180 000,
-    307 200)."""
-    monkeypatch.setenv("TN_FUSED_LZ", fused)
+def test_lanczos_bulk_sizes(T, oracle):
+    """The device Lanczos gives the oracle's Ritz value on bulk sites whose
+    vectors fill a fraction of the grid, about one element per thread and
+    several per thread (N = 8192, 180 000, 307 200)."""
     c = T.Context(0)
     for (d, D, site) in [(2, 64, 3), (2, 300, 3), (3, 320, 3)]:
         W, A, F, G = envs(oracle, d, D, D, site)
