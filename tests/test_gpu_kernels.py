@@ -180,6 +180,22 @@ def test_qr_rank_deficient_panels(T, ctx, oracle, m, n):
     assert np.abs(Q @ R - A).max() < 1e-12
 
 
+@pytest.mark.parametrize("cond", [1.0, 1e4, 1e8, 1e14])
+def test_qr_graded_conditioning(T, ctx, oracle, cond):
+    """The gauge shape 512 x 256 with singular values graded over `cond` (the
+    spread of a site tensor's Schmidt values): orthonormal Q, Q R = A, and R
+    equal to the oracle's up to the rounding that the conditioning amplifies."""
+    rng = np.random.default_rng(int(np.log10(cond)) + 5)
+    m, n = 512, 256
+    U, _ = np.linalg.qr(rng.standard_normal((m, n)))
+    V, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = (U * np.logspace(0, -np.log10(cond), n)) @ V.T
+    Q, R = T.CudaQRSolver(ctx).SolveThinQR(A)
+    assert np.abs(Q.T @ Q - np.eye(n)).max() < 1e-13
+    assert np.abs(Q @ R - A).max() < 1e-13
+    np.testing.assert_allclose(R, oracle.qr(A)[1], atol=1e-14 * max(1.0, cond ** 0.5), rtol=0)
+
+
 @pytest.mark.parametrize("env", [{}, {"TN_QR_FORWARD_Q": "0"}, {"TN_NO_PERSISTENT_QR": "1"}])
 def test_qr_paths_gauge_shapes(T, oracle, monkeypatch, env):
     """The persistent QR -- Q^T accumulated beside the panels (default) or the
