@@ -465,23 +465,24 @@ __global__ void dv_correct_kernel(const double* __restrict__ r, const double* __
     const double eps = 1e-8 * fmax(1.0, fabs(th));
     const bool use_mlp = (w16 != nullptr) && st->learned && !st->stalled;
     if (use_mlp) {
-        __shared__ float w[MLP_NP];
-        for (int e = threadIdx.x; e < MLP_NP; e += blockDim.x) w[e] = __bfloat162float(w16[e]);
+        __shared__ MlpInferSmem s;
+        mlp_stage(w16, s);
         __syncthreads();
         const double rs = st->rms_r, sg = st->sigma;
         const float sqn = (float)sqrt((double)N);
         const float rinv = rs > 0 ? (float)(1.0 / rs) : 0.f, sinv = (float)(1.0 / sg);
         const float pos = (float)st->pos;
         const double back = rs / sg;
-        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
-             i += (long long)gridDim.x * blockDim.x) {
-            float f[MLP_IN];
-            f[0] = mlp_clip((float)(diag[i] - th) * sinv, MLP_FEAT_CLIP);
-            f[1] = mlp_clip((float)r[i] * rinv, MLP_FEAT_CLIP);
-            f[2] = mlp_clip((float)u[i] * sqn, MLP_FEAT_CLIP);
-            f[3] = pos;
-            t[i] = diag_correction(r[i], diag[i], th, eps) + (double)mlp_eval(w, f) * back;
-        }
+        mlp_tiles(
+            s, N,
+            [&](long long i, float(&f)[MLP_IN]) {
+                const bool in = i < N;
+                f[0] = in ? mlp_clip((float)(diag[i] - th) * sinv, MLP_FEAT_CLIP) : 0.f;
+                f[1] = in ? mlp_clip((float)r[i] * rinv, MLP_FEAT_CLIP) : 0.f;
+                f[2] = in ? mlp_clip((float)u[i] * sqn, MLP_FEAT_CLIP) : 0.f;
+                f[3] = pos;
+            },
+            [&](long long i, float y) { t[i] = diag_correction(r[i], diag[i], th, eps) + (double)y * back; });
         if (blockIdx.x == 0 && threadIdx.x == 0) st->learned_steps += 1;
         return;
     }

@@ -7,8 +7,8 @@
 // correction x/(u.x) - u towards the converged eigenvector x, minus the
 // diagonal correction r/(theta - diag)).
 //
-// Inference reads BF16 weights (FP32 in shared memory, FP32 accumulation);
-// training keeps an FP32 master copy: per block, every thread runs forward
+// Inference reads BF16 weights, with the hidden layer on the tensor cores
+// (mlp_tiles); training keeps an FP32 master copy: per block, every thread runs forward
 // and backward for one pair, the activations go to shared memory, and the
 // weight gradients are reduced there (dW2 = H1^T dH2 as a 64 x 64 x chunk
 // product), then written as one partial per block and summed in a fixed
@@ -28,15 +28,16 @@ constexpr int TR_THREADS = 128;  // pairs per block and chunk
 
 __global__ void mlp_forward_kernel(const __nv_bfloat16* __restrict__ w16, const float* __restrict__ F, long long n,
                                    float* __restrict__ Y) {
-    __shared__ float w[MLP_NP];
-    for (int e = threadIdx.x; e < MLP_NP; e += blockDim.x) w[e] = __bfloat162float(w16[e]);
+    __shared__ MlpInferSmem s;
+    mlp_stage(w16, s);
     __syncthreads();
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        float f[MLP_IN];
+    mlp_tiles(
+        s, n,
+        [&](long long e, float(&f)[MLP_IN]) {
 #pragma unroll
-        for (int q = 0; q < MLP_IN; ++q) f[q] = F[i * MLP_IN + q];
-        Y[i] = mlp_eval(w, f);
-    }
+            for (int q = 0; q < MLP_IN; ++q) f[q] = e < n ? F[e * MLP_IN + q] : 0.f;
+        },
+        [&](long long e, float y) { Y[e] = y; });
 }
 
 // Gradient of L = inv_n * sum (y - t)^2 over pairs [first, first + count) of
@@ -269,7 +270,7 @@ int mlp_get_params(const MlpModel& m, float* host) {
 
 int mlp_forward(const MlpModel& m, const float* F, long long n, float* Y, cudaStream_t st) {
     if (n <= 0) return TN_OK;
-    const long long b = (n + 255) / 256;
+    const long long b = (n + 127) / 128;  // 8 warps of 16-element tiles per block
     const int grid = (int)std::min<long long>(b, (long long)m.ctx->sm_count * 4);
     mlp_forward_kernel<<<grid, 256, 0, st>>>(m.w16.as<__nv_bfloat16>(), F, n, Y);
     TN_LAUNCH_CHECK();
