@@ -1301,6 +1301,269 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
     return TN_OK;
 }
 
+// ---- tall matrices (512 < m <= 1536) -----------------------------------------
+//
+// 16-column panels factored by qr_panel_tall_kernel -- one CTA, warp w owns
+// column w with RPL rows per lane in registers, the reflector u_j read from
+// shared memory in the dot pass and again in the update pass (holding it in
+// registers as panel_wc does would need 4 RPL registers a thread) -- then the
+// panel's block reflector applied to the trailing columns, and after the last
+// panel to Q (formed backwards, the dorgqr order), by wy_cols_kernel: one CTA
+// per four columns c of C, z = V^T c, z2 = T' z, c -= V z2, with V (read
+// below the diagonal of the factored W) and T read through L1.
+constexpr int TALL_B = 16;        // columns per panel (one per warp)
+constexpr int TALL_MAXR = 1536;   // rows
+
+struct PanelTallSmem {
+    double ub[2][TALL_MAXR];  // u_j by step parity
+    double alph[2];
+    double Gs[32][33];        // Gs[l][jj] = v_l^T v_jj, l < jj (b <= 16 of 32 used)
+    double taus[32], scals[32], betas[32];
+    double Tsm[32][33];
+    double Xs[32][33];
+};
+
+template <int RPL>
+__global__ void __launch_bounds__(PWC_THREADS, 1) qr_panel_tall_kernel(double* __restrict__ W, int ldw, int m, int j0,
+                                                                        int b, double* __restrict__ T, int ldt) {
+    static_assert(32 * RPL <= TALL_MAXR, "panel rows");
+    extern __shared__ double tall_dyn[];
+    PanelTallSmem& sm = *reinterpret_cast<PanelTallSmem*>(tall_dyn);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;  // warp w: column w of the panel (w < b)
+    const int mp = m - j0;
+    for (int e = tid; e < 32 * 33; e += PWC_THREADS) (&sm.Gs[0][0])[e] = 0.0;
+    double p[RPL];
+#pragma unroll
+    for (int q = 0; q < RPL; ++q) {
+        const int ri = lane + 32 * q;
+        p[q] = (w < b && ri < mp) ? __ldcg(W + (size_t)(j0 + w) * ldw + j0 + ri) : 0.0;
+    }
+    auto publish = [&](int c, int par) {  // by the warp that owns column c
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            const int ri = lane + 32 * q;
+            sm.ub[par][ri] = ri > c ? p[q] : 0.0;
+        }
+        if (lane == c) sm.alph[par] = p[0];
+    };
+    if (w == 0) publish(0, 0);
+    __syncthreads();
+#pragma unroll 1
+    for (int j = 0; j < b; ++j) {
+        const int par = j & 1;
+        const double* u = sm.ub[par];
+        const double alpha = sm.alph[par];
+        double x0 = 0, x1 = 0, n0 = 0, n1 = 0;
+#pragma unroll
+        for (int q = 0; q < RPL; q += 2) {
+            const double ua = u[lane + 32 * q];
+            x0 = fma(ua, p[q], x0);
+            n0 = fma(ua, ua, n0);
+            if (q + 1 < RPL) {
+                const double ub = u[lane + 32 * (q + 1)];
+                x1 = fma(ub, p[q + 1], x1);
+                n1 = fma(ub, ub, n1);
+            }
+        }
+        double x = x0 + x1, xn2 = n0 + n1;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_xor_sync(0xffffffffu, x, o);
+            xn2 += __shfl_xor_sync(0xffffffffu, xn2, o);
+        }
+        double tau = 0, beta = alpha, scal = 1;
+        if (xn2 > 0.0) {
+            const double nrm = sqrt(alpha * alpha + xn2);
+            beta = alpha >= 0 ? -nrm : nrm;
+            const double amb = alpha - beta;
+            const double rinv = 1.0 / (beta * amb);  // tau = -amb / beta, scal = 1 / amb
+            tau = -amb * amb * rinv;
+            scal = beta * rinv;
+        }
+        const double pj = __shfl_sync(0xffffffffu, p[0], j);  // row j of this warp's column
+        const double g = fma(scal, x, pj);                   // v_j^T p
+        if (w > j && w < b) {
+            if (tau != 0.0) {
+                const double tt = tau * g, cu = tt * scal;
+#pragma unroll
+                for (int q = 0; q < RPL; ++q) p[q] = fma(-cu, u[lane + 32 * q], p[q]);
+                if (lane == j) p[0] -= tt;
+            }
+        } else if (w < j && lane == 0) {
+            sm.Gs[w][j] = sm.scals[w] * g;
+        }
+        if (w == j && lane == 0) {
+            sm.taus[j] = tau;
+            sm.scals[j] = scal;
+            sm.betas[j] = beta;
+        }
+        if (j + 1 < b && w == j + 1) publish(j + 1, par ^ 1);
+        __syncthreads();
+    }
+    // the factored panel: R above and on the diagonal, v below it
+    if (w < b) {
+        const double sc = sm.scals[w], be = sm.betas[w];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            const int ri = lane + 32 * q;
+            if (ri < mp) W[(size_t)(j0 + w) * ldw + j0 + ri] = ri < w ? p[q] : (ri == w ? be : sc * p[q]);
+        }
+    }
+    build_t(sm.Gs, sm.taus, sm.Tsm, sm.Xs, b, T, ldt);
+}
+
+// C (mp x nc, ld ldc) <- (I - V T' V^T) C, V mp x b (b <= 16) unit lower
+// trapezoidal read below its diagonal (ld ldv), T' = T^T (TRANS: applying
+// Q^T, the trailing update) or T (forming Q); T b x b upper, ld ldt.  One CTA
+// per WYC_COLS columns of C; its 8 warps split the rows (so that enough loads
+// are in flight), each warp's partial V^T c reduced by a butterfly, the 8
+// partials summed through shared memory in a fixed order.
+constexpr int WYC_COLS = 4;
+constexpr int WYC_THREADS = 256;
+
+template <bool TRANS>
+__global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __restrict__ V, int ldv,
+                                                              const double* __restrict__ T, int ldt, int b,
+                                                              double* __restrict__ C, int ldc, int mp, int nc) {
+    constexpr int NW = WYC_THREADS / 32, NZ = WYC_COLS * TALL_B;
+    __shared__ double zs[NW][NZ];
+    __shared__ double zt[NZ];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int c0 = WYC_COLS * blockIdx.x;
+    double* Cc[WYC_COLS];
+#pragma unroll
+    for (int q = 0; q < WYC_COLS; ++q) Cc[q] = C + (size_t)min(c0 + q, nc - 1) * ldc;  // past nc: read, never written
+    double z[WYC_COLS][TALL_B];
+#pragma unroll
+    for (int q = 0; q < WYC_COLS; ++q)
+#pragma unroll
+        for (int l = 0; l < TALL_B; ++l) z[q][l] = 0.0;
+    for (int r = lane + 32 * w; r < mp; r += WYC_THREADS) {
+        double x[WYC_COLS];
+#pragma unroll
+        for (int q = 0; q < WYC_COLS; ++q) x[q] = Cc[q][r];
+#pragma unroll
+        for (int l = 0; l < TALL_B; ++l) {
+            if (l < b) {
+                const double v = r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0);
+#pragma unroll
+                for (int q = 0; q < WYC_COLS; ++q) z[q][l] = fma(v, x[q], z[q][l]);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < WYC_COLS; ++q)
+#pragma unroll
+            for (int l = 0; l < TALL_B; ++l) z[q][l] += __shfl_xor_sync(0xffffffffu, z[q][l], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < WYC_COLS; ++q)
+#pragma unroll
+            for (int l = 0; l < TALL_B; ++l) zs[w][q * TALL_B + l] = z[q][l];
+    }
+    __syncthreads();
+    if (threadIdx.x < NZ) {
+        double s = 0.0;
+#pragma unroll
+        for (int p = 0; p < NW; ++p) s += zs[p][threadIdx.x];
+        zt[threadIdx.x] = s;
+    }
+    __syncthreads();
+    // z2 = T' z: T^T z takes z_k for k <= l, T z takes k >= l
+#pragma unroll
+    for (int q = 0; q < WYC_COLS; ++q) {
+#pragma unroll
+        for (int l = 0; l < TALL_B; ++l) {
+            double a = 0.0;
+            if (l < b) {
+#pragma unroll
+                for (int k = 0; k < TALL_B; ++k) {
+                    if (k < b && (TRANS ? k <= l : k >= l))
+                        a = fma(TRANS ? T[(size_t)l * ldt + k] : T[(size_t)k * ldt + l], zt[q * TALL_B + k], a);
+                }
+            }
+            z[q][l] = a;
+        }
+    }
+    for (int r = lane + 32 * w; r < mp; r += WYC_THREADS) {
+        double x[WYC_COLS];
+#pragma unroll
+        for (int q = 0; q < WYC_COLS; ++q) x[q] = Cc[q][r];
+#pragma unroll
+        for (int l = 0; l < TALL_B; ++l) {
+            if (l < b) {
+                const double v = r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0);
+#pragma unroll
+                for (int q = 0; q < WYC_COLS; ++q) x[q] = fma(-v, z[q][l], x[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < WYC_COLS; ++q)
+            if (c0 + q < nc) Cc[q][r] = x[q];
+    }
+}
+
+template <int RPL>
+int launch_panel_tall(cudaStream_t st, double* W, int ldw, int m, int j0, int b, double* T, int ldt) {
+    static thread_local int attr_dev = -1;
+    int dev = 0;
+    TN_CUDA_CHECK(cudaGetDevice(&dev));
+    if (attr_dev != dev) {
+        TN_CUDA_CHECK(cudaFuncSetAttribute(qr_panel_tall_kernel<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sizeof(PanelTallSmem)));
+        attr_dev = dev;
+    }
+    qr_panel_tall_kernel<RPL><<<1, PWC_THREADS, sizeof(PanelTallSmem), st>>>(W, ldw, m, j0, b, T, ldt);
+    TN_LAUNCH_CHECK();
+    return TN_OK;
+}
+
+// Householder QR of an m x n matrix W (ld m), 512 < m <= 1536, in 16-column
+// panels; R to Rout (k x n), Q (m x k) to Qout, when given.
+int qr_tall(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout, int ldr) {
+    cudaStream_t st = c.stream;
+    const int k = std::min(m, n), B = TALL_B;
+    if (m > TALL_MAXR) return TN_BAD_SHAPE;
+    TN_CHECK(c.qrw.ensure(sizeof(double) * ((size_t)B * k + 16)));
+    double* Tall = c.qrw.as<double>();
+    auto update = [&](bool trans, int j0, int b, double* Cp, int ldc, int mp, int nc) -> int {
+        const int blocks = (nc + WYC_COLS - 1) / WYC_COLS;
+        const double* Vp = W + (size_t)j0 * m + j0;
+        const double* Tp = Tall + (size_t)j0 * B;
+        if (trans) wy_cols_kernel<true><<<blocks, WYC_THREADS, 0, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
+        else wy_cols_kernel<false><<<blocks, WYC_THREADS, 0, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
+        TN_LAUNCH_CHECK();
+        return TN_OK;
+    };
+    for (int j0 = 0; j0 < k; j0 += B) {
+        const int b = std::min(B, k - j0), mp = m - j0;
+        double* Tp = Tall + (size_t)j0 * B;
+        if (mp <= 512) TN_CHECK(launch_panel_tall<16>(st, W, m, m, j0, b, Tp, B));
+        else if (mp <= 768) TN_CHECK(launch_panel_tall<24>(st, W, m, m, j0, b, Tp, B));
+        else if (mp <= 1024) TN_CHECK(launch_panel_tall<32>(st, W, m, m, j0, b, Tp, B));
+        else if (mp <= 1280) TN_CHECK(launch_panel_tall<40>(st, W, m, m, j0, b, Tp, B));
+        else TN_CHECK(launch_panel_tall<48>(st, W, m, m, j0, b, Tp, B));
+        const int nt = n - j0 - b;
+        if (nt > 0) TN_CHECK(update(true, j0, b, W + (size_t)(j0 + b) * m + j0, m, mp, nt));
+    }
+    if (Rout) {
+        extract_r_kernel<<<g1d((long long)k * n), 256, 0, st>>>(W, m, k, n, Rout, ldr);
+        TN_LAUNCH_CHECK();
+    }
+    if (Qout) {
+        set_identity_kernel<<<g1d((long long)m * k), 256, 0, st>>>(Qout, m, k, ldq);
+        TN_LAUNCH_CHECK();
+        for (int j0 = ((k - 1) / B) * B; j0 >= 0; j0 -= B) {
+            const int b = std::min(B, k - j0);
+            TN_CHECK(update(false, j0, b, Qout + (size_t)j0 * ldq + j0, ldq, m - j0, k - j0));
+        }
+    }
+    return TN_OK;
+}
+
 }  // namespace
 
 int check_device_error(Ctx& c) {
@@ -1317,6 +1580,7 @@ int qr_dense(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rou
     cudaStream_t st = c.stream;
     if (m <= 0 || n <= 0) return TN_BAD_SHAPE;
     if (m <= 512) return qr_dense_reg<256, 2, 32, 2>(c, m, n, W, Qout, ldq, Rout, ldr);
+    if (m <= TALL_MAXR && (m > 1024 || c.qr_tall_mid)) return qr_tall(c, m, n, W, Qout, ldq, Rout, ldr);
     if (m <= 1024) return qr_dense_reg<256, 4, 16, 2>(c, m, n, W, Qout, ldq, Rout, ldr);
     const int k = std::min(m, n);
     const int bmax = panel_width(m);

@@ -180,6 +180,31 @@ def test_qr_rank_deficient_panels(T, ctx, oracle, m, n):
     assert np.abs(Q @ R - A).max() < 1e-12
 
 
+@pytest.mark.parametrize("mid", ["0", "1"])
+def test_qr_tall_path(T, oracle, monkeypatch, mid):
+    """The 16-column-panel QR for 512 < m <= 1536 (the S = 1, D = 512 gauge
+    shape 1536 x 512 among them; with TN_QR_TALL_MID=1 also for m <= 1024):
+    orthonormal Q, Q R = A and the oracle's R, ragged last panels and wide
+    matrices included; the LQ of the transposed shape goes the same way."""
+    monkeypatch.setenv("TN_QR_TALL_MID", mid)
+    c = T.Context(0)
+    rng = np.random.default_rng(41)
+    shapes = [(1536, 512), (1100, 300), (1300, 1400), (1536, 23)]
+    if mid == "1":
+        shapes += [(768, 256), (1024, 512), (600, 700), (513, 40)]
+    for m, n in shapes:
+        A = rng.uniform(-1, 1, size=(m, n))
+        Q, R = T.CudaQRSolver(c).SolveThinQR(A)
+        k = min(m, n)
+        assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-13, (m, n)
+        assert np.abs(Q @ R - A).max() < 1e-12, (m, n)
+        np.testing.assert_allclose(R, oracle.qr(A)[1], atol=1e-11)
+    A = rng.uniform(-1, 1, size=(512, 1536))
+    Lm, Q2 = T.CudaQRSolver(c).SolveThinLQ(A)
+    assert np.abs(Q2 @ Q2.T - np.eye(512)).max() < 1e-13
+    assert np.abs(Lm @ Q2 - A).max() < 1e-12
+
+
 @pytest.mark.parametrize("cond", [1.0, 1e4, 1e8, 1e14])
 def test_qr_graded_conditioning(T, ctx, oracle, cond):
     """The gauge shape 512 x 256 with singular values graded over `cond` (the
