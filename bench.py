@@ -331,6 +331,8 @@ def learned_arms(args, T, ctx, run_path, t_step, E_after, fp64_cmp):
 
 
 def run_ours(args, rank, world, local_rank):
+    import ctypes as C
+
     import numpy as np
     import torch
     torch.cuda.set_device(local_rank)
@@ -438,21 +440,38 @@ def run_ours(args, rank, world, local_rank):
     sched_stats, schedule_s = main_run["sched_stats"], main_run["schedule_s"]
     E_sched, E_after = main_run["E_sched"], main_run["E_after"]
 
-    # --- end to end through the C ABI with host buffers: per step upload the grown
-    #     snapshot, normalise + environments, one sweep pair, download all sites
+    # --- end to end through the C ABI with host buffers, as a reference-side
+    #     caller makes it: per step upload the grown snapshot from pinned host
+    #     memory in the library's (oml) site layout, normalise + environments,
+    #     one sweep pair, download every site into pinned host memory
     grown = main_run["grown"]
+    lib, hmps = psi._lib, psi.handle
+    up = []
+    for a in grown:
+        d_, D1_, D2_ = a.shape
+        buf = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        buf.numpy()[:] = np.transpose(a, (0, 2, 1)).ravel()  # A(n, i1, i2) at n*D1*D2 + i2*D1 + i1
+        up.append((D1_, D2_, buf))
+    down = [torch.empty(a.size, dtype=torch.float64, pin_memory=True) for a in grown]
     h2d = sum(a.nbytes for a in grown)
-    e2e_times, sites = [], None
+    e2e_times, d2h = [], 0
     for _ in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for i, a in enumerate(grown, start=1):
-            psi.SetSite(i, a)
+        for i, (D1_, D2_, buf) in enumerate(up, start=1):
+            T._capi.check(lib.tn_mps_set_site(hmps, i, D1_, D2_, buf.data_ptr()), "tn_mps_set_site")
         psi.PrepareSweeps(H)
         psi.Sweep(H, 1, EPS_EIGEN, opts)
-        sites = [psi.GetSite(i) for i in range(1, args.L + 1)]
+        d2h = 0
+        for i in range(1, args.L + 1):
+            D1c, D2c = C.c_int(), C.c_int()
+            T._capi.check(lib.tn_mps_get_site_dims(hmps, i, C.byref(D1c), C.byref(D2c)), "dims")
+            n_ = psi.d * D1c.value * D2c.value
+            if down[i - 1].numel() < n_:
+                down[i - 1] = torch.empty(n_, dtype=torch.float64, pin_memory=True)
+            T._capi.check(lib.tn_mps_get_site(hmps, i, down[i - 1].data_ptr()), "tn_mps_get_site")
+            d2h += 8 * n_
         e2e_times.append(time.perf_counter() - t0)
-    d2h = sum(a.nbytes for a in sites)
     e2e = sum(e2e_times) / len(e2e_times)
 
     # --- the plain FP64 GPU sweep on the same schedule and seed
