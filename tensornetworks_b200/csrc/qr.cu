@@ -1309,8 +1309,8 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
 // registers as panel_wc does would need 4 RPL registers a thread) -- then the
 // panel's block reflector applied to the trailing columns, and after the last
 // panel to Q (formed backwards, the dorgqr order), by wy_cols_kernel: one CTA
-// per four columns c of C, z = V^T c, z2 = T' z, c -= V z2, with V (read
-// below the diagonal of the factored W) and T read through L1.
+// per four columns c of C, z = V^T c, z2 = T' z, c -= V z2, with V (from
+// below the diagonal of the factored W) staged in shared memory.
 constexpr int TALL_B = 16;        // columns per panel (one per warp)
 constexpr int TALL_MAXR = 1536;   // rows
 
@@ -1415,24 +1415,35 @@ __global__ void __launch_bounds__(PWC_THREADS, 1) qr_panel_tall_kernel(double* _
 // C (mp x nc, ld ldc) <- (I - V T' V^T) C, V mp x b (b <= 16) unit lower
 // trapezoidal read below its diagonal (ld ldv), T' = T^T (TRANS: applying
 // Q^T, the trailing update) or T (forming Q); T b x b upper, ld ldt.  One CTA
-// per WYC_COLS columns of C; its 8 warps split the rows (so that enough loads
-// are in flight), each warp's partial V^T c reduced by a butterfly, the 8
-// partials summed through shared memory in a fixed order.
+// per WYC_COLS columns of C: V is staged in shared memory once, with its unit
+// diagonal, zeros above it and zero columns past b written out, so both passes
+// are branch-free shared loads; the 8 warps split the rows, each warp's
+// partial V^T c is reduced by a butterfly, and the 8 partials are summed
+// through shared memory in a fixed order.
 constexpr int WYC_COLS = 4;
 constexpr int WYC_THREADS = 256;
+
+inline size_t wyc_smem_bytes(int mp) { return sizeof(double) * (size_t)TALL_B * (size_t)mp; }
 
 template <bool TRANS>
 __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __restrict__ V, int ldv,
                                                               const double* __restrict__ T, int ldt, int b,
                                                               double* __restrict__ C, int ldc, int mp, int nc) {
     constexpr int NW = WYC_THREADS / 32, NZ = WYC_COLS * TALL_B;
+    extern __shared__ double Vs[];  // [TALL_B][mp]
     __shared__ double zs[NW][NZ];
     __shared__ double zt[NZ];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int c0 = WYC_COLS * blockIdx.x;
-    double* Cc[WYC_COLS];
+#pragma unroll 8
+    for (int e = tid; e < TALL_B * mp; e += WYC_THREADS) {
+        const int l = e / mp, r = e - l * mp;
+        Vs[e] = l < b ? (r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0)) : 0.0;
+    }
+    const double* Cc[WYC_COLS];
 #pragma unroll
     for (int q = 0; q < WYC_COLS; ++q) Cc[q] = C + (size_t)min(c0 + q, nc - 1) * ldc;  // past nc: read, never written
+    __syncthreads();
     double z[WYC_COLS][TALL_B];
 #pragma unroll
     for (int q = 0; q < WYC_COLS; ++q)
@@ -1444,11 +1455,9 @@ __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __re
         for (int q = 0; q < WYC_COLS; ++q) x[q] = Cc[q][r];
 #pragma unroll
         for (int l = 0; l < TALL_B; ++l) {
-            if (l < b) {
-                const double v = r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0);
+            const double v = Vs[l * mp + r];
 #pragma unroll
-                for (int q = 0; q < WYC_COLS; ++q) z[q][l] = fma(v, x[q], z[q][l]);
-            }
+            for (int q = 0; q < WYC_COLS; ++q) z[q][l] = fma(v, x[q], z[q][l]);
         }
     }
 #pragma unroll
@@ -1465,11 +1474,11 @@ __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __re
             for (int l = 0; l < TALL_B; ++l) zs[w][q * TALL_B + l] = z[q][l];
     }
     __syncthreads();
-    if (threadIdx.x < NZ) {
+    if (tid < NZ) {
         double s = 0.0;
 #pragma unroll
-        for (int p = 0; p < NW; ++p) s += zs[p][threadIdx.x];
-        zt[threadIdx.x] = s;
+        for (int p = 0; p < NW; ++p) s += zs[p][tid];
+        zt[tid] = s;
     }
     __syncthreads();
     // z2 = T' z: T^T z takes z_k for k <= l, T z takes k >= l
@@ -1494,15 +1503,13 @@ __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __re
         for (int q = 0; q < WYC_COLS; ++q) x[q] = Cc[q][r];
 #pragma unroll
         for (int l = 0; l < TALL_B; ++l) {
-            if (l < b) {
-                const double v = r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0);
+            const double v = Vs[l * mp + r];
 #pragma unroll
-                for (int q = 0; q < WYC_COLS; ++q) x[q] = fma(-v, z[q][l], x[q]);
-            }
+            for (int q = 0; q < WYC_COLS; ++q) x[q] = fma(-v, z[q][l], x[q]);
         }
 #pragma unroll
         for (int q = 0; q < WYC_COLS; ++q)
-            if (c0 + q < nc) Cc[q][r] = x[q];
+            if (c0 + q < nc) C[(size_t)(c0 + q) * ldc + r] = x[q];
     }
 }
 
@@ -1529,12 +1536,22 @@ int qr_tall(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout
     if (m > TALL_MAXR) return TN_BAD_SHAPE;
     TN_CHECK(c.qrw.ensure(sizeof(double) * ((size_t)B * k + 16)));
     double* Tall = c.qrw.as<double>();
+    static thread_local int attr_dev = -1;
+    int dev = 0;
+    TN_CUDA_CHECK(cudaGetDevice(&dev));
+    if (attr_dev != dev) {
+        const int bytes = (int)wyc_smem_bytes(TALL_MAXR);
+        TN_CUDA_CHECK(cudaFuncSetAttribute(wy_cols_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        TN_CUDA_CHECK(cudaFuncSetAttribute(wy_cols_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        attr_dev = dev;
+    }
     auto update = [&](bool trans, int j0, int b, double* Cp, int ldc, int mp, int nc) -> int {
         const int blocks = (nc + WYC_COLS - 1) / WYC_COLS;
         const double* Vp = W + (size_t)j0 * m + j0;
         const double* Tp = Tall + (size_t)j0 * B;
-        if (trans) wy_cols_kernel<true><<<blocks, WYC_THREADS, 0, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
-        else wy_cols_kernel<false><<<blocks, WYC_THREADS, 0, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
+        const size_t smem = wyc_smem_bytes(mp);
+        if (trans) wy_cols_kernel<true><<<blocks, WYC_THREADS, smem, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
+        else wy_cols_kernel<false><<<blocks, WYC_THREADS, smem, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
         TN_LAUNCH_CHECK();
         return TN_OK;
     };
