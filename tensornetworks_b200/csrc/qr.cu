@@ -1309,8 +1309,15 @@ int qr_dense_reg(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double*
 // registers as panel_wc does would need 4 RPL registers a thread) -- then the
 // panel's block reflector applied to the trailing columns, and after the last
 // panel to Q (formed backwards, the dorgqr order), by wy_cols_kernel: one CTA
-// per four columns c of C, z = V^T c, z2 = T' z, c -= V z2, with V (from
-// below the diagonal of the factored W) staged in shared memory.
+// per eight columns of C, Z = V^T C and C -= V (T' Z) on the FP64 tensor
+// cores, with V (from below the diagonal of the factored W) staged in shared
+// memory.
+__device__ __forceinline__ void cq_dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
 constexpr int TALL_B = 16;        // columns per panel (one per warp)
 constexpr int TALL_MAXR = 1536;   // rows
 
@@ -1415,101 +1422,100 @@ __global__ void __launch_bounds__(PWC_THREADS, 1) qr_panel_tall_kernel(double* _
 // C (mp x nc, ld ldc) <- (I - V T' V^T) C, V mp x b (b <= 16) unit lower
 // trapezoidal read below its diagonal (ld ldv), T' = T^T (TRANS: applying
 // Q^T, the trailing update) or T (forming Q); T b x b upper, ld ldt.  One CTA
-// per WYC_COLS columns of C: V is staged in shared memory once, with its unit
-// diagonal, zeros above it and zero columns past b written out, so both passes
-// are branch-free shared loads; the 8 warps split the rows, each warp's
-// partial V^T c is reduced by a butterfly, and the 8 partials are summed
-// through shared memory in a fixed order.
-constexpr int WYC_COLS = 4;
+// per WYC_COLS = 8 columns of C, both products on the FP64 tensor cores (mma
+// m8n8k4): V is staged in shared memory once (unit diagonal, zeros above it
+// and past b written out; leading dimension 4 mod 16 doubles, so the
+// fragment loads of both products are conflict-free), Z = V^T C is summed
+// over the warps' row ranges in a fixed order, Z2 = T' Z is formed once, and
+// each warp takes row tiles of C -= V Z2.
+constexpr int WYC_COLS = 8;
 constexpr int WYC_THREADS = 256;
 
-inline size_t wyc_smem_bytes(int mp) { return sizeof(double) * (size_t)TALL_B * (size_t)mp; }
+inline int wyc_ldv(int mp) {
+    const int m4 = (mp + 7) & ~7;
+    return m4 + ((m4 & 15) == 0 ? 4 : 12);  // 4 mod 16
+}
+inline size_t wyc_smem_bytes(int mp) { return sizeof(double) * (size_t)TALL_B * (size_t)wyc_ldv(mp); }
 
 template <bool TRANS>
 __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __restrict__ V, int ldv,
                                                               const double* __restrict__ T, int ldt, int b,
                                                               double* __restrict__ C, int ldc, int mp, int nc) {
-    constexpr int NW = WYC_THREADS / 32, NZ = WYC_COLS * TALL_B;
-    extern __shared__ double Vs[];  // [TALL_B][mp]
-    __shared__ double zs[NW][NZ];
-    __shared__ double zt[NZ];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    constexpr int NW = WYC_THREADS / 32;
+    extern __shared__ double Vs[];                   // [TALL_B][lds]
+    __shared__ double zp[NW][2][64];                 // per-warp partial Z tiles (two 8 x 8 M-tiles)
+    __shared__ double Zs[TALL_B][WYC_COLS + 1];      // Z, then Z2 = T' Z
+    __shared__ double Tp[TALL_B][TALL_B + 1];        // T'
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, t4 = lane & 3;
     const int c0 = WYC_COLS * blockIdx.x;
-#pragma unroll 8
-    for (int e = tid; e < TALL_B * mp; e += WYC_THREADS) {
-        const int l = e / mp, r = e - l * mp;
-        Vs[e] = l < b ? (r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0)) : 0.0;
+    const int mp8 = (mp + 7) & ~7;
+    const int lds = mp8 + ((mp8 & 15) == 0 ? 4 : 12);
+#pragma unroll 4
+    for (int l = 0; l < TALL_B; ++l) {
+        for (int r = tid; r < mp8; r += WYC_THREADS)
+            Vs[l * lds + r] = (l < b && r < mp) ? (r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0)) : 0.0;
     }
-    const double* Cc[WYC_COLS];
-#pragma unroll
-    for (int q = 0; q < WYC_COLS; ++q) Cc[q] = C + (size_t)min(c0 + q, nc - 1) * ldc;  // past nc: read, never written
+    {
+        const int l = tid / TALL_B, k = tid % TALL_B;  // 256 threads: the 16 x 16 T'
+        double v = 0.0;
+        if (l < b && k < b && (TRANS ? k <= l : k >= l)) v = TRANS ? T[(size_t)l * ldt + k] : T[(size_t)k * ldt + l];
+        Tp[l][k] = v;
+    }
     __syncthreads();
-    double z[WYC_COLS][TALL_B];
+    // Z = V^T C over this warp's groups of 4 rows
+    {
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        const int col = c0 + g;
+        const double* Cg = C + (size_t)min(col, nc - 1) * ldc;
+        for (int ks = w; 4 * ks < mp8; ks += NW) {
+            const int r = 4 * ks + t4;
+            const double bv = (col < nc && r < mp) ? Cg[r] : 0.0;  // B[t][g] = C[4ks + t][c0 + g]
 #pragma unroll
-    for (int q = 0; q < WYC_COLS; ++q)
+            for (int mi = 0; mi < 2; ++mi) {
+                const double av = Vs[(8 * mi + g) * lds + r];    // A[g][t] = V[4ks + t][8mi + g]
+                cq_dmma(acc[mi], av, bv);
+            }
+        }
 #pragma unroll
-        for (int l = 0; l < TALL_B; ++l) z[q][l] = 0.0;
-    for (int r = lane + 32 * w; r < mp; r += WYC_THREADS) {
-        double x[WYC_COLS];
-#pragma unroll
-        for (int q = 0; q < WYC_COLS; ++q) x[q] = Cc[q][r];
-#pragma unroll
-        for (int l = 0; l < TALL_B; ++l) {
-            const double v = Vs[l * mp + r];
-#pragma unroll
-            for (int q = 0; q < WYC_COLS; ++q) z[q][l] = fma(v, x[q], z[q][l]);
+        for (int mi = 0; mi < 2; ++mi) {
+            zp[w][mi][2 * lane] = acc[mi][0];
+            zp[w][mi][2 * lane + 1] = acc[mi][1];
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int q = 0; q < WYC_COLS; ++q)
-#pragma unroll
-            for (int l = 0; l < TALL_B; ++l) z[q][l] += __shfl_xor_sync(0xffffffffu, z[q][l], o);
-    }
-    if (lane == 0) {
-#pragma unroll
-        for (int q = 0; q < WYC_COLS; ++q)
-#pragma unroll
-            for (int l = 0; l < TALL_B; ++l) zs[w][q * TALL_B + l] = z[q][l];
-    }
     __syncthreads();
-    if (tid < NZ) {
+    if (tid < 128) {  // Z[l][n]: tile mi = l / 8, fragment row l % 8, column n
+        const int mi = tid >> 6, e = tid & 63, ln = e >> 1;
+        const int l = 8 * mi + (ln >> 2), n = 2 * (ln & 3) + (e & 1);
         double s = 0.0;
 #pragma unroll
-        for (int p = 0; p < NW; ++p) s += zs[p][tid];
-        zt[tid] = s;
+        for (int p = 0; p < NW; ++p) s += zp[p][mi][e];
+        Zs[l][n] = s;
     }
     __syncthreads();
-    // z2 = T' z: T^T z takes z_k for k <= l, T z takes k >= l
+    double z2 = 0.0;
+    if (tid < 128) {
+        const int l = tid >> 3, n = tid & 7;
 #pragma unroll
-    for (int q = 0; q < WYC_COLS; ++q) {
-#pragma unroll
-        for (int l = 0; l < TALL_B; ++l) {
-            double a = 0.0;
-            if (l < b) {
-#pragma unroll
-                for (int k = 0; k < TALL_B; ++k) {
-                    if (k < b && (TRANS ? k <= l : k >= l))
-                        a = fma(TRANS ? T[(size_t)l * ldt + k] : T[(size_t)k * ldt + l], zt[q * TALL_B + k], a);
-                }
-            }
-            z[q][l] = a;
-        }
+        for (int k = 0; k < TALL_B; ++k) z2 = fma(Tp[l][k], Zs[k][n], z2);
     }
-    for (int r = lane + 32 * w; r < mp; r += WYC_THREADS) {
-        double x[WYC_COLS];
+    __syncthreads();
+    if (tid < 128) Zs[tid >> 3][tid & 7] = z2;
+    __syncthreads();
+    // C -= V Z2, 8-row tiles
+    double bz[4];
 #pragma unroll
-        for (int q = 0; q < WYC_COLS; ++q) x[q] = Cc[q][r];
+    for (int ks = 0; ks < 4; ++ks) bz[ks] = Zs[4 * ks + t4][g];  // B[t][g] = Z2[4ks + t][g]
+    for (int rt = w; 8 * rt < mp8; rt += NW) {
+        const int r0 = 8 * rt;
+        double d[2] = {0.0, 0.0};
 #pragma unroll
-        for (int l = 0; l < TALL_B; ++l) {
-            const double v = Vs[l * mp + r];
+        for (int ks = 0; ks < 4; ++ks) cq_dmma(d, Vs[(4 * ks + t4) * lds + r0 + g], bz[ks]);  // A[g][t] = V[r0 + g][4ks + t]
+        const int r = r0 + g;
 #pragma unroll
-            for (int q = 0; q < WYC_COLS; ++q) x[q] = fma(-v, z[q][l], x[q]);
+        for (int h = 0; h < 2; ++h) {
+            const int col = c0 + 2 * t4 + h;
+            if (r < mp && col < nc) C[(size_t)col * ldc + r] -= d[h];
         }
-#pragma unroll
-        for (int q = 0; q < WYC_COLS; ++q)
-            if (c0 + q < nc) C[(size_t)(c0 + q) * ldc + r] = x[q];
     }
 }
 
