@@ -682,6 +682,14 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
     key = hash_val(key, op.nLR);
     for (const DevBuf* b : {&msite.Fs, &msite.Gc, &msite.Xs, &msite.Ps, &msite.segs, &msite.shifts, &msite.err})
         key = hash_val(key, b->p);
+    // the Lanczos kernels that produce each Krylov vector also write its BF16
+    // pieces, so the matvec starts with its first GEMM
+    const VecSplit vsp{msite.Xs.as<uint16_t>(), ns, (long long)msite.nX};
+    struct PresplitScope {
+        MixedSite& m;
+        explicit PresplitScope(MixedSite& mm) : m(mm) { m.presplit = true; }
+        ~PresplitScope() { m.presplit = false; }
+    } presplit_scope(msite);
     const bool deferred = opt.refine_tol <= 0 && opt.verbose < 3 && ctx->aux2;
     if (deferred) {
         // nothing here waits for the host: restarts decided on the device, the
@@ -689,7 +697,7 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
         TN_CHECK(rq_slots());
         LzSummary* slot = reinterpret_cast<LzSummary*>(reinterpret_cast<double*>(rqhost.p) + RQ_SLOT * (size_t)ia + 4);
         const int rc = lanczos_solve_async(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, tol_rel,
-                                           key, slot);
+                                           key, slot, &vsp);
         if (rc == TN_OK) {
             rq_lz[ia] = 1;
             rq_flop[ia] = heff_flops(s);
@@ -702,7 +710,7 @@ int MPSState::refine_site_mixed(int ia, double epsEigen) {
         if (rc != LZ_ASYNC_UNAVAILABLE) return rc;
     }
     LzResult rm{};
-    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel, key));
+    TN_CHECK(lanczos_solve(*ctx, N, A[ia]->as<double>(), krylov, restarts, epsEigen, mvm, &rm, tol_rel, key, &vsp));
     if (ctx->prof) {  // the solve ended with a host wait, so the events have completed
         float a = 0;
         cudaEventElapsedTime(&a, ctx->pev[0], ctx->pev[1]);

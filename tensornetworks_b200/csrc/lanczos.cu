@@ -222,7 +222,7 @@ __global__ void lz_norm_kernel(const double* __restrict__ x, long long N, double
 
 // v0 = x / |x| (and the matvec input copy xcur when given).
 __global__ void lz_scale_kernel(const double* x, double* v0, long long N, const LzState* st, int fill_if_zero,
-                                double* xcur) {
+                                double* xcur, VecSplit sp = VecSplit{}) {
     double nr = st->xnorm;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         double v;
@@ -235,6 +235,7 @@ __global__ void lz_scale_kernel(const double* x, double* v0, long long N, const 
         } else v = 0.0;
         v0[i] = v;
         if (xcur) xcur[i] = v;
+        if (sp.out) split_bf16((float)v, sp.ns, sp.out, sp.stride, i);
     }
 }
 
@@ -314,7 +315,7 @@ __global__ void lz_update_kernel(const double* __restrict__ V, double* __restric
 // vector is then unused (and the half-counted ticket is cleared by the next
 // reset).
 __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict__ w, long long N,
-                               const double* partB, LzState* st, double* __restrict__ xcur,
+                               const double* partB, LzState* st, double* __restrict__ xcur, VecSplit sp,
                                cudaGraphConditionalHandle cond = 0) {
     pdl_wait();
     if (st->done) {
@@ -338,6 +339,7 @@ __global__ void lz_next_kernel(double* __restrict__ V, const double* __restrict_
         wi *= inv;
         vn[i] = wi;
         xcur[i] = wi;
+        if (sp.out) split_bf16((float)wi, sp.ns, sp.out, sp.stride, i);
     }
     if (blockIdx.x == 0) {
         if (threadIdx.x == 0) {
@@ -502,17 +504,18 @@ int step_matvec_dots(Ctx& c, const MatvecFn& mv, int grid, const double* V, doub
 
 // One Lanczos step: the matvec, then the vector work as three kernels.
 static int enqueue_lz_step(Ctx& c, const MatvecFn& mv, int grid, double* V, double* w, double* xcur, long long N,
-                           double* partial, LzState* s, cudaGraphConditionalHandle cond) {
+                           double* partial, LzState* s, const VecSplit& sp, cudaGraphConditionalHandle cond) {
     double* partB = partial + (size_t)grid * LZ_MAXK;
     TN_CHECK(step_matvec_dots(c, mv, grid, V, w, xcur, N, partial, s));
     TN_CHECK(launch_pdl(lz_update_kernel, grid, LZ_THREADS, 0, c.stream, (const double*)V, w, N,
                         (const double*)partial, partB, s));
     return launch_pdl(lz_next_kernel, grid, LZ_THREADS, 0, c.stream, V, (const double*)w, N, (const double*)partB, s,
-                      xcur, cond);
+                      xcur, sp, cond);
 }
 
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                  LzResult* out, double tol_rel, unsigned long long graph_key) {
+                  LzResult* out, double tol_rel, unsigned long long graph_key, const VecSplit* split) {
+    const VecSplit sp = split ? *split : VecSplit{};
     cudaStream_t st = c.stream;
     if (N <= 0) return TN_BAD_SHAPE;
     int mm = m;
@@ -534,7 +537,7 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
 
     // one Lanczos step; cond != 0 inside the graph body
     auto enqueue_step = [&](cudaGraphConditionalHandle cond) -> int {
-        return enqueue_lz_step(c, mv, grid, V, w, xcur, N, partial, s, cond);
+        return enqueue_lz_step(c, mv, grid, V, w, xcur, N, partial, s, sp, cond);
     };
 
     LzGraph* gr = nullptr;
@@ -543,6 +546,7 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         key = hash_val(key, N);
         key = hash_val(key, mm);
         key = hash_val(key, grid);
+        key = hash_val(key, (const void*)sp.out);
         key = hash_val(key, (const void*)V);
         key = hash_val(key, (const void*)s);
         key = hash_val(key, st);
@@ -593,7 +597,7 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
         TN_LAUNCH_CHECK();
         lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(x, N, partial, s);
         TN_LAUNCH_CHECK();
-        lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, V, N, s, 1, xcur);
+        lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(x, V, N, s, 1, xcur, sp);
         TN_LAUNCH_CHECK();
         if (c.prof) TN_CUDA_CHECK(cudaEventRecord(c.pev[3], st));
         if (gr) {
@@ -685,7 +689,8 @@ int add_while(cudaGraph_t owner, cudaGraph_t g, const std::vector<cudaGraphNode_
 }
 
 int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                        double tol_rel, unsigned long long graph_key, LzSummary* host_out) {
+                        double tol_rel, unsigned long long graph_key, LzSummary* host_out, const VecSplit* split) {
+    const VecSplit sp = split ? *split : VecSplit{};
     cudaStream_t st = c.stream;
     if (!graph_key || !c.use_graphs || st == nullptr || c.prof || N <= 0) return LZ_ASYNC_UNAVAILABLE;
     int mm = std::min(m, LZ_MAXK - 1);
@@ -713,6 +718,7 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
     key = hash_val(key, tol_rel);
     key = hash_val(key, (const void*)V);
     key = hash_val(key, (const void*)s);
+    key = hash_val(key, (const void*)sp.out);
     key = hash_val(key, st);
     auto it = c.lzgraphs.find(key);
     if (it == c.lzgraphs.end()) {
@@ -742,7 +748,7 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
         rc = capture_into(st, b_out, {}, [&]() -> int {
             lz_reset_kernel<<<1, 32, 0, st>>>(s, tol, tol_rel, 0, mm, h_in);
             lz_norm_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, N, partial, s);
-            lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, V, N, s, 1, xcur);
+            lz_scale_kernel<<<grid, LZ_THREADS, 0, st>>>(xw, V, N, s, 1, xcur, sp);
             return cudaGetLastError() == cudaSuccess ? TN_OK : TN_CUDA_ERROR;
         }, &front);
         if (rc != TN_OK) return fail(rc);
@@ -757,7 +763,7 @@ int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, 
         }
         const unsigned long long n0 = launch_count();
         rc = capture_into(st, b_in, {}, [&]() -> int {
-            return enqueue_lz_step(c, mv, grid, V, w, xcur, N, partial, s, h_in);
+            return enqueue_lz_step(c, mv, grid, V, w, xcur, N, partial, s, sp, h_in);
         }, nullptr);
         const unsigned long long kpi = launch_count() - n0;
         if (rc != TN_OK) return fail(rc);

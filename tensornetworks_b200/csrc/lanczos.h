@@ -1,5 +1,6 @@
 // lanczos.h -- device Lanczos state and host driver.
 #pragma once
+#include "split.cuh"
 #include <functional>
 
 #include "tn_internal.h"
@@ -62,8 +63,11 @@ int rayleigh_residual_async(cudaStream_t st, int sm_count, long long N, const do
 // graph_key != 0 identifies the operator (every pointer and shape mv's launches
 // depend on): the Lanczos steps of a restart then run as one CUDA graph with a
 // device-driven WHILE loop, recorded on first use of the key and replayed.
+// split (optional): the kernels that produce each Krylov vector also write its
+// BF16 pieces there (for a split-precision mv that skips its own splitting).
 int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                  LzResult* out, double tol_rel = 0.0, unsigned long long graph_key = 0);
+                  LzResult* out, double tol_rel = 0.0, unsigned long long graph_key = 0,
+                  const VecSplit* split = nullptr);
 
 // The same solve with the restart loop on the device too (a WHILE node around
 // the WHILE node of the steps), so that nothing waits for the host: enqueues
@@ -72,6 +76,7 @@ int lanczos_solve(Ctx& c, long long N, double* x, int m, int maxRestarts, double
 // nested graph cannot be built; the caller then uses lanczos_solve.
 constexpr int LZ_ASYNC_UNAVAILABLE = -1;
 int lanczos_solve_async(Ctx& c, long long N, double* x, int m, int maxRestarts, double tol, const MatvecFn& mv,
-                        double tol_rel, unsigned long long graph_key, LzSummary* host_out);
+                        double tol_rel, unsigned long long graph_key, LzSummary* host_out,
+                        const VecSplit* split = nullptr);
 
 }  // namespace tnb

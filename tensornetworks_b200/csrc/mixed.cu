@@ -29,21 +29,13 @@
 
 #include "mixed.h"
 #include "pdl.cuh"
+#include "split.cuh"
 
 namespace tnb {
 
 namespace {
 
 // v = piece0 + piece1 (+ piece2) + O(2^-8 per piece): successive BF16 remainders.
-__device__ __forceinline__ void split_bf16(float v, int ns, uint16_t* base, long long pstride, long long e) {
-    float r = v;
-    for (int q = 0; q < ns; ++q) {
-        __nv_bfloat16 h = __float2bfloat16_rn(r);
-        base[q * pstride + e] = __bfloat16_as_ushort(h);
-        r -= __bfloat162float(h);
-    }
-}
-
 inline int g1d(long long n) {
     long long b = (n + 255) / 256;
     return (int)(b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b));
@@ -358,8 +350,9 @@ int heff_matvec_mixed(Ctx& c, MixedSite& ms, const double* x, double* y, const i
     cudaStream_t st = c.stream;
     const ContractShape& s = ms.shape;
     const long long nX = (long long)s.d * s.D1 * s.D2;
-    TN_CHECK(launch_pdl(split_vec_kernel, g1d(nX), 256, 0, st, x, nX, ms.Xs.as<uint16_t>(), ms.nsplit,
-                        (long long)ms.nX, skip));
+    if (!ms.presplit)
+        TN_CHECK(launch_pdl(split_vec_kernel, g1d(nX), 256, 0, st, x, nX, ms.Xs.as<uint16_t>(), ms.nsplit,
+                            (long long)ms.nX, skip));
     TcChainPlan p1 = ms.plan1;
     p1.args.skip = skip;
     TN_CHECK(tc_chain_run(p1, st));

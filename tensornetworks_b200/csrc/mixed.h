@@ -29,6 +29,9 @@ struct MixedSite {
     TcChainPlan plan1, plan2;
     int splitk1 = 1, splitk2 = 1;  // chosen split-K factors of the two GEMMs
     bool ready = false;
+    // the input vector's pieces are already in Xs, written by the kernels that
+    // produced the vector (the Lanczos steps): heff_matvec_mixed skips its split
+    bool presplit = false;
 };
 
 inline bool mixed_supported(const ContractShape& s) {
