@@ -1450,11 +1450,16 @@ __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __re
     const int c0 = WYC_COLS * blockIdx.x;
     const int mp8 = (mp + 7) & ~7;
     const int lds = mp8 + ((mp8 & 15) == 0 ? 4 : 12);
-#pragma unroll 4
+    // V by asynchronous copies, all in flight at once; the unit diagonal, the
+    // zeros above it and past b, and the padding rows by plain stores
     for (int l = 0; l < TALL_B; ++l) {
-        for (int r = tid; r < mp8; r += WYC_THREADS)
-            Vs[l * lds + r] = (l < b && r < mp) ? (r > l ? V[(size_t)l * ldv + r] : (r == l ? 1.0 : 0.0)) : 0.0;
+        for (int r = tid; r < mp8; r += WYC_THREADS) {
+            double* dst = Vs + l * lds + r;
+            if (l < b && r > l && r < mp) cp_async8(dst, V + (size_t)l * ldv + r);
+            else *dst = (l < b && r == l) ? 1.0 : 0.0;
+        }
     }
+    cp_async_wait_all();
     {
         const int l = tid / TALL_B, k = tid % TALL_B;  // 256 threads: the 16 x 16 T'
         double v = 0.0;
@@ -1462,18 +1467,26 @@ __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __re
         Tp[l][k] = v;
     }
     __syncthreads();
-    // Z = V^T C over this warp's groups of 4 rows
+    // Z = V^T C over this warp's groups of 4 rows; the warp's C entries are
+    // loaded up front (independent loads in flight together)
     {
+        constexpr int MAXKS = (TALL_MAXR / 4 + NW - 1) / NW;
         double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
         const int col = c0 + g;
         const double* Cg = C + (size_t)min(col, nc - 1) * ldc;
-        for (int ks = w; 4 * ks < mp8; ks += NW) {
-            const int r = 4 * ks + t4;
-            const double bv = (col < nc && r < mp) ? Cg[r] : 0.0;  // B[t][g] = C[4ks + t][c0 + g]
+        double cv[MAXKS];
 #pragma unroll
-            for (int mi = 0; mi < 2; ++mi) {
-                const double av = Vs[(8 * mi + g) * lds + r];    // A[g][t] = V[4ks + t][8mi + g]
-                cq_dmma(acc[mi], av, bv);
+        for (int i = 0; i < MAXKS; ++i) {
+            const int r = 4 * (w + NW * i) + t4;
+            cv[i] = (col < nc && r < mp) ? Cg[r] : 0.0;  // B[t][g] = C[4ks + t][c0 + g]
+        }
+#pragma unroll
+        for (int i = 0; i < MAXKS; ++i) {
+            const int ks = w + NW * i;
+            if (4 * ks < mp8) {
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+                    cq_dmma(acc[mi], Vs[(8 * mi + g) * lds + 4 * ks + t4], cv[i]);  // A[g][t] = V[4ks + t][8mi + g]
             }
         }
 #pragma unroll
@@ -1505,16 +1518,25 @@ __global__ void __launch_bounds__(WYC_THREADS) wy_cols_kernel(const double* __re
     double bz[4];
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) bz[ks] = Zs[4 * ks + t4][g];  // B[t][g] = Z2[4ks + t][g]
-    for (int rt = w; 8 * rt < mp8; rt += NW) {
-        const int r0 = 8 * rt;
-        double d[2] = {0.0, 0.0};
+    constexpr int MAXRT = (TALL_MAXR / 8 + NW - 1) / NW;
+    double dd[MAXRT][2];
 #pragma unroll
-        for (int ks = 0; ks < 4; ++ks) cq_dmma(d, Vs[(4 * ks + t4) * lds + r0 + g], bz[ks]);  // A[g][t] = V[r0 + g][4ks + t]
-        const int r = r0 + g;
+    for (int i = 0; i < MAXRT; ++i) {
+        const int r0 = 8 * (w + NW * i);
+        dd[i][0] = dd[i][1] = 0.0;
+        if (r0 < mp8) {
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) cq_dmma(dd[i], Vs[(4 * ks + t4) * lds + r0 + g], bz[ks]);  // A[g][t] = V[r0 + g][4ks + t]
+        }
+    }
+    // the read-modify-writes of C after all the products, so their loads overlap
+#pragma unroll
+    for (int i = 0; i < MAXRT; ++i) {
+        const int r = 8 * (w + NW * i) + g;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int col = c0 + 2 * t4 + h;
-            if (r < mp && col < nc) C[(size_t)col * ldc + r] -= d[h];
+            if (r < mp && col < nc) C[(size_t)col * ldc + r] -= dd[i][h];
         }
     }
 }
@@ -1551,16 +1573,28 @@ int qr_tall(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout
         TN_CUDA_CHECK(cudaFuncSetAttribute(wy_cols_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         attr_dev = dev;
     }
-    auto update = [&](bool trans, int j0, int b, double* Cp, int ldc, int mp, int nc) -> int {
+    auto update = [&](cudaStream_t us, bool trans, int j0, int b, double* Cp, int ldc, int mp, int nc) -> int {
         const int blocks = (nc + WYC_COLS - 1) / WYC_COLS;
         const double* Vp = W + (size_t)j0 * m + j0;
         const double* Tp = Tall + (size_t)j0 * B;
         const size_t smem = wyc_smem_bytes(mp);
-        if (trans) wy_cols_kernel<true><<<blocks, WYC_THREADS, smem, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
-        else wy_cols_kernel<false><<<blocks, WYC_THREADS, smem, st>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
+        if (trans) wy_cols_kernel<true><<<blocks, WYC_THREADS, smem, us>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
+        else wy_cols_kernel<false><<<blocks, WYC_THREADS, smem, us>>>(Vp, m, Tp, B, b, Cp, ldc, mp, nc);
         TN_LAUNCH_CHECK();
         return TN_OK;
     };
+    // Look-ahead on two streams (as qr_lookahead): the main stream factors
+    // panel k, applies its reflector to panel k+1's columns only ("narrow") and
+    // factors panel k+1; the side stream applies it to every column beyond
+    // ("wide") meanwhile.  A narrow update waits for the previous wide update,
+    // which brought the same columns up to date with the reflector before.
+    cudaStream_t s1 = c.aux;
+    cudaEvent_t ev_p = c.ev_x[0], ev_w = c.ev_x[1], ev_q = c.ev_x[2];
+    if (s1) {
+        TN_CUDA_CHECK(cudaEventRecord(ev_p, st));  // the side stream starts after what is queued already
+        TN_CUDA_CHECK(cudaStreamWaitEvent(s1, ev_p, 0));
+    }
+    bool have_wide = false;
     for (int j0 = 0; j0 < k; j0 += B) {
         const int b = std::min(B, k - j0), mp = m - j0;
         double* Tp = Tall + (size_t)j0 * B;
@@ -1569,8 +1603,27 @@ int qr_tall(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout
         else if (mp <= 1024) TN_CHECK(launch_panel_tall<32>(st, W, m, m, j0, b, Tp, B));
         else if (mp <= 1280) TN_CHECK(launch_panel_tall<40>(st, W, m, m, j0, b, Tp, B));
         else TN_CHECK(launch_panel_tall<48>(st, W, m, m, j0, b, Tp, B));
-        const int nt = n - j0 - b;
-        if (nt > 0) TN_CHECK(update(true, j0, b, W + (size_t)(j0 + b) * m + j0, m, mp, nt));
+        const int c1 = j0 + b, nt = n - c1;
+        if (nt <= 0) continue;
+        if (!s1) {
+            TN_CHECK(update(st, true, j0, b, W + (size_t)c1 * m + j0, m, mp, nt));
+            continue;
+        }
+        TN_CUDA_CHECK(cudaEventRecord(ev_p, st));
+        const int nb_next = std::max(0, std::min(B, k - c1));
+        if (nb_next > 0) {
+            if (have_wide) TN_CUDA_CHECK(cudaStreamWaitEvent(st, ev_w, 0));
+            TN_CHECK(update(st, true, j0, b, W + (size_t)c1 * m + j0, m, mp, nb_next));
+        }
+        const int c2 = c1 + nb_next, nw = n - c2;
+        TN_CUDA_CHECK(cudaStreamWaitEvent(s1, ev_p, 0));
+        if (nw > 0) TN_CHECK(update(s1, true, j0, b, W + (size_t)c2 * m + j0, m, mp, nw));
+        TN_CUDA_CHECK(cudaEventRecord(ev_w, s1));
+        have_wide = true;
+    }
+    if (s1) {
+        TN_CUDA_CHECK(cudaEventRecord(ev_q, s1));
+        TN_CUDA_CHECK(cudaStreamWaitEvent(st, ev_q, 0));
     }
     if (Rout) {
         extract_r_kernel<<<g1d((long long)k * n), 256, 0, st>>>(W, m, k, n, Rout, ldr);
@@ -1581,7 +1634,7 @@ int qr_tall(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rout
         TN_LAUNCH_CHECK();
         for (int j0 = ((k - 1) / B) * B; j0 >= 0; j0 -= B) {
             const int b = std::min(B, k - j0);
-            TN_CHECK(update(false, j0, b, Qout + (size_t)j0 * ldq + j0, ldq, m - j0, k - j0));
+            TN_CHECK(update(st, false, j0, b, Qout + (size_t)j0 * ldq + j0, ldq, m - j0, k - j0));
         }
     }
     return TN_OK;
