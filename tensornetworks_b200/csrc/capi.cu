@@ -160,7 +160,6 @@ int tn_ctx_create(int device, tn_ctx* out) {
     if (const char* ng = std::getenv("TN_NO_GRAPHS")) c->c.use_graphs = !(ng[0] == '1');
     if (const char* np = std::getenv("TN_NO_PERSISTENT_QR")) c->c.use_persistent_qr = !(np[0] == '1');
     if (const char* fq = std::getenv("TN_QR_FORWARD_Q")) c->c.qr_forward_q = (fq[0] != '0');
-    if (const char* tm = std::getenv("TN_QR_TALL_MID")) c->c.qr_tall_mid = (tm[0] == '1');
     if (const char* sl = std::getenv("TN_QR_SPIN_LIMIT")) c->c.qr_spin_limit = std::max(1LL, std::atoll(sl));
     TN_CUDA_CHECK(cudaStreamCreateWithFlags(&c->c.own_stream, cudaStreamNonBlocking));
     c->c.stream = c->c.own_stream;

@@ -2,12 +2,16 @@
 //
 // Replaces LapackQRSolver::SolveThinQR / SolveThinLQ (dgeqrf + dorgqr,
 // LapackQRSolver.C:116-160,277-320) and is the gauge step of the sweep's site
-// normalisation.  A panel of b columns is factored by one CTA in shared
-// memory (column norms by block reduction, reflector application by one warp
-// per column); the trailing matrix and the explicit Q are updated with the
-// compact WY form I - V T V^T through the FP64 GEMM.  Reflectors follow the
-// dlarfg convention (no reflection when the sub-column is already zero), so a
-// zero column gives a zero R row and Q still gets an orthonormal column.
+// normalisation.  One path per row range: m <= 512, 32-column panels by the
+// warp-column panel (panel_wc) inside the persistent cooperative kernel (or,
+// when that cannot launch, the two-stream look-ahead); 512 < m <= 1536,
+// 16-column panels (qr_panel_tall_kernel) with block-reflector updates on the
+// FP64 tensor cores (wy_cols_kernel); m > 1536, a shared-memory panel
+// (qr_panel_kernel) with FP64-GEMM updates.  The trailing matrix and the
+// explicit Q are updated with the compact WY form I - V T V^T.  Reflectors
+// follow the dlarfg convention (no reflection when the sub-column is already
+// zero), so a zero column gives a zero R row and Q still gets an orthonormal
+// column.
 #include <algorithm>
 
 #include "qr.h"
@@ -133,206 +137,6 @@ __global__ void __launch_bounds__(QR_THREADS) qr_panel_kernel(double* __restrict
     for (int e = tid; e < b * b; e += blockDim.x) {
         int i = e % b, jj = e / b;
         T[(size_t)jj * ldt + i] = Ts[jj * 32 + i];
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Register-resident panel (m <= NT*R rows).  Thread t of NT owns rows t + k*NT
-// (R rows of B columns in registers), so each column step costs two block
-// reductions and two barriers: the norm of the sub-column, then one
-// reduce-scatter of v^T P over every other column of the panel.  The same
-// reduce-scatter yields V(:,0:jj)^T v_jj (the Gram column of the reflectors),
-// from which lane i of warp 0 builds row i of the dlarft T factor at the end.
-// Reflectors follow the dlarfg convention as above.
-//
-// Register indices must be compile-time, but unrolling all B column steps is
-// instruction-fetch bound; so the loop runs over groups of U steps and the
-// register window rotates by U columns per group.  At the start of a group
-// (first column jj0) slot i holds column jj0 + i for i < B - jj0 and the
-// finished reflector l < jj0 sits in slot B - jj0 + l.  (Measured: 256 x 2 x
-// 32 with U = 2 is as fast as 128 x 4 x 16, 256 x 2 x 16 and U = 1; 512
-// threads are slower.)
-
-// Reduce-scatter of B per-lane values over the warp: afterwards lane l holds
-// the warp's sum for slot (l mod B).  B is 16 or 32; f(i) yields slot i.
-template <int B, class F>
-__device__ __forceinline__ double warp_reduce_scatter(F f) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    double h[16];
-    if (B == 32) {
-        const bool up = lane & 16;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const double a = f(i), b = f(i + 16);
-            const double send = up ? a : b, keep = up ? b : a;
-            h[i] = keep + __shfl_xor_sync(full, send, 16);
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const double a = f(i);
-            h[i] = a + __shfl_xor_sync(full, a, 16);
-        }
-    }
-#pragma unroll
-    for (int k = 8; k >= 1; k >>= 1) {
-        const bool up = lane & k;
-#pragma unroll
-        for (int i = 0; i < k; ++i) {
-            const double send = up ? h[i] : h[i + k], keep = up ? h[i + k] : h[i];
-            h[i] = keep + __shfl_xor_sync(full, send, k);
-        }
-    }
-    return h[0];
-}
-
-template <int NT, int R, int B, int U>
-__global__ void __launch_bounds__(NT) qr_panel_reg_kernel(double* __restrict__ W, int ldw, int m, int j0, int b,
-                                                            double* __restrict__ V, int ldv,
-                                                            double* __restrict__ T, int ldt) {
-    static_assert(B % U == 0, "panel width must be a multiple of the group size");
-    constexpr int QRP_THREADS = NT, QRP_WARPS = NT / 32;
-    __shared__ double redN[QRP_WARPS];
-    __shared__ double redD[QRP_WARPS][32];
-    __shared__ double gsh[QRP_WARPS][32];
-    __shared__ double alpha_sh;
-    __shared__ double Gs[B][B + 1];   // Gs[l][jj] = v_l^T v_jj, l < jj
-    __shared__ double taus[B];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int mp = m - j0;
-    double p[R][B];
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int r = tid + k * QRP_THREADS;
-#pragma unroll
-        for (int c = 0; c < B; ++c)
-            p[k][c] = (r < mp && c < b) ? W[(size_t)(j0 + c) * ldw + j0 + r] : 0.0;
-    }
-#pragma unroll 1
-    for (int jj0 = 0; jj0 < b; jj0 += U) {
-        const int last_trail = B - 1 - jj0;  // slots u+1 .. last_trail are trailing columns
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int jj = jj0 + u;
-            if (jj >= b) break;
-            double part = 0;
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int r = tid + k * QRP_THREADS;
-                if (r > jj && r < mp) part = fma(p[k][u], p[k][u], part);
-            }
-            part = wsum(part);
-            if (lane == 0) redN[wid] = part;
-            if (tid == jj) alpha_sh = p[0][u];
-            __syncthreads();
-            double xn2 = 0;
-#pragma unroll
-            for (int w = 0; w < QRP_WARPS; ++w) xn2 += redN[w];
-            const double alpha = alpha_sh;
-            double t = 0, beta = alpha, scal = 0;
-            if (xn2 > 0.0) {
-                const double nrm = sqrt(alpha * alpha + xn2);
-                beta = alpha >= 0 ? -nrm : nrm;
-                const double amb = alpha - beta;
-                const double rinv = 1.0 / (beta * amb);  // tau = -amb / beta, scal = 1 / amb
-                t = -amb * amb * rinv;
-                scal = beta * rinv;
-            }
-            double v[R];
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int r = tid + k * QRP_THREADS;
-                if (r == jj) {
-                    v[k] = 1.0;
-                    p[k][u] = beta;
-                } else if (r > jj && r < mp) {
-                    if (t != 0.0) p[k][u] *= scal;
-                    v[k] = p[k][u];
-                } else {
-                    v[k] = 0.0;
-                }
-            }
-            // every slot but u: v_jj^T (trailing column or finished reflector)
-            const double red = warp_reduce_scatter<B>([&](int i) {
-                double sacc = 0;
-                if (i != u) {
-#pragma unroll
-                    for (int k = 0; k < R; ++k) sacc = fma(v[k], p[k][i], sacc);
-                }
-                return sacc;
-            });
-            redD[wid][lane] = red;
-            __syncthreads();
-            double g = 0;
-#pragma unroll
-            for (int w = 0; w < QRP_WARPS; ++w) g += redD[w][lane];
-            gsh[wid][lane] = g;
-            __syncwarp();
-            if (t != 0.0) {
-#pragma unroll
-                for (int i = u + 1; i < B; ++i) {
-                    if (i <= last_trail) {
-                        const double ts = t * gsh[wid][i];
-#pragma unroll
-                        for (int k = 0; k < R; ++k) p[k][i] = fma(-ts, v[k], p[k][i]);
-                    }
-                }
-            }
-            if (wid == 0) {
-                // column jj of V^T V (reflector l sits in slot B - jj0 + l or l - jj0)
-                if (lane < jj) Gs[lane][jj] = gsh[0][lane < jj0 ? B - jj0 + lane : lane - jj0];
-                if (lane == 0) taus[jj] = t;
-            }
-        }
-        // rotate the window left by U columns
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            double keep[U];
-#pragma unroll
-            for (int i = 0; i < U; ++i) keep[i] = p[k][i];
-#pragma unroll
-            for (int i = 0; i < B - U; ++i) p[k][i] = p[k][i + U];
-#pragma unroll
-            for (int i = 0; i < U; ++i) p[k][B - U + i] = keep[i];
-        }
-    }
-    // after the groups slot i holds column (i + rb) mod B, rb = b rounded up to the group size
-    const int rb = ((b + U - 1) / U) * U;
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int r = tid + k * QRP_THREADS;
-        if (r < mp) {
-#pragma unroll
-            for (int i = 0; i < B; ++i) {
-                const int c = (i + rb) % B;
-                if (c < b) {
-                    W[(size_t)(j0 + c) * ldw + j0 + r] = p[k][i];
-                    V[(size_t)c * ldv + r] = (r < c) ? 0.0 : (r == c ? 1.0 : p[k][i]);
-                }
-            }
-        }
-    }
-    __syncthreads();
-    // dlarft (forward, columnwise): T(i, jj) = -tau_jj sum_{l=i}^{jj-1} T(i, l) G(l, jj),
-    // T(i, i) = tau_i.  Row i needs only row i, so lane i builds it in registers.
-    if (wid == 0 && lane < B) {
-        const int i = lane;
-        double trow[B];
-#pragma unroll
-        for (int jj = 0; jj < B; ++jj) {
-            double a0 = 0, a1 = 0;
-#pragma unroll
-            for (int l = 0; l < jj; ++l) {
-                const double term = (l >= i) ? trow[l] * Gs[l][jj] : 0.0;
-                if (l & 1) a1 += term; else a0 += term;
-            }
-            const double tj = jj < b ? taus[jj] : 0.0;
-            trow[jj] = (jj < i) ? 0.0 : (jj == i ? tj : -tj * (a0 + a1));
-        }
-#pragma unroll
-        for (int jj = 0; jj < B; ++jj)
-            if (i < b && jj < b) T[(size_t)jj * ldt + i] = trow[jj];
     }
 }
 
@@ -572,16 +376,12 @@ __global__ void __launch_bounds__(PWC_THREADS) qr_panel_wc_kernel(double* __rest
     panel_wc_any(W, ldw, m, j0, b, V, ldv, T, ldt, sm);
 }
 
-// Panel launch: the warp-column kernel for 32-wide panels of at most 512 rows,
-// the row-per-thread register kernel otherwise.
+// Panel launch of the look-ahead and single-stream paths (m <= 512, 32-wide
+// panels): the warp-column kernel.
 template <int NT, int R, int B, int U>
 void launch_panel(cudaStream_t st, double* W, int ldw, int m, int j0, int b, double* V, int ldv, double* T, int ldt) {
-    const int mp = m - j0;
-    if (B == 32 && mp <= PWC_MAXR) {
-        qr_panel_wc_kernel<<<1, PWC_THREADS, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
-    } else {
-        qr_panel_reg_kernel<NT, R, B, U><<<1, NT, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
-    }
+    static_assert(B == 32, "the warp-column panel is 32 columns wide");
+    qr_panel_wc_kernel<<<1, PWC_THREADS, 0, st>>>(W, ldw, m, j0, b, V, ldv, T, ldt);
 }
 
 // C (mp x nc, ld ldc) <- (I - V T' V^T) C with T' = T^T (TRANS: applying Q^T,
@@ -1656,8 +1456,7 @@ int qr_dense(Ctx& c, int m, int n, double* W, double* Qout, int ldq, double* Rou
     cudaStream_t st = c.stream;
     if (m <= 0 || n <= 0) return TN_BAD_SHAPE;
     if (m <= 512) return qr_dense_reg<256, 2, 32, 2>(c, m, n, W, Qout, ldq, Rout, ldr);
-    if (m <= TALL_MAXR && (m > 1024 || c.qr_tall_mid)) return qr_tall(c, m, n, W, Qout, ldq, Rout, ldr);
-    if (m <= 1024) return qr_dense_reg<256, 4, 16, 2>(c, m, n, W, Qout, ldq, Rout, ldr);
+    if (m <= TALL_MAXR) return qr_tall(c, m, n, W, Qout, ldq, Rout, ldr);
     const int k = std::min(m, n);
     const int bmax = panel_width(m);
     if ((size_t)m * bmax * 8 > 200 * 1024 || bmax < 1) {

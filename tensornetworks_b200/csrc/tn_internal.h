@@ -200,7 +200,6 @@ struct Ctx {
     int sm_count = 148;
     bool use_persistent_qr = true;  // TN_NO_PERSISTENT_QR=1: the two-stream look-ahead QR instead
     bool qr_forward_q = true;       // TN_QR_FORWARD_Q=0: the persistent QR forms the thin Q after the panels
-    bool qr_tall_mid = false;       // TN_QR_TALL_MID=1: the 16-column tall QR also for 512 < m <= 1024
     long long qr_spin_limit = 1LL << 21;  // polls per wait in the persistent QR (TN_QR_SPIN_LIMIT)
     // cache of the last MPO term list uploaded through the C ABI
     std::vector<double> wcache_W;

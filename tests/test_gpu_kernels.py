@@ -180,18 +180,14 @@ def test_qr_rank_deficient_panels(T, ctx, oracle, m, n):
     assert np.abs(Q @ R - A).max() < 1e-12
 
 
-@pytest.mark.parametrize("mid", ["0", "1"])
-def test_qr_tall_path(T, oracle, monkeypatch, mid):
+def test_qr_tall_path(T, oracle):
     """The 16-column-panel QR for 512 < m <= 1536 (the S = 1, D = 512 gauge
-    shape 1536 x 512 among them; with TN_QR_TALL_MID=1 also for m <= 1024):
-    orthonormal Q, Q R = A and the oracle's R, ragged last panels and wide
-    matrices included; the LQ of the transposed shape goes the same way."""
-    monkeypatch.setenv("TN_QR_TALL_MID", mid)
+    shape 1536 x 512 among them): orthonormal Q, Q R = A and the oracle's R,
+    ragged last panels and wide matrices included; the LQ of the transposed
+    shape goes the same way."""
     c = T.Context(0)
     rng = np.random.default_rng(41)
-    shapes = [(1536, 512), (1100, 300), (1300, 1400), (1536, 23)]
-    if mid == "1":
-        shapes += [(768, 256), (1024, 512), (600, 700), (513, 40)]
+    shapes = [(1536, 512), (1100, 300), (1300, 1400), (1536, 23), (768, 256), (1024, 512), (600, 700), (513, 40)]
     for m, n in shapes:
         A = rng.uniform(-1, 1, size=(m, n))
         Q, R = T.CudaQRSolver(c).SolveThinQR(A)
